@@ -1,0 +1,335 @@
+"""Benchmark of the Genz QMC multivariate-normal probability path on B200.
+
+Metric: time of one d = 1000 probability (the factor-model workload: Sigma =
+B B' + diag(psi) normalised, B 1000 x 20, a = -inf, b = Phi^-1(p),
+Richtmyer lattice, 2^17 points x 16 shifts = 2,097,152 samples), in the
+mixed-precision mode, beside the FP64 GPU path on the same points and
+shifts; one step = one qmc_pnorm! pass over all samples.
+
+  value      device time per step (CUDA events on the library's stream),
+             problem resident in HBM, L2 flushed (256 MiB write) between steps
+  e2e        the same step through the C ABI from host buffers: upload of
+             Sigma/a/b/shifts, GPU factorisation, integration, read-back
+  roofline   the integration-loop kernel against the measured dense bf16
+             tensor peak (contraction flops = samples * d (d - 1) per launch)
+  cpu_baseline  the CPU checker (C restatement of the reference's Float64
+             loop, OpenMP on all host cores) on a bounded sample, projected
+             to the full step
+
+``--impl reference`` times only the CPU restatement of the reference path
+(all host threads), on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "d=1000 MVN P time at |err|<=1e-5 vs FP64: mixed-prec vs FP64 GPU; grad/fwd cost"
+UNIT = "ms"
+MIXED = "fp32_simt"   # best mixed-precision mode built into this library
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.lines: list[str] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(rank: int, world: int, quick: bool):
+    from dbgenzpaper_b200 import workloads as W
+    if quick:
+        w = W.c3(d=200, m=2**12, n_reps=16)
+    else:
+        w = W.c3()
+    # weak scaling: every rank integrates its own 16 shifts of the same problem
+    if world > 1:
+        rng = np.random.default_rng(10_000 + rank)
+        w.shifts = rng.random(w.shifts.shape)
+    return w
+
+
+def cpu_baseline(w, threads: int, target_s: float = 12.0):
+    """Time the CPU checker on a bounded sample of workload w; project to a full step."""
+    from oracle import oracle as O
+    F = O.cholesky_genz(w.Sigma, w.a, w.b)
+    U = O.truncate_U(F["U"])
+    kw = dict(block_size_i=1024, block_size_i2=64, block_size_j=64, threads=threads)
+    # calibrate on a small sample, then size the timed sample to ~target_s
+    m0, r0 = 1024, 2
+    t = time.perf_counter()
+    O.qmc_pnorm(U, F["a"], F["b"], m=m0, n_reps=r0, shifts=w.shifts[:, :r0], **kw)
+    rate0 = m0 * r0 / (time.perf_counter() - t)
+    n_reps = min(w.n_reps, 4)
+    m = int(min(w.m, max(1024, rate0 * target_s / n_reps)))
+    t = time.perf_counter()
+    O.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=n_reps, shifts=w.shifts[:, :n_reps], **kw)
+    dt = time.perf_counter() - t
+    rate = m * n_reps / dt
+    return {
+        "value": 1e3 * w.samples / rate,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": "port",
+        "sample": f"{m} points x {n_reps} shifts of the d={w.d} workload ({m * n_reps} samples, "
+                  f"{dt:.1f} s on {threads} threads, FP64, factorisation excluded); "
+                  f"projected to {w.samples} samples",
+        "samples_per_s": rate,
+    }
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    O.build()
+    w = workload(0, 1, args.quick)
+    F = O.cholesky_genz(w.Sigma, w.a, w.b)
+    U = O.truncate_U(F["U"])
+    kw = dict(block_size_i=1024, block_size_i2=64, block_size_j=64, threads=threads)
+    # bounded step: 2 shifts x m points, sized to ~1.5 s of CPU work
+    t = time.perf_counter()
+    O.qmc_pnorm(U, F["a"], F["b"], m=512, n_reps=2, shifts=w.shifts[:, :2], **kw)
+    rate0 = 1024 / (time.perf_counter() - t)
+    m = int(min(w.m, max(512, rate0 * 1.5 / 2)))
+    for _ in range(args.warmup):
+        O.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=2, shifts=w.shifts[:, :2], **kw)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        O.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=2, shifts=w.shifts[:, :2], **kw)
+        times.append(time.perf_counter() - t)
+    rate = 2 * m / statistics.mean(times)
+    val = 1e3 * w.samples / rate
+    line = {
+        "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": val, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "d": w.d, "points": w.m, "shifts": w.n_reps,
+                   "samples": w.samples},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"each step {m} points x 2 shifts ({2 * m} samples) of the d={w.d} "
+                                   f"workload on {threads} threads, projected to {w.samples} samples "
+                                   "(C restatement of the reference's Float64 qmc_loop!; Julia is "
+                                   "not installed on this image)"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=MIXED)
+    ap.add_argument("--quick", action="store_true", help="small d=200 case for smoke runs")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import dbgenzpaper_b200 as D
+    from dbgenzpaper_b200 import _lib as L
+    from dbgenzpaper_b200 import shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    lib = L.lib()
+    ctx = D.get_context(local)
+    lib.dbgz_set_profiling(ctx.handle, 1)
+    prec_mixed = D.PRECISIONS[args.precision]
+    w = workload(rank, world, args.quick)
+    d = w.d
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def make(precision):
+        opts = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0)
+        return D.QMCData(w.Sigma, w.a, w.b, opts, qmc_type="Richtmyer", shifts=w.shifts,
+                         precision=precision, device=local)
+
+    prof = L.DbgzProfile()
+
+    def step(Q, precision):
+        flush.zero_()
+        torch.cuda.synchronize()
+        r = D.qmc_pnorm(Q, precision=precision, return_reps=True)
+        lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+        return r, prof.pnorm_ms, prof.loop_ms, prof.loop_launches, prof.kernel_launches
+
+    def timed(Q, precision, steps, warmup):
+        for _ in range(warmup):
+            step(Q, precision)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        tot = loop = 0.0
+        nl = nk = 0
+        res = None
+        for _ in range(steps):
+            res, pm, lm, ll, kl = step(Q, precision)
+            tot += pm
+            loop += lm
+            nl += ll
+            nk += kl
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return res, tot / steps, loop / max(nl, 1), nl, nk
+
+    Q = make(prec_mixed)
+    peaks, peak_kind = _peaks()
+    with ClockSampler(local) as clk:
+        (P_mix, err_mix, npts, reps_mix), ms_mix, loop_ms, n_loop, n_kern = timed(
+            Q, prec_mixed, args.steps, args.warmup)
+    clocks = clk.summary()
+    # FP64 GPU path on the same points and shifts
+    k64 = max(2, args.steps // 2)
+    (P64, err64, _, reps64), ms64, loop64_ms, _, _ = timed(Q, L.PREC_FP64, k64, 1)
+
+    # e2e: the public API from host buffers, upload and factorisation included
+    def e2e_step():
+        t = time.perf_counter()
+        Qe = make(prec_mixed)
+        r = D.qmc_pnorm(Qe, precision=prec_mixed)
+        Qe.close()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t, r
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    e2e_t = [e2e_step()[0] for _ in range(max(3, args.steps // 2))]
+    e2e_ms = 1e3 * statistics.mean(e2e_t)
+    h2d = w.Sigma.nbytes + w.a.nbytes + w.b.nbytes + w.shifts.nbytes
+    d2h = 8 * w.n_reps + 3 * 8
+
+    ms_step = ms_mix
+    if dist:
+        t = torch.tensor([ms_mix, ms64, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step, ms64, e2e_ms = (float(x) for x in t.cpu())
+        reps_all = shard.gather_reps(reps_mix, w.n_reps * world)
+        reps64_all = shard.gather_reps(reps64, w.n_reps * world)
+        P_mix, err_mix = shard.combine(reps_all)
+        P64, err64 = shard.combine(reps64_all)
+
+    if rank == 0:
+        flops = float(w.samples) * d * (d - 1)
+        achieved = flops / (loop_ms * 1e-3) / 1e12
+        peak = float(peaks.get("bf16_tflops", 1590.0))
+        line = {
+            "metric": METRIC, "value": ms_step, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": w.name, "d": d, "points": w.m, "shifts_per_gpu": w.n_reps,
+                       "samples_per_gpu": w.samples, "precision": args.precision,
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"shifts sharded over {world} GPU(s)"},
+            "fp64_ms_per_step": ms64,
+            "speedup_vs_fp64": ms64 / ms_step,
+            "P": P_mix, "P_fp64": P64, "abs_err_vs_fp64": abs(P_mix - P64),
+            "rel_err_vs_fp64": abs(P_mix - P64) / abs(P64) if P64 else None,
+            "qmc_3sem": err_mix,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": f"integration loop ({args.precision})",
+                         "flops_per_launch": flops, "launch_ms": loop_ms,
+                         "peak_source": f"{peak_kind} bf16_tflops (burst)"},
+            "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(n_kern),
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(w, os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    del Q
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,345 @@
+"""dbgenzpaper_b200 -- B200-native Genz QMC multivariate-normal probabilities.
+
+Host-side mirror of the reference package's API (JakobPeterlin/DBGenzPaper,
+src/DBGenzPaper.jl exports) over the C ABI of ``libdbgenz.so``:
+
+====================================  =====================================
+reference (Julia)                     here
+====================================  =====================================
+``QMC_opts(T; kw...)`` qmc.jl:111     ``QMC_opts(T, **kw)``
+``QMCData(C,a,b,opts,rng,type)``      ``QMCData(C, a, b, opts, rng, type)``
+``QMCDataSparse(...)`` qmc.jl:225     ``QMCDataSparse(...)``
+``QMCData_Distributions(D)`` :210     ``QMCData_Distributions(D)``
+``qmc_pnorm!(D)`` qmc.jl:783          ``qmc_pnorm(D)``
+``cholesky_genz!`` cholesky.jl:445    ``cholesky_genz(M, a, b, ...)``
+``cholesky_classic!`` :144            ``cholesky_classic(M, a, b, ...)``
+``get_sqrt_primes!`` generators:300   ``get_sqrt_primes(n)``
+``richtmyer_mat!`` generators:314     ``richtmyer_mat(m, q, n0)``
+``sobol_mat!`` generators:331         ``sobol_mat(m, V, first)``
+====================================  =====================================
+
+Everything computes on the GPU; there is no CPU path.  The working type ``T``
+of ``QMC_opts`` selects the precision: ``np.float64`` runs the FP64 kernels,
+``np.float32`` the mixed-precision ones (FP32 special functions, FP64 weight
+product and reductions, tensor-core contraction).  A ``precision=`` keyword
+picks any mode of ``dbgz_precision`` explicitly.
+
+Random shifts: the reference draws them from a Julia RNG inside the
+constructor (``rand(rng, T, n-1, n_reps)``); here ``rng`` is a numpy
+``Generator`` (or the shifts are passed explicitly with ``shifts=``), since
+Julia's stream cannot be reproduced outside Julia.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, replace
+from typing import NamedTuple, Optional
+
+import numpy as np
+
+from . import _lib as L
+
+__all__ = [
+    "QMCOpts", "QMC_opts", "QMCData", "QMCDataSparse", "QMCData_Distributions",
+    "qmc_pnorm", "CholeskyGenz", "cholesky_genz", "cholesky_classic",
+    "get_sqrt_primes", "richtmyer_mat", "sobol_mat", "sobol_dirnums", "Context",
+    "get_context", "DbgzError", "PRECISIONS",
+]
+
+DbgzError = L.DbgzError
+PRECISIONS = {
+    "fp64": L.PREC_FP64,
+    "fp32_tf32": L.PREC_FP32_TF32,
+    "fp32_split_bf16": L.PREC_FP32_SPLIT_BF16,
+    "fp32_simt": L.PREC_FP32_SIMT,
+}
+# precision used for QMC_opts(np.float32)
+DEFAULT_FP32_PRECISION = L.PREC_FP32_SIMT
+
+
+class Context:
+    """One CUDA device and stream of libdbgenz (dbgz_create/dbgz_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = L.lib()
+        h = C.c_void_p()
+        L.check(self._lib.dbgz_create(int(device), C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self._lib.dbgz_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_contexts: dict[int, Context] = {}
+
+
+def get_context(device: int = 0) -> Context:
+    ctx = _contexts.get(device)
+    if ctx is None:
+        ctx = _contexts[device] = Context(device)
+    return ctx
+
+
+# ---------------------------------------------------------------------------
+@dataclass(frozen=True)
+class QMCOpts:
+    """QMCOpts{T} (src/qmc.jl:15-27)."""
+    T: type
+    chol_block_size: int
+    chol_block_size2: int
+    m: int
+    block_size_i: int
+    block_size_i2: int
+    block_size_j: int
+    n_blocks: int
+    n_reps: int
+    n_bits: int
+    max_pts: int
+    max_abs_err: float
+
+    def to_c(self) -> L.DbgzOpts:
+        return L.DbgzOpts(self.chol_block_size, self.chol_block_size2, self.m,
+                          self.block_size_i, self.block_size_i2, self.block_size_j,
+                          self.n_blocks, self.n_reps, self.n_bits, self.max_pts,
+                          float(self.max_abs_err))
+
+
+def QMC_opts(T=np.float64, *, chol_block_size=2**6, chol_block_size2=2**9, m=10**4,
+             block_size_i=2**6, block_size_j=2**6, block_size_i2=2**5, n_blocks=1,
+             n_reps=12, n_bits=32, max_pts=10**4, max_abs_err=1e-6) -> QMCOpts:
+    """QMC_opts(T; ...) with the reference's defaults (src/qmc.jl:111-125)."""
+    T = np.dtype(T).type
+    if T not in (np.float64, np.float32):
+        raise TypeError("T must be float64 or float32")
+    return QMCOpts(T, int(chol_block_size), int(chol_block_size2), int(m), int(block_size_i),
+                   int(block_size_i2), int(block_size_j), int(n_blocks), int(n_reps),
+                   int(n_bits), int(max_pts), float(max_abs_err))
+
+
+class CholeskyGenz(NamedTuple):
+    """CholeskyGenz{T} (src/cholesky.jl:5-14); perm is 0-based."""
+    U: np.ndarray
+    perm: np.ndarray
+    rank: int
+    a: np.ndarray
+    b: np.ndarray
+    block_size: int
+    pivot_method: str
+    scale_vec: np.ndarray
+
+
+def _f64(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+# ---------------------------------------------------------------------------
+class QMCData:
+    """QMCData (src/qmc.jl:149-202): factorisation, generator and workspaces
+    of one problem, resident on the GPU."""
+
+    _structure = L.STRUCTURE_DENSE
+    _default_type = "Richtmyer"
+
+    def __init__(self, C_mat, a, b, opts: Optional[QMCOpts] = None, rng=None, qmc_type=None, *,
+                 shifts=None, ushifts=None, sobol_dirnums=None, sobol_first=None,
+                 precision: Optional[int] = None, cdf_form: int = L.CDF_ERF, device: int = 0):
+        qmc_type = self._default_type if qmc_type is None else str(qmc_type).lstrip(":")
+        if qmc_type not in ("Richtmyer", "Sobol"):
+            raise ValueError("qmc_type must be 'Richtmyer' or 'Sobol'")
+        opts = QMC_opts() if opts is None else opts
+        Sig = np.asfortranarray(np.asarray(C_mat, dtype=np.float64))
+        n = Sig.shape[0]
+        if Sig.shape != (n, n):
+            raise ValueError("C must be square")
+        a, b = _f64(a), _f64(b)
+        if a.shape != (n,) or b.shape != (n,):
+            raise ValueError("a and b must have length n")
+        rng = np.random.default_rng() if rng is None else rng
+        self.ctx = get_context(device)
+        self.n = n
+        self.opts = opts
+        self.qmc_type = qmc_type
+        self.precision = precision
+        self.cdf_form = cdf_form
+        d1 = max(n - 1, 1)
+        sh = ush = V = None
+        first = 0
+        if qmc_type == "Richtmyer":
+            sh = rng.random((d1, opts.n_reps)) if shifts is None else np.asarray(shifts, np.float64)
+            if opts.T == np.float32 and shifts is None:
+                sh = sh.astype(np.float32).astype(np.float64)
+            sh = np.asfortranarray(sh)
+            if sh.shape != (d1, opts.n_reps):
+                raise ValueError(f"shifts must be {(d1, opts.n_reps)}")
+        else:
+            if ushifts is None:
+                ush = rng.integers(0, 2**64, size=(d1, opts.n_reps), dtype=np.uint64, endpoint=False)
+            else:
+                ush = np.asarray(ushifts, dtype=np.uint64)
+            ush = np.asfortranarray(ush)
+            if sobol_dirnums is not None:
+                V = np.ascontiguousarray(sobol_dirnums, dtype=np.uint32)
+            # SobolQMC skips skip0 = 2m - 1 points (src/qmc.jl:178)
+            first = (2 * opts.m - 1) + 1 if sobol_first is None else int(sobol_first)
+        self.shifts, self.ushifts, self.sobol_dirnums, self.sobol_first = sh, ush, V, first
+        h = C.c_void_p()
+        co = opts.to_c()
+        st = L.lib().dbgz_prepare(self.ctx.handle, n, L.ptr(Sig), L.ptr(a), L.ptr(b), C.byref(co),
+                                  L.QMC_RICHTMYER if qmc_type == "Richtmyer" else L.QMC_SOBOL,
+                                  self._structure, int(cdf_form), L.ptr(sh),
+                                  L.ptr(ush, C.c_uint64), L.ptr(V, C.c_uint32), first, C.byref(h))
+        L.check(st, self.ctx.handle)
+        self.handle = h
+        self._chol = None
+
+    @property
+    def C(self) -> CholeskyGenz:
+        if self._chol is None:
+            n = self.n
+            U = np.zeros((n, n), order="F")
+            perm = np.zeros(n, dtype=np.int64)
+            a, b, sv = np.zeros(n), np.zeros(n), np.zeros(n)
+            rank = C.c_int64()
+            L.check(L.lib().dbgz_problem_factor(self.handle, L.ptr(U), L.ptr(perm, C.c_int64),
+                                                L.ptr(a), L.ptr(b), L.ptr(sv), C.byref(rank)),
+                    self.ctx.handle)
+            method = "genz" if self._structure == L.STRUCTURE_DENSE else "none"
+            self._chol = CholeskyGenz(U, perm, rank.value, a, b, self.opts.chol_block_size,
+                                      method, sv)
+        return self._chol
+
+    @property
+    def a(self):
+        return self.C.a
+
+    @property
+    def b(self):
+        return self.C.b
+
+    def resolved_precision(self) -> int:
+        if self.precision is not None:
+            return int(self.precision)
+        return L.PREC_FP64 if self.opts.T == np.float64 else DEFAULT_FP32_PRECISION
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib().dbgz_problem_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class QMCDataSparse(QMCData):
+    """QMCDataSparse (src/qmc.jl:225-282): classic (unpivoted) Cholesky and
+    the loop over the strict-upper CSC of U.  Default generator: Sobol."""
+
+    _structure = L.STRUCTURE_SPARSE
+    _default_type = "Sobol"
+
+
+class QMCData_Distributions:
+    """QMCData_Distributions(D) (src/qmc.jl:210-215): the same problem and
+    generator state as D, integrated with the erfc form of the CDF."""
+
+    def __init__(self, D: QMCData):
+        self.D = D
+
+    def __getattr__(self, name):
+        return getattr(self.D, name)
+
+
+def qmc_pnorm(D, use_AppleBLAS=None, *, precision: Optional[int] = None, return_reps=False):
+    """qmc_pnorm!(D) (src/qmc.jl:783-850) -> (result, err, n_pts).
+
+    ``use_AppleBLAS`` is accepted for signature compatibility (it only steers
+    CPU BLAS threading in the reference).  With ``return_reps`` the per-shift
+    running means are returned as a fourth element."""
+    dist = isinstance(D, QMCData_Distributions)
+    base = D.D if dist else D
+    prec = base.resolved_precision() if precision is None else int(precision)
+    res, err, npts = C.c_double(), C.c_double(), C.c_int64()
+    reps = np.zeros(base.opts.n_reps)
+    lib = L.lib()
+    if dist:
+        lib.dbgz_problem_set_cdf_form(base.handle, L.CDF_ERFC)
+    try:
+        st = lib.dbgz_pnorm(base.handle, prec, C.byref(res), C.byref(err), C.byref(npts), L.ptr(reps))
+    finally:
+        if dist:
+            lib.dbgz_problem_set_cdf_form(base.handle, int(base.cdf_form))
+    L.check(st, base.ctx.handle)
+    out = (res.value, err.value, int(npts.value))
+    return out + (reps,) if return_reps else out
+
+
+# ---- primitives -------------------------------------------------------------
+def cholesky_genz(M, a, b, block_size=2**7, block_size2=2**9, block_size3=2**10,
+                  block_size4=2**11, *, device=0) -> CholeskyGenz:
+    """cholesky_genz!(copy(M), copy(a), copy(b), ...) on the GPU (src/cholesky.jl:445)."""
+    ctx = get_context(device)
+    Mf = np.array(M, dtype=np.float64, order="F", copy=True)
+    n = Mf.shape[0]
+    a, b = _f64(a).copy(), _f64(b).copy()
+    perm = np.zeros(n, dtype=np.int64)
+    sv = np.zeros(n)
+    rank = C.c_int64()
+    L.check(L.lib().dbgz_cholesky_genz(ctx.handle, n, L.ptr(Mf), L.ptr(a), L.ptr(b), block_size,
+                                       block_size2, block_size3, block_size4,
+                                       L.ptr(perm, C.c_int64), L.ptr(sv), C.byref(rank)), ctx.handle)
+    return CholeskyGenz(Mf, perm, rank.value, a, b, block_size, "genz", sv)
+
+
+def cholesky_classic(M, a, b, block_size=2**7, block_size2=2**9, block_size3=2**10,
+                     block_size4=2**11, *, device=0) -> CholeskyGenz:
+    """cholesky_classic!(copy(M), copy(a), copy(b), ...) on the GPU (src/cholesky.jl:144)."""
+    ctx = get_context(device)
+    Mf = np.array(M, dtype=np.float64, order="F", copy=True)
+    n = Mf.shape[0]
+    a, b = _f64(a).copy(), _f64(b).copy()
+    sv = np.zeros(n)
+    L.check(L.lib().dbgz_cholesky_classic(ctx.handle, n, L.ptr(Mf), L.ptr(a), L.ptr(b), block_size,
+                                          block_size2, block_size3, block_size4, L.ptr(sv)),
+            ctx.handle)
+    return CholeskyGenz(Mf, np.arange(n), n, a, b, block_size, "none", sv)
+
+
+def get_sqrt_primes(n: int) -> np.ndarray:
+    q = np.zeros(n)
+    L.check(L.lib().dbgz_sqrt_primes(n, L.ptr(q)))
+    return q
+
+
+def richtmyer_mat(m: int, q, n0: int = 0, *, device=0) -> np.ndarray:
+    ctx = get_context(device)
+    q = _f64(q)
+    X = np.zeros((m, q.size), order="F")
+    L.check(L.lib().dbgz_richtmyer_mat(ctx.handle, m, q.size, L.ptr(q), n0, L.ptr(X)), ctx.handle)
+    return X
+
+
+def sobol_dirnums(dims: int) -> np.ndarray:
+    V = np.zeros((dims, 32), dtype=np.uint32)
+    L.check(L.lib().dbgz_sobol_dirnums(dims, L.ptr(V, C.c_uint32)))
+    return V
+
+
+def sobol_mat(m: int, V, first: int, *, device=0) -> np.ndarray:
+    ctx = get_context(device)
+    V = np.ascontiguousarray(V, dtype=np.uint32)
+    X = np.zeros((m, V.shape[0]), dtype=np.uint32, order="F")
+    L.check(L.lib().dbgz_sobol_mat(ctx.handle, m, V.shape[0], L.ptr(V, C.c_uint32), first,
+                                   L.ptr(X, C.c_uint32)), ctx.handle)
+    return X

@@ -1,0 +1,498 @@
+// chol.cu -- FP64 blocked Cholesky factorisations on the GPU.
+//
+//  * cholesky_genz!  (reference src/cholesky.jl:445-628): Genz variable
+//    reordering inside every bs2 panel, panel-restricted argmin pivoting,
+//    s_vec carried only inside the current panel.
+//  * cholesky_classic! (src/cholesky.jl:144-242): no pivoting.
+//
+// Arithmetic contract: every sum the reference hands to BLAS (mul!, ldiv!,
+// dot) is evaluated here as ONE fused-multiply-add chain in ascending index
+// order, and every other operation is a single IEEE operation with
+// contraction disabled (dm_* in detmath.h).  The CPU checker follows the
+// same contract, so U, the pivot permutation and the permuted bounds agree
+// bit for bit.  Parallelism comes from computing independent chains
+// concurrently (one chain per output element), never from splitting a
+// chain.
+//
+// Layout: M is d x d column-major in HBM (8 MB at d = 1000, L2 resident);
+// a sequential pivot step runs in one CTA (latency-bound: scores, argmin,
+// swaps, row update), the trailing Schur updates and triangular solves run
+// on the whole GPU.
+#include "internal.cuh"
+#include "detmath.h"
+#include <cfloat>
+
+namespace {
+
+constexpr int kStepThreads = 1024;
+
+__device__ __forceinline__ bool julia_min_less(double x, double y) {
+  // Base.isgreater order used by findmin/argmin: NaN lowest, -0.0 < +0.0.
+  if (x != x) return y == y;
+  if (y != y) return false;
+  if (x < y) return true;
+  if (x == y && x == 0.0) return signbit(x) && !signbit(y);
+  return false;
+}
+
+__device__ __forceinline__ void argmin_combine(double &v, int64_t &i, double v2, int64_t i2) {
+  if (julia_min_less(v2, v) || (!julia_min_less(v, v2) && i2 < i)) {
+    v = v2;
+    i = i2;
+  }
+}
+
+__global__ void k_diag_absmax(const double *M, int64_t n, double *out) {
+  __shared__ double sh[32];
+  double mx = 0.0;
+  bool nan = false;
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+    double v = fabs(M[j * n + j]);
+    if (v != v) nan = true;
+    else if (v > mx) mx = v;
+  }
+  nan = __syncthreads_or(nan);
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, sh[w]);
+    out[0] = nan ? NAN : dm_mul(DBL_EPSILON, r);
+  }
+}
+
+__global__ void k_scale_vec(const double *M, int64_t n, double *scale) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double v = M[j * n + j];
+  scale[j] = v > 0 ? dm_sqrt(v) : 1.0;
+}
+
+// src/cholesky.jl:458-473 (genz, mirror = 1) / :154-166 (classic, mirror = 0)
+__global__ void k_scale_apply(double *M, int64_t n, double *a, double *b, const double *scale,
+                              int mirror) {
+  int64_t j = blockIdx.y;
+  double s_j = scale[j];
+  double inv_s_j = dm_div(1.0, s_j);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= j;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == j) {
+      M[j * n + j] = 1.0;
+      a[j] = dm_mul(a[j], inv_s_j);
+      b[j] = dm_mul(b[j], inv_s_j);
+    } else {
+      double val = dm_mul(M[j * n + i], dm_div(inv_s_j, scale[i]));
+      M[j * n + i] = val;
+      if (mirror) M[i * n + j] = val;
+    }
+  }
+}
+
+// One bs1 block [i0, i1] of cholesky_genz! inside the bs2 panel ending at
+// ii1 (0-based, inclusive), src/cholesky.jl:494-572.  One CTA.
+__global__ void __launch_bounds__(kStepThreads)
+k_genz_block(double *M, int64_t n, double *a, double *b, double *dvec, double *svec,
+             double *ovec, int64_t *perm, int64_t i0, int64_t i1, int64_t ii1,
+             const double *eps0_ptr, int64_t *rank) {
+  __shared__ double red_v[kStepThreads / 32];
+  __shared__ int64_t red_i[kStepThreads / 32];
+  __shared__ int64_t sh_im;
+  __shared__ double sh_mii, sh_yi;
+  __shared__ int sh_stop;
+  const double c2 = dm_div(1.0, dm_sqrt(2.0));
+  const double is2pi = dm_div(2.0, dm_sqrt(dm_mul(2.0, M_PI)));
+  const double eps0 = eps0_ptr[0];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (rank[0] < n) return;  // an earlier block already stopped
+  for (int64_t k = i0 + tid; k <= ii1; k += blockDim.x) dvec[k] = 0.0;
+  __syncthreads();
+  for (int64_t i = i0; i <= i1; ++i) {
+    // pivot scores :500-512, then argmin :514
+    double bv = 0.0;
+    int64_t bi = INT64_MAX;
+    for (int64_t k = i + tid; k <= ii1; k += blockDim.x) {
+      double m_kk = dm_sub(M[k * n + k], dvec[k]);
+      m_kk = m_kk < 0 ? 0.0 : dm_sqrt(m_kk);
+      double a_k = dm_mul(dm_div(dm_sub(a[k], svec[k]), m_kk), c2);
+      double b_k = dm_mul(dm_div(dm_sub(b[k], svec[k]), m_kk), c2);
+      double o = dm_sub(det_erf(b_k), det_erf(a_k));
+      ovec[k] = o;
+      if (bi == INT64_MAX) { bv = o; bi = k; }
+      else argmin_combine(bv, bi, o, k);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
+      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
+      if (lane + off < 32 && i2 != INT64_MAX) {
+        if (bi == INT64_MAX) { bv = v2; bi = i2; }
+        else argmin_combine(bv, bi, v2, i2);
+      }
+    }
+    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double v = red_v[0];
+      int64_t im = red_i[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        if (red_i[w] == INT64_MAX) continue;
+        if (im == INT64_MAX) { v = red_v[w]; im = red_i[w]; }
+        else argmin_combine(v, im, red_v[w], red_i[w]);
+      }
+      double d_ii = ovec[im];
+      double m_ii = dm_sub(M[im * n + im], dvec[im]);
+      if (im != i) {  // :518-523
+        int64_t tp = perm[i]; perm[i] = perm[im]; perm[im] = tp;
+        double t;
+        t = dvec[im]; dvec[im] = dvec[i]; dvec[i] = t;
+        t = svec[im]; svec[im] = svec[i]; svec[i] = t;
+        t = a[im]; a[im] = a[i]; a[i] = t;
+        t = b[im]; b[im] = b[i]; b[i] = t;
+      }
+      sh_im = im;
+      sh_mii = m_ii;
+      sh_yi = d_ii;  // carried to the y_i step
+    }
+    __syncthreads();
+    const int64_t im = sh_im;
+    if (im != i) {  // :525-530: rows over columns i0..n, then full columns
+      for (int64_t k = i0 + tid; k < n; k += blockDim.x) {
+        double t = M[k * n + i];
+        M[k * n + i] = M[k * n + im];
+        M[k * n + im] = t;
+      }
+      __syncthreads();
+      for (int64_t k = tid; k < n; k += blockDim.x) {
+        double t = M[i * n + k];
+        M[i * n + k] = M[im * n + k];
+        M[im * n + k] = t;
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      double m_ii = sh_mii;
+      double d_ii = sh_yi;
+      int stop = 0;
+      if (m_ii > eps0) {
+        m_ii = dm_sqrt(m_ii);
+      } else {
+        rank[0] = i;  // 0-based i == reference's i - 1
+        stop = 1;
+      }
+      if (!stop) {
+        M[i * n + i] = m_ii;
+        double a_norm = dm_div(dm_sub(a[i], svec[i]), m_ii);
+        double b_norm = dm_div(dm_sub(b[i], svec[i]), m_ii);
+        double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
+        double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
+        sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), d_ii);
+        sh_mii = m_ii;
+      }
+      sh_stop = stop;
+    }
+    __syncthreads();
+    if (sh_stop) return;
+    const double m_ii = sh_mii, y_i = sh_yi;
+    if (i == i0) {  // :547-554
+      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
+        double m_ij = dm_div(M[j * n + i], m_ii);
+        M[j * n + i] = m_ij;
+        M[i * n + j] = m_ij;
+        dvec[j] = dm_add(dvec[j], dm_mul(m_ij, m_ij));
+        svec[j] = dm_add(svec[j], dm_mul(y_i, m_ij));
+      }
+    } else if (i < ii1) {  // :555-570
+      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
+        double acc = 0.0;
+        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[l * n + j], M[i * n + l], acc);
+        double m_ij = dm_div(dm_sub(M[i * n + j], acc), m_ii);
+        M[j * n + i] = m_ij;
+        M[i * n + j] = m_ij;
+        dvec[j] = dm_add(dvec[j], dm_mul(m_ij, m_ij));
+        svec[j] = dm_add(svec[j], dm_mul(y_i, m_ij));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// C[j,k] -= sum_{l=p0..p1} A(l,j) * B(l,k) for j,k in [c0, c1], one
+// ascending fma chain per element.  A(l,j) = M[j,l] (row form, the
+// reference's lower-triangle copy) when a_row, else M[l,j]; B(l,k) = M[l,k].
+constexpr int kTile = 32;
+__global__ void __launch_bounds__(256)
+k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, int a_row) {
+  __shared__ double As[kTile][kTile + 1];
+  __shared__ double Bs[kTile][kTile + 1];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  const int64_t j0 = c0 + blockIdx.x * (int64_t)kTile, k0 = c0 + blockIdx.y * (int64_t)kTile;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t l0 = p0; l0 <= p1; l0 += kTile) {
+    for (int r = ty; r < kTile; r += 8) {
+      // As[l][c] = A(l0 + l, j0 + c); Bs[l][c] = B(l0 + l, k0 + c)
+      int64_t l = l0 + tx, jj = j0 + r, kk = k0 + r;
+      if (a_row) {
+        int64_t lr = l0 + r, jc = j0 + tx;  // coalesced over j
+        As[r][tx] = (lr <= p1 && jc <= c1) ? M[lr * n + jc] : 0.0;
+      } else {
+        As[tx][r] = (l <= p1 && jj <= c1) ? M[jj * n + l] : 0.0;
+      }
+      Bs[tx][r] = (l <= p1 && kk <= c1) ? M[kk * n + l] : 0.0;
+    }
+    __syncthreads();
+    const int lmax = (int)((p1 - l0 + 1) < kTile ? (p1 - l0 + 1) : kTile);
+    for (int l = 0; l < lmax; ++l) {
+      double av = As[l][tx];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[r] = dm_fma(av, Bs[l][ty + 8 * r], acc[r]);
+    }
+    __syncthreads();
+  }
+  const int64_t j = j0 + tx;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    int64_t k = k0 + ty + 8 * r;
+    if (j <= c1 && k <= c1) M[k * n + j] = dm_sub(M[k * n + j], acc[r]);
+  }
+}
+
+// ldiv!(UpperTriangular(M[p0:p1,p0:p1])', M[p0:p1, c0:c1]): forward
+// substitution, one column per thread, ascending fma chains.
+__global__ void k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1) {
+  int64_t c = c0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c > c1) return;
+  double *X = M + c * n;
+  for (int64_t r = p0; r <= p1; ++r) {
+    const double *Ur = M + r * n;
+    double acc = 0.0;
+    for (int64_t l = p0; l < r; ++l) acc = dm_fma(Ur[l], X[l], acc);
+    X[r] = dm_div(dm_sub(X[r], acc), Ur[r]);
+  }
+}
+
+// One bs1 block of cholesky_classic! (src/cholesky.jl:180-198), one CTA.
+__global__ void __launch_bounds__(kStepThreads)
+k_classic_block(double *M, int64_t n, int64_t i0, int64_t i1) {
+  for (int64_t i = i0; i <= i1; ++i) {
+    __shared__ double sh_mii;
+    if (threadIdx.x == 0) {
+      double m_ii = M[i * n + i];
+      if (i > i0) {
+        double acc = 0.0;
+        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[i * n + l], M[i * n + l], acc);
+        m_ii = dm_sub(m_ii, acc);
+      }
+      m_ii = dm_sqrt(m_ii);
+      M[i * n + i] = m_ii;
+      sh_mii = m_ii;
+    }
+    __syncthreads();
+    const double m_ii = sh_mii;
+    for (int64_t j = i + 1 + threadIdx.x; j <= i1; j += blockDim.x) {
+      if (i > i0 && i < i1) {
+        double acc = 0.0;
+        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[j * n + l], M[i * n + l], acc);
+        M[j * n + i] = dm_sub(M[j * n + i], acc);
+        M[i * n + j] = 0.0;
+      }
+      M[j * n + i] = dm_div(M[j * n + i], m_ii);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_truncate(double *U, int64_t nn, double min_val) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn;
+       t += (int64_t)gridDim.x * blockDim.x)
+    if (fabs(U[t]) < min_val) U[t] = 0.0;
+}
+
+__global__ void k_targets(const double *U, int64_t n, const double *a, const double *b,
+                          TargetParams64 *t64, TargetParams32 *t32) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double c2 = sqrt(2.0);
+  double inv_u = 1.0 / (U[t * n + t] * c2);
+  t64[t] = TargetParams64{a[t], b[t], inv_u};
+  t32[t] = TargetParams32{(float)a[t], (float)b[t], (float)inv_u, 0.f};
+}
+
+__global__ void k_to_f32(const double *src, float *dst, int64_t nn) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn;
+       t += (int64_t)gridDim.x * blockDim.x)
+    dst[t] = (float)src[t];
+}
+
+int launch_schur(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0,
+                 int64_t c1, int a_row) {
+  if (c1 < c0 || p1 < p0) return DBGZ_OK;
+  int64_t nt = (c1 - c0 + kTile) / kTile;
+  dim3 grid((unsigned)nt, (unsigned)nt);
+  k_schur_update<<<grid, 256, 0, ctx->stream>>>(M, n, p0, p1, c0, c1, a_row);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+int launch_trsm(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0,
+                int64_t c1) {
+  if (c1 < c0) return DBGZ_OK;
+  int64_t nc = c1 - c0 + 1;
+  k_trsm_ut<<<(unsigned)((nc + 63) / 64), 64, 0, ctx->stream>>>(M, n, p0, p1, c0, c1);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+int scale_correlation(dbgz_ctx *ctx, double *M, int64_t n, double *a, double *b, double *scale,
+                      int mirror) {
+  k_scale_vec<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(M, n, scale);
+  dbgz_count_launch(ctx);
+  dim3 grid((unsigned)((n + 255) / 256), (unsigned)n);
+  k_scale_apply<<<grid, 256, 0, ctx->stream>>>(M, n, a, b, scale, mirror);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+}  // namespace
+
+int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b, int64_t bs1,
+                       int64_t bs2, int64_t bs3, int64_t bs4, int64_t *perm, double *scale,
+                       int64_t *rank_host) {
+  if (bs1 < 1 || bs2 < 1 || bs3 < 1 || bs4 < 1)
+    return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "block sizes must be positive");
+  DevBuf work;
+  DBGZ_TRY(dbgz_ensure(ctx, work, sizeof(double) * (3 * n + 2) + sizeof(int64_t) * 2));
+  double *dvec = (double *)work.p, *svec = dvec + n, *ovec = svec + n, *eps0 = ovec + n;
+  int64_t *rank = (int64_t *)(eps0 + 2);
+  cudaStream_t st = ctx->stream;
+  cudaMemsetAsync(dvec, 0, sizeof(double) * 3 * n, st);
+  k_diag_absmax<<<1, 1024, 0, st>>>(M, n, eps0);
+  dbgz_count_launch(ctx);
+  int st_ = scale_correlation(ctx, M, n, a, b, scale, 1);
+  if (st_) { dbgz_release(work); return st_; }
+  {
+    std::vector<int64_t> id(n);
+    for (int64_t i = 0; i < n; ++i) id[i] = i;
+    cudaMemcpyAsync(perm, id.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+    int64_t rn = n;
+    cudaMemcpyAsync(rank, &rn, sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+  }
+  int rc = DBGZ_OK;
+  for (int64_t iv0 = 0; iv0 < n && rc == DBGZ_OK; iv0 += bs4) {
+    int64_t iv1 = std::min(n - 1, iv0 + bs4 - 1);
+    for (int64_t iii0 = iv0; iii0 <= iv1 && rc == DBGZ_OK; iii0 += bs3) {
+      int64_t iii1 = std::min(iv1, iii0 + bs3 - 1);
+      for (int64_t ii0 = iii0; ii0 <= iii1 && rc == DBGZ_OK; ii0 += bs2) {
+        int64_t ii1 = std::min(iii1, ii0 + bs2 - 1);
+        for (int64_t i0 = ii0; i0 <= ii1 && rc == DBGZ_OK; i0 += bs1) {
+          int64_t i1 = std::min(ii1, i0 + bs1 - 1);
+          k_genz_block<<<1, kStepThreads, 0, st>>>(M, n, a, b, dvec, svec, ovec, perm, i0, i1,
+                                                    ii1, eps0, rank);
+          dbgz_count_launch(ctx);
+          if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1);
+        }
+        if (ii1 < iii1 && rc == DBGZ_OK) {
+          rc = launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1);
+          if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0);
+        }
+      }
+      if (iii1 < iv1 && rc == DBGZ_OK) {
+        rc = launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1);
+        if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0);
+      }
+    }
+    if (iv1 < n - 1 && rc == DBGZ_OK) {
+      rc = launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1);
+      if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0);
+    }
+  }
+  // Blocks after a rank failure return immediately (they read rank < n),
+  // and the Schur updates after it only touch entries the reference leaves
+  // as scratch beyond the failure point; callers reject rank < n anyway.
+  if (rc == DBGZ_OK) {
+    cudaError_t e = cudaMemcpyAsync(rank_host, rank, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "cholesky_genz: %s", cudaGetErrorString(e));
+  }
+  cudaStreamSynchronize(st);
+  dbgz_release(work);
+  return rc;
+}
+
+int dbgz_chol_classic_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b,
+                          int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4, double *scale) {
+  if (bs1 < 1 || bs2 < 1 || bs3 < 1 || bs4 < 1)
+    return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "block sizes must be positive");
+  cudaStream_t st = ctx->stream;
+  DBGZ_TRY(scale_correlation(ctx, M, n, a, b, scale, 0));
+  for (int64_t iv0 = 0; iv0 < n; iv0 += bs4) {
+    int64_t iv1 = std::min(n - 1, iv0 + bs4 - 1);
+    for (int64_t iii0 = iv0; iii0 <= iv1; iii0 += bs3) {
+      int64_t iii1 = std::min(iv1, iii0 + bs3 - 1);
+      for (int64_t ii0 = iii0; ii0 <= iii1; ii0 += bs2) {
+        int64_t ii1 = std::min(iii1, ii0 + bs2 - 1);
+        for (int64_t i0 = ii0; i0 <= ii1; i0 += bs1) {
+          int64_t i1 = std::min(ii1, i0 + bs1 - 1);
+          k_classic_block<<<1, kStepThreads, 0, st>>>(M, n, i0, i1);
+          dbgz_count_launch(ctx);
+          if (i1 < ii1) {
+            DBGZ_TRY(launch_trsm(ctx, M, n, i0, i1, i1 + 1, ii1));
+            DBGZ_TRY(launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 0));
+          }
+        }
+        if (ii1 < iii1) {
+          DBGZ_TRY(launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1));
+          DBGZ_TRY(launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0));
+        }
+      }
+      if (iii1 < iv1) {
+        DBGZ_TRY(launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1));
+        DBGZ_TRY(launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0));
+      }
+    }
+    if (iv1 < n - 1) {
+      DBGZ_TRY(launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1));
+      DBGZ_TRY(launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0));
+    }
+  }
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return DBGZ_OK;
+}
+
+int dbgz_truncate_dev(dbgz_ctx *ctx, int64_t n, double *U, double eps_T) {
+  double min_val = eps_T / (double)(n * 9);
+  int64_t nn = n * n;
+  int blocks = (int)std::min<int64_t>((nn + 255) / 256, 4096);
+  k_truncate<<<blocks, 256, 0, ctx->stream>>>(U, nn, min_val);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+int dbgz_make_targets(dbgz_problem *p) {
+  dbgz_ctx *ctx = p->ctx;
+  int64_t n = p->d;
+  DBGZ_TRY(dbgz_ensure(ctx, p->tgt64, sizeof(TargetParams64) * n));
+  DBGZ_TRY(dbgz_ensure(ctx, p->tgt32, sizeof(TargetParams32) * n));
+  k_targets<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+      (const double *)p->U.p, n, (const double *)p->a.p, (const double *)p->b.p,
+      (TargetParams64 *)p->tgt64.p, (TargetParams32 *)p->tgt32.p);
+  dbgz_count_launch(p->ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+int dbgz_make_U32(dbgz_problem *p) {
+  dbgz_ctx *ctx = p->ctx;
+  int64_t nn = p->d * p->d;
+  DBGZ_TRY(dbgz_ensure(ctx, p->U32, sizeof(float) * nn));
+  int blocks = (int)std::min<int64_t>((nn + 255) / 256, 4096);
+  k_to_f32<<<blocks, 256, 0, ctx->stream>>>((const double *)p->U.p, (float *)p->U32.p, nn);
+  dbgz_count_launch(p->ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}

@@ -1,0 +1,173 @@
+// genz_step.cuh -- the per-sample, per-dimension step of the Genz
+// sequential conditioning loop, shared by the SIMT and tensor-core loops.
+//
+// For one sample (point j of shift k) and one y-index l (QMC dimension l,
+// conditioning variable l, target variable l+1) the reference does
+// (src/qmc_generators.jl:137-204, src/qmc.jl:384-429):
+//
+//   u   = point(j, l) shifted (Richtmyer: + shift mod 1; Sobol: XOR shift)
+//   w   = |2u - 1|                           (tent / baker transform)
+//   u   = clamp(c + w dc, eps, 1 - eps)
+//   y_l = sqrt(2) erfinv(2u - 1)             (= Phi^-1(u))
+//   s   = sum_{i<=l} y_i U[i, l+1]           (the conditioning contraction)
+//   c   = Phi((a_{l+1} - s)/U_{l+1,l+1}),  dc = Phi((b_{l+1} - s)/U) - c
+//   p  *= dc
+//
+// Two numerics are provided:
+//  * StepFp64: the reference's Float64 arithmetic (erf form or erfc form of
+//    the CDF, the clamp to [-9, 9] in erf units, the same fma pattern).
+//  * StepFp32: FP32 special functions written to stay within ~1e-7
+//    relative of the FP64 result where the reference's Float32 loop loses
+//    digits: the state keeps both tails -- lo = Phi(alpha), up = Phi(-beta)
+//    -- and dc, so that u (when u <= 1/2) and 1 - u (otherwise) are formed
+//    without cancellation and Phi^-1 is taken of the smaller one; dc is the
+//    difference of two tails of the same side only when the interval lies
+//    in one tail, and then in FP64 (erfc) if the FP32 difference would
+//    cancel.  The weight product p stays FP64 (no underflow at d = 1000).
+//    u is clamped to [eps64, 1 - eps64] like the Float64 reference.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cfloat>
+
+namespace dbgz {
+
+constexpr double kSqrt2 = 1.4142135623730951;
+
+struct GenParams {
+  int qmc_type;          // 0 Richtmyer, 1 Sobol
+  int n_bits;
+  int64_t gen_base;      // Richtmyer: n_base; Sobol: pass offset
+  int64_t sobol_first;
+  const double *q;       // Richtmyer generators (d-1)
+  const double *shift64; // (d-1) x n_reps
+  const float *shift32;  // (d-1) x n_reps
+  const uint32_t *V;     // Sobol direction numbers (d-1) x 32
+  const uint64_t *ushift;// (d-1) x n_reps
+};
+
+// Gray-code Sobol integer of point index idx in dimension l.
+__device__ __forceinline__ uint32_t sobol_int(const uint32_t *Vl, uint64_t idx) {
+  uint32_t g = (uint32_t)(idx ^ (idx >> 1));
+  uint32_t x = 0;
+  while (g) {
+    int k = __ffs(g) - 1;
+    x ^= __ldg(Vl + k);
+    g &= g - 1;
+  }
+  return x;
+}
+
+// ---------------------------------------------------------------- FP64 ---
+struct StepFp64 {
+  double c, dc;
+  double p;
+  __device__ __forceinline__ void init(double c1, double dc1, double /*up1*/) {
+    c = c1;
+    dc = dc1;
+    p = dc1;
+  }
+  // Returns y_l for QMC dimension l of sample (point index j in the pass,
+  // 0-based; shift k).
+  __device__ __forceinline__ double quantile(const GenParams &g, int64_t d, int64_t j, int64_t k,
+                                             int64_t l, double qv, double shiftv) const {
+    double u;
+    if (g.qmc_type == 0) {
+      double x = __dmul_rn((double)(g.gen_base + j + 1), qv);
+      x = x - floor(x);
+      u = shiftv + x;
+      u = u > 1.0 ? u - 1.0 : u;
+    } else {
+      const int L = g.n_bits;
+      const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
+      uint64_t xi = (uint64_t)sobol_int(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
+      uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
+      u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
+    }
+    u = fabs(fma(u, 2.0, -1.0));
+    u = fma(u, dc, c);
+    u = fmin(fmax(u, DBL_EPSILON), 1.0 - DBL_EPSILON);
+    double v = fma(2.0, u, -1.0);
+    return kSqrt2 * erfinv(v);
+  }
+  __device__ __forceinline__ void cdf(double s, double a, double b, double inv_u, int erfc_form) {
+    double cv = (a - s) * inv_u;
+    double dv = (b - s) * inv_u;
+    cv = fmax(fmin(cv, 9.0), -9.0);
+    dv = fmax(fmin(dv, 9.0), -9.0);
+    if (!erfc_form) {
+      cv = 0.5 * (1.0 + erf(cv));
+      dv = 0.5 * (1.0 + erf(dv)) - cv;
+    } else {
+      double c_val = 0.5 * erfc(-cv);
+      dv = 0.5 * erfc(-dv) - c_val;
+      cv = c_val;
+    }
+    c = cv;
+    dc = dv;
+    p *= dv;
+  }
+};
+
+// ---------------------------------------------------------------- FP32 ---
+struct StepFp32 {
+  float lo, up, dc;  // Phi(alpha), Phi(-beta), Phi(beta) - Phi(alpha)
+  double p;
+  __device__ __forceinline__ void init(double c1, double dc1, double up1) {
+    lo = (float)c1;
+    dc = (float)dc1;
+    up = (float)up1;
+    p = dc1;
+  }
+  __device__ __forceinline__ float quantile(const GenParams &g, int64_t d, int64_t j, int64_t k,
+                                            int64_t l, double qv, float shiftv) const {
+    float w, w1;
+    if (g.qmc_type == 0) {
+      double x = __dmul_rn((double)(g.gen_base + j + 1), qv);
+      x = x - floor(x);
+      float u = shiftv + (float)x;
+      u = u > 1.0f ? u - 1.0f : u;
+      w = fabsf(fmaf(u, 2.0f, -1.0f));
+      w1 = 2.0f * fminf(u, 1.0f - u);  // 1 - |2u - 1|
+    } else {
+      const int L = g.n_bits;
+      const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
+      uint64_t xi = (uint64_t)sobol_int(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
+      uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
+      double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
+      w = (float)fabs(fma(u, 2.0, -1.0));
+      w1 = (float)(2.0 * fmin(u, 1.0 - u));
+    }
+    const float kEps = (float)DBL_EPSILON;
+    float t = fmaf(w, dc, lo);
+    if (t <= 0.5f) return normcdfinvf(fmaxf(t, kEps));
+    float qq = fmaf(w1, dc, up);
+    return -normcdfinvf(fmaxf(qq, kEps));
+  }
+  __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
+    float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
+    float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
+    float ea = 0.5f * erfcf(fabsf(xa));  // mass beyond |alpha| on its side
+    float eb = 0.5f * erfcf(fabsf(xb));
+    float d;
+    if (xa >= 0.0f) {                   // both bounds in the upper tail
+      d = ea - eb;
+      if (eb > 0.5f * ea) d = (float)(0.5 * (erfc((double)xa) - erfc((double)xb)));
+      lo = 1.0f - ea;
+      up = eb;
+    } else if (xb <= 0.0f) {            // both bounds in the lower tail
+      d = eb - ea;
+      if (ea > 0.5f * eb) d = (float)(0.5 * (erfc(-(double)xb) - erfc(-(double)xa)));
+      lo = ea;
+      up = 1.0f - eb;
+    } else {                            // alpha < 0 < beta
+      d = (1.0f - ea) - eb;
+      lo = ea;
+      up = eb;
+    }
+    dc = d;
+    p *= (double)d;
+  }
+};
+
+}  // namespace dbgz

@@ -1,0 +1,113 @@
+// internal.cuh -- shared declarations of libdbgenz (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstdarg>
+#include <string>
+#include <vector>
+
+#include "../../include/dbgenz.h"
+
+#define DBGZ_CUDA_TRY(ctx, call)                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return dbgz_fail((ctx), DBGZ_ERR_CUDA, "%s failed: %s (%s:%d)", #call,        \
+                       cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+  } while (0)
+
+#define DBGZ_TRY(call)                \
+  do {                                \
+    int s_ = (call);                  \
+    if (s_ != DBGZ_OK) return s_;     \
+  } while (0)
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct dbgz_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int *d_status = nullptr;  // device-side error word written by bounded waits
+  bool profiling = false;
+  cudaEvent_t ev[6] = {};   // 0/1: call bracket, 2/3: loop launch, 4/5: finalize
+  dbgz_profile prof{};
+  int64_t launch_count = 0; // kernels launched by the library on this context
+};
+
+// Counts a kernel launch of the library (for dbgz_profile).
+inline void dbgz_count_launch(dbgz_ctx *ctx, int n = 1) { ctx->launch_count += n; }
+
+int dbgz_fail(dbgz_ctx *ctx, int status, const char *fmt, ...);
+int dbgz_ensure(dbgz_ctx *ctx, DevBuf &b, size_t bytes);
+void dbgz_release(DevBuf &b);
+
+// Parameters of one target dimension t (variable t, 0-based) of the loop:
+// the lower/upper bound and 1/(U[t,t] sqrt 2).
+struct TargetParams64 {
+  double a, b, inv_u;
+};
+struct TargetParams32 {
+  float a, b, inv_u, pad;
+};
+
+struct dbgz_problem {
+  dbgz_ctx *ctx = nullptr;
+  int64_t d = 0;
+  dbgz_opts opts{};
+  int qmc_type = 0, structure = 0, cdf_form = 0;
+  int64_t rank = 0;
+  // factorisation (device, FP64)
+  DevBuf U, a, b, perm, scale;
+  // generator (device)
+  DevBuf q, shifts, shifts32, V, ushifts;
+  int64_t sobol_first = 0;
+  int64_t gen_base = 0;  // offset of the current point block (next_points! state)
+  // derived operands (device, built on first use)
+  DevBuf tgt64, tgt32, U32;
+  DevBuf Uhi, Ulo, Utf;  // tensor-core operands of the contraction
+  int64_t ldU = 0;       // padded leading dimension of Uhi/Ulo/Utf
+  // workspaces
+  DevBuf yws, partials, reps;
+  double c1 = 0, dc1 = 0;
+  bool c1_ready = false;
+};
+
+// ---- factorisation (chol.cu) -------------------------------------------
+int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b, int64_t bs1,
+                       int64_t bs2, int64_t bs3, int64_t bs4, int64_t *perm, double *scale,
+                       int64_t *rank_host);
+int dbgz_chol_classic_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b,
+                          int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4, double *scale);
+int dbgz_truncate_dev(dbgz_ctx *ctx, int64_t n, double *U, double eps_T);
+int dbgz_make_targets(dbgz_problem *p);
+int dbgz_make_U32(dbgz_problem *p);
+
+// ---- points (points.cu) --------------------------------------------------
+int dbgz_richtmyer_dev(dbgz_ctx *ctx, int64_t m, int64_t n, const double *q, int64_t n0,
+                       double *X);
+int dbgz_sobol_dev(dbgz_ctx *ctx, int64_t m, int64_t dims, const uint32_t *V, int64_t first,
+                   uint32_t *X);
+
+// ---- integration loop (loop_simt.cu) ---------------------------------------
+struct PassArgs {
+  int64_t d;
+  int64_t m;          // points per pass
+  int64_t n_reps;
+  int64_t gen_base;   // Richtmyer: n_base; Sobol: offset added to sobol_first
+  int64_t sobol_first;
+  int n_bits;
+  int qmc_type;
+  int cdf_form;
+  double c1, dc1;
+};
+int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
+                   int64_t n_tiles);
+int dbgz_finalize_pass(dbgz_problem *p, const double *partials, int64_t tiles_per_shift,
+                       int64_t n_pts0, int64_t m, double *reps);

@@ -1,0 +1,205 @@
+/*
+ * dbgenz.h -- C ABI of the B200 Genz QMC multivariate-normal probability
+ * library (libdbgenz.so).
+ *
+ * This is the drop-in boundary for the reference's qmc_pnorm! path
+ * (JakobPeterlin/DBGenzPaper, Julia).  Every entry point names the
+ * reference function it replaces (file:line in that repository).  A Julia
+ * caller binds these with ccall; any C caller can use
+ * them directly.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Matrices are column-major (Julia
+ *     layout) with leading dimension equal to the row count.
+ *   - Host pointers unless the name says _dev.  Every call is synchronous
+ *     on the context's own CUDA stream unless it says otherwise.
+ *   - Indices are 0-based (perm[i] is the 0-based original variable).
+ *   - Every function returns a dbgz_status; nothing throws or aborts across
+ *     the ABI.  dbgz_last_error() gives a one-line message for the last
+ *     failing call on a context.
+ *   - One context per host thread (the reference's QMCData is not reentrant
+ *     either, src/qmc.jl:335).  Contexts are independent.
+ *   - There is no CPU fallback: without a usable CUDA device dbgz_create
+ *     fails with DBGZ_ERR_CUDA.
+ */
+#ifndef DBGENZ_H
+#define DBGENZ_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DBGZ_ABI_VERSION 1
+
+typedef enum dbgz_status {
+  DBGZ_OK = 0,
+  DBGZ_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad enum, bad size */
+  DBGZ_ERR_RANK_DEFICIENT = 2,   /* src/qmc.jl:195-197 ArgumentError */
+  DBGZ_ERR_NONFINITE_INPUT = 3,  /* NaN in Sigma, NaN bounds, a > b */
+  DBGZ_ERR_DIMENSION = 4,        /* d < 2, or beyond a kernel's limit */
+  DBGZ_ERR_OUT_OF_MEMORY = 5,
+  DBGZ_ERR_CUDA = 6,             /* CUDA runtime error or no device */
+  DBGZ_ERR_TIMEOUT = 7,          /* a bounded device-side wait gave up */
+  DBGZ_ERR_UNSUPPORTED = 8       /* mode not available for this problem */
+} dbgz_status;
+
+typedef enum dbgz_qmc_type {
+  DBGZ_QMC_RICHTMYER = 0, /* RichtmyerQMC, src/qmc_generators.jl:8-13,47-54 */
+  DBGZ_QMC_SOBOL = 1      /* SobolQMC,     src/qmc_generators.jl:16-26,57-65 */
+} dbgz_qmc_type;
+
+typedef enum dbgz_structure {
+  DBGZ_STRUCTURE_DENSE = 0,  /* QMCData:       cholesky_genz!, dense loop  */
+  DBGZ_STRUCTURE_SPARSE = 1  /* QMCDataSparse: cholesky_classic!, CSC loop */
+} dbgz_structure;
+
+typedef enum dbgz_cdf_form {
+  DBGZ_CDF_ERF = 0,  /* QMCData: c = (1 + erf(x))/2            src/qmc.jl:405-429 */
+  DBGZ_CDF_ERFC = 1  /* QMCData_Distributions: c = erfc(-x)/2  src/qmc.jl:579-593 */
+} dbgz_cdf_form;
+
+typedef enum dbgz_precision {
+  /* Double precision everywhere: the reference's Float64 arithmetic. */
+  DBGZ_PREC_FP64 = 0,
+  /* FP32 special functions and weights (FP64 tail, FP64 weight product
+   * and reductions); the conditioning contraction on tcgen05 tensor cores
+   * with TF32 operands accumulated in FP32. */
+  DBGZ_PREC_FP32_TF32 = 1,
+  /* As above with the contraction as three BF16 products (hi*hi + hi*lo +
+   * lo*hi of the split operands) accumulated in FP32. */
+  DBGZ_PREC_FP32_SPLIT_BF16 = 2,
+  /* FP32 numerics of the two modes above with the contraction on CUDA
+   * cores (no tensor cores); an ablation of the tensor-core choice. */
+  DBGZ_PREC_FP32_SIMT = 3
+} dbgz_precision;
+
+/* Mirrors QMCOpts (src/qmc.jl:15-27).  Block sizes that only steer CPU
+ * threading (block_size_j, n_blocks) are accepted and ignored; the GPU
+ * tiles are chosen by the library. */
+typedef struct dbgz_opts {
+  int64_t chol_block_size;   /* bs1 of cholesky_genz!/classic! (64)   */
+  int64_t chol_block_size2;  /* bs2 (512)                             */
+  int64_t m;                 /* QMC points per pass (10^4)            */
+  int64_t block_size_i;      /* accepted, unused on the GPU (64)      */
+  int64_t block_size_i2;     /* accepted, unused on the GPU (32)      */
+  int64_t block_size_j;      /* accepted, unused on the GPU (64)      */
+  int64_t n_blocks;          /* accepted, unused on the GPU           */
+  int64_t n_reps;            /* random shifts (12)                    */
+  int64_t n_bits;            /* Sobol integer grid bits, 1..32 (32)   */
+  int64_t max_pts;           /* adaptive stop: points per shift (10^4)*/
+  double max_abs_err;        /* adaptive stop: 3*SEM target (1e-6)    */
+} dbgz_opts;
+
+typedef struct dbgz_ctx dbgz_ctx;
+typedef struct dbgz_problem dbgz_problem;
+
+/* Fills the defaults of QMC_opts(T) (src/qmc.jl:111-125). */
+void dbgz_default_opts(dbgz_opts *opts);
+const char *dbgz_status_string(int status);
+int dbgz_abi_version(void);
+
+/* Context: one CUDA device, one stream, reusable workspaces. */
+int dbgz_create(int device, dbgz_ctx **out);
+int dbgz_destroy(dbgz_ctx *ctx);
+const char *dbgz_last_error(const dbgz_ctx *ctx);
+
+/* Device-side timing of the library's own work, measured with CUDA events
+ * recorded on the context's stream (the stream every kernel is launched
+ * on).  Off by default; costs two event records per launch when on. */
+typedef struct dbgz_profile {
+  double pnorm_ms;          /* last dbgz_pnorm*: first launch to last copy  */
+  double loop_ms;           /* its integration-loop launches, summed        */
+  double finalize_ms;       /* its per-shift reduction launches, summed     */
+  int64_t loop_launches;    /* integration-loop kernels it launched         */
+  int64_t kernel_launches;  /* every kernel it launched                     */
+  double prepare_ms;        /* last dbgz_prepare: upload + factorisation    */
+  int64_t prepare_launches; /* kernels the last dbgz_prepare launched       */
+} dbgz_profile;
+int dbgz_set_profiling(dbgz_ctx *ctx, int enable);
+int dbgz_get_profile(const dbgz_ctx *ctx, dbgz_profile *out);
+
+/* ---- the qmc_pnorm! path ------------------------------------------- */
+
+/* Constructor of QMCData / QMCDataSparse (src/qmc.jl:149-202, :225-282):
+ * copies Sigma (d x d), a, b (length d) to the device, runs the pivoted
+ * (dense) or classic (sparse) blocked Cholesky there in FP64, checks the
+ * rank (DBGZ_ERR_RANK_DEFICIENT, as the reference's ArgumentError),
+ * truncates |U_ij| < eps/(9d) (src/qmc.jl:133-142) and stores the point
+ * generator:
+ *   Richtmyer: shifts is (d-1) x n_reps doubles in [0,1), the values the
+ *              reference draws with rand(rng, T, n-1, n_reps)
+ *              (src/qmc_generators.jl:52); ushifts, sobol_* unused.
+ *   Sobol:     ushifts is (d-1) x n_reps uint64 digital shifts
+ *              (src/qmc_generators.jl:63); sobol_dirnums is (d-1) x 32
+ *              direction numbers v_k of each dimension as 32-bit integers
+ *              (row per dimension), or NULL for the library's own table
+ *              (dbgz_sobol_dirnums); sobol_first is the index of the first
+ *              point of the first pass (skip0 + 1 when the caller skipped
+ *              skip0 points as SobolQMC does with skip0 = 2m-1).
+ * The problem keeps its own generator position: like the reference's
+ * QMCData, a second dbgz_pnorm on the same problem continues from the
+ * points the previous call ended on (src/qmc.jl:836). */
+int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
+                 const double *b, const dbgz_opts *opts, int qmc_type, int structure,
+                 int cdf_form, const double *shifts, const uint64_t *ushifts,
+                 const uint32_t *sobol_dirnums, int64_t sobol_first,
+                 dbgz_problem **out);
+int dbgz_problem_free(dbgz_problem *p);
+
+/* Selects the CDF form used by later dbgz_pnorm calls on p.  The
+ * reference's QMCData_Distributions(D) (src/qmc.jl:210-215) wraps the same
+ * factorisation and generator state as D with the erfc form; a caller
+ * switches the form of one problem instead of copying it. */
+int dbgz_problem_set_cdf_form(dbgz_problem *p, int cdf_form);
+
+/* Reads back the factorisation held by a prepared problem: U (d x d,
+ * upper triangle meaningful, as CholeskyGenz.U), perm, permuted and scaled
+ * a and b, scale_vec, rank (src/cholesky.jl:5-14).  Any pointer may be
+ * NULL. */
+int dbgz_problem_factor(const dbgz_problem *p, double *U, int64_t *perm, double *a,
+                        double *b, double *scale_vec, int64_t *rank);
+
+/* qmc_pnorm!(D) (src/qmc.jl:783-850): runs passes of m points x n_reps
+ * shifts until n_pts >= max_pts or 3*SEM < max_abs_err and returns the
+ * mean over shifts, 3*SEM and the number of points per shift.  qmc_reps
+ * (length n_reps, may be NULL) receives the per-shift running means. */
+int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err,
+               int64_t *n_pts, double *qmc_reps);
+
+/* ---- primitives of the path (device compute, host buffers) ---------- */
+
+/* cholesky_genz!(M, a, b, bs1, bs2, bs3, bs4) (src/cholesky.jl:445-628):
+ * in place on M (d x d), a, b.  perm (d), scale_vec (d) and rank are
+ * outputs.  Pivot choices are made with the library's deterministic FP64
+ * erf/exp, so the permutation is reproducible bit for bit. */
+int dbgz_cholesky_genz(dbgz_ctx *ctx, int64_t d, double *M, double *a, double *b,
+                       int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
+                       int64_t *perm, double *scale_vec, int64_t *rank);
+/* cholesky_classic!(M, a, b, bs1..bs4) (src/cholesky.jl:144-242). */
+int dbgz_cholesky_classic(dbgz_ctx *ctx, int64_t d, double *M, double *a, double *b,
+                          int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
+                          double *scale_vec);
+/* get_sqrt_primes!(q) (src/qmc_generators.jl:300-310), host only. */
+int dbgz_sqrt_primes(int64_t n, double *q);
+/* richtmyer_mat!(X, q, n0) (src/qmc_generators.jl:314-325): X is m x n
+ * doubles, X[i,j] = frac((n0 + i + 1) q_j) computed in FP64. */
+int dbgz_richtmyer_mat(dbgz_ctx *ctx, int64_t m, int64_t n, const double *q, int64_t n0,
+                       double *X);
+/* sobol_mat! + copyt_as_UInt64! (src/qmc_generators.jl:331-352) on the
+ * 32-bit grid: X is m x dims uint32, X[j,i] = floor(x_{first+j,i} 2^32)
+ * of the Gray-code Sobol sequence with direction numbers V (dims x 32). */
+int dbgz_sobol_mat(dbgz_ctx *ctx, int64_t m, int64_t dims, const uint32_t *V,
+                   int64_t first, uint32_t *X);
+/* The library's own direction numbers (host only): dimension 0 is the
+ * van der Corput sequence; dimension i >= 1 uses the i-th primitive
+ * polynomial over GF(2) (ordered by degree, then value) with odd initial
+ * values m_k < 2^k drawn from a fixed-seed generator (Bratley-Fox
+ * construction).  V is dims x 32, V[i*32 + k] = m_{k+1} << (31 - k). */
+int dbgz_sobol_dirnums(int64_t dims, uint32_t *V);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DBGENZ_H */

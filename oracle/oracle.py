@@ -1,0 +1,196 @@
+"""ctypes front end of the CPU checker (test infrastructure only).
+
+Loads ``oracle/libgenz_oracle.so`` (built by ``oracle/Makefile``) and exposes
+the restated reference functions with numpy arrays.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline legs of ``bench.py`` import
+this module; the product package never does.
+
+All matrices are column-major (Julia layout): a numpy array ``A`` of shape
+(n, n) is passed as ``np.asfortranarray(A)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libgenz_oracle.so")
+_lib = None
+
+RICHTMYER, SOBOL = 0, 1
+CDF_ERF, CDF_ERFC = 0, 1
+
+
+class OrcOpts(C.Structure):
+    _fields_ = [
+        ("chol_block_size", C.c_int64),
+        ("chol_block_size2", C.c_int64),
+        ("m", C.c_int64),
+        ("block_size_i", C.c_int64),
+        ("block_size_i2", C.c_int64),
+        ("block_size_j", C.c_int64),
+        ("n_reps", C.c_int64),
+        ("n_bits", C.c_int64),
+        ("max_pts", C.c_int64),
+        ("max_abs_err", C.c_double),
+    ]
+
+
+class OrcProblem(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("U", C.POINTER(C.c_double)),
+        ("a", C.POINTER(C.c_double)),
+        ("b", C.POINTER(C.c_double)),
+        ("qmc_type", C.c_int),
+        ("q", C.POINTER(C.c_double)),
+        ("shifts", C.POINTER(C.c_double)),
+        ("V", C.POINTER(C.c_uint32)),
+        ("sobol_first", C.c_int64),
+        ("ushifts", C.POINTER(C.c_uint64)),
+        ("cdf_form", C.c_int),
+        ("sparse", C.c_int),
+        ("gen_base0", C.c_int64),
+    ]
+
+
+def build() -> str:
+    """Compile the checker with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        d, i64, pd, pi64 = C.c_double, C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_int64)
+        L.orc_det_erf.restype = d
+        L.orc_det_erf.argtypes = [d]
+        L.orc_det_exp.restype = d
+        L.orc_det_exp.argtypes = [d]
+        L.orc_erfinv.restype = d
+        L.orc_erfinv.argtypes = [d]
+        L.orc_cholesky_genz.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pi64, pd, pi64]
+        L.orc_cholesky_classic.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pd]
+        L.orc_truncate_U.argtypes = [i64, pd, d]
+        L.orc_sqrt_primes.argtypes = [i64, pd]
+        L.orc_richtmyer_mat.argtypes = [i64, i64, pd, i64, pd]
+        L.orc_sobol_points.argtypes = [i64, C.POINTER(C.c_uint32), i64, i64, C.POINTER(C.c_uint32)]
+        L.orc_qmc_pnorm.argtypes = [C.POINTER(OrcProblem), C.POINTER(OrcOpts), C.c_int, pd, pd, pi64, pd]
+        _lib = L
+    return _lib
+
+
+def _pd(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def det_erf(x: float) -> float:
+    return lib().orc_det_erf(float(x))
+
+
+def det_exp(x: float) -> float:
+    return lib().orc_det_exp(float(x))
+
+
+def erfinv(x: float) -> float:
+    return lib().orc_erfinv(float(x))
+
+
+def cholesky_genz(Sigma, a, b, bs1=64, bs2=512, bs3=1024, bs4=2048):
+    """cholesky_genz!(copy(Σ), copy(a), copy(b), bs1, bs2) -> dict (src/cholesky.jl:445)."""
+    n = Sigma.shape[0]
+    M = np.array(Sigma, dtype=np.float64, order="F", copy=True)
+    a = np.array(a, dtype=np.float64, copy=True)
+    b = np.array(b, dtype=np.float64, copy=True)
+    perm = np.zeros(n, dtype=np.int64)
+    scale = np.zeros(n, dtype=np.float64)
+    rank = C.c_int64(0)
+    lib().orc_cholesky_genz(n, _pd(M), _pd(a), _pd(b), bs1, bs2, bs3, bs4,
+                            perm.ctypes.data_as(C.POINTER(C.c_int64)), _pd(scale), C.byref(rank))
+    return dict(U=M, perm=perm, rank=rank.value, a=a, b=b, scale_vec=scale)
+
+
+def cholesky_classic(Sigma, a, b, bs1=128, bs2=512, bs3=1024, bs4=2048):
+    n = Sigma.shape[0]
+    M = np.array(Sigma, dtype=np.float64, order="F", copy=True)
+    a = np.array(a, dtype=np.float64, copy=True)
+    b = np.array(b, dtype=np.float64, copy=True)
+    scale = np.zeros(n, dtype=np.float64)
+    lib().orc_cholesky_classic(n, _pd(M), _pd(a), _pd(b), bs1, bs2, bs3, bs4, _pd(scale))
+    return dict(U=M, perm=np.arange(n), rank=n, a=a, b=b, scale_vec=scale)
+
+
+def truncate_U(U, eps_T=np.finfo(np.float64).eps):
+    U = np.array(U, dtype=np.float64, order="F", copy=True)
+    lib().orc_truncate_U(U.shape[0], _pd(U), float(eps_T))
+    return U
+
+
+def sqrt_primes(n):
+    q = np.zeros(n, dtype=np.float64)
+    lib().orc_sqrt_primes(n, _pd(q))
+    return q
+
+
+def richtmyer_mat(m, q, n0=0):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    X = np.zeros((m, q.size), dtype=np.float64, order="F")
+    lib().orc_richtmyer_mat(m, q.size, _pd(q), n0, _pd(X))
+    return X
+
+
+def sobol_points(V, first, m):
+    V = np.ascontiguousarray(V, dtype=np.uint32)
+    dims = V.shape[0]
+    X = np.zeros((m, dims), dtype=np.uint32, order="F")
+    lib().orc_sobol_points(dims, V.ctypes.data_as(C.POINTER(C.c_uint32)), first, m,
+                           X.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return X
+
+
+def qmc_pnorm(U, a, b, *, m, n_reps, qmc_type=RICHTMYER, shifts=None, q=None, V=None,
+              sobol_first=0, ushifts=None, cdf_form=CDF_ERF, sparse=False,
+              block_size_i=64, block_size_i2=32, block_size_j=64, n_bits=32,
+              max_pts=None, max_abs_err=1e-6, threads=0, gen_base0=0):
+    """qmc_pnorm! on a prepared problem (U, permuted/scaled a, b) -> (P, err, n_pts, reps)."""
+    n = U.shape[0]
+    U = np.asfortranarray(U, dtype=np.float64)
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    keep = [U, a, b]
+    P = OrcProblem()
+    P.n = n
+    P.U, P.a, P.b = _pd(U), _pd(a), _pd(b)
+    P.qmc_type = qmc_type
+    P.cdf_form = cdf_form
+    P.sparse = 1 if sparse else 0
+    P.gen_base0 = int(gen_base0)
+    if qmc_type == RICHTMYER:
+        q = sqrt_primes(n - 1) if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        sh = np.asfortranarray(shifts, dtype=np.float64)
+        assert sh.shape == (n - 1, n_reps)
+        keep += [q, sh]
+        P.q, P.shifts = _pd(q), _pd(sh)
+    else:
+        Vv = np.ascontiguousarray(V, dtype=np.uint32)
+        us = np.asfortranarray(ushifts, dtype=np.uint64)
+        assert us.shape == (n - 1, n_reps) and Vv.shape == (n - 1, 32)
+        keep += [Vv, us]
+        P.V = Vv.ctypes.data_as(C.POINTER(C.c_uint32))
+        P.ushifts = us.ctypes.data_as(C.POINTER(C.c_uint64))
+        P.sobol_first = sobol_first
+    o = OrcOpts(64, 512, m, block_size_i, block_size_i2, block_size_j, n_reps, n_bits,
+                m if max_pts is None else max_pts, max_abs_err)
+    res, err, npts = C.c_double(0), C.c_double(0), C.c_int64(0)
+    reps = np.zeros(n_reps, dtype=np.float64)
+    lib().orc_qmc_pnorm(C.byref(P), C.byref(o), threads, C.byref(res), C.byref(err),
+                        C.byref(npts), _pd(reps))
+    del keep
+    return res.value, err.value, npts.value, reps

@@ -1,0 +1,252 @@
+"""CUDA path against the CPU checker and the golden fixtures (needs a B200).
+
+Bars: bit-exact for the factorisation (U, pivot permutation, permuted
+bounds) and the point sets; FP64 probabilities within 1e-12 relative of the
+checker (the two use different erf/erfinv implementations and summation
+orders); FP32 modes within the tolerances written in each test."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from dbgenzpaper_b200 import workloads as W
+from dbgenzpaper_b200 import _lib as L
+from oracle import kat
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def D(dbgz):
+    dbgz.get_context(0)
+    return dbgz
+
+
+def _spd(n, seed, jitter=1.0):
+    return W.rand_spd(n, jitter, np.random.default_rng(seed))
+
+
+# ---------------------------------------------------------------- factor ---
+@pytest.mark.parametrize("n,bs1,bs2,seed", [(7, 64, 512, 1), (64, 64, 512, 2), (130, 16, 64, 3),
+                                            (600, 64, 512, 4), (300, 8, 32, 5)])
+def test_cholesky_genz_bitexact(D, oracle, n, bs1, bs2, seed):
+    S = _spd(n, seed)
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-3, 0, n)
+    b = rng.uniform(0, 3, n)
+    a[::5] = -np.inf
+    G = D.cholesky_genz(S, a, b, bs1, bs2)
+    F = oracle.cholesky_genz(S, a, b, bs1, bs2)
+    assert G.rank == F["rank"] == n
+    assert np.array_equal(G.perm, F["perm"])
+    assert np.array_equal(G.U, F["U"])  # whole matrix, lower-triangle scratch included
+    assert np.array_equal(G.a, F["a"]) and np.array_equal(G.b, F["b"])
+    assert np.array_equal(G.scale_vec, F["scale_vec"])
+
+
+def test_cholesky_genz_reference_case(D, oracle):
+    # test/runtests.jl:15-36 at n = 1024 (three bs2 panels with bs2 = 512? no: 2)
+    rng = np.random.default_rng(101)
+    n = 1024
+    A = rng.random((n, n))
+    Cm = A @ A.T + 100.0 * np.eye(n)
+    G = D.cholesky_genz(Cm, -np.ones(n), np.ones(n), 64, 512)
+    F = oracle.cholesky_genz(Cm, -np.ones(n), np.ones(n), 64, 512)
+    assert np.array_equal(G.perm, F["perm"]) and np.array_equal(G.U, F["U"])
+    d = np.sqrt(np.diag(Cm))
+    Ct = Cm / np.outer(d, d)
+    U = np.triu(G.U)
+    assert np.max(np.abs(Ct[np.ix_(G.perm, G.perm)] - U.T @ U)) < 1e-10
+
+
+def test_cholesky_genz_ties_pick_first_index(D, oracle):
+    # equicorrelated Sigma with equal bounds: every score ties exactly
+    n = 40
+    S = W.fixed_dense(n)
+    lo, up = W.bounds_quarter(S)
+    G = D.cholesky_genz(S, lo, up, 8, 16)
+    F = oracle.cholesky_genz(S, lo, up, 8, 16)
+    assert np.array_equal(G.perm, F["perm"]) and np.array_equal(G.U, F["U"])
+
+
+def test_cholesky_genz_rank_deficient(D, oracle):
+    rng = np.random.default_rng(9)
+    B = rng.standard_normal((20, 5))
+    S = B @ B.T
+    G = D.cholesky_genz(S, -np.ones(20), np.ones(20), 8, 16)
+    F = oracle.cholesky_genz(S, -np.ones(20), np.ones(20), 8, 16)
+    assert G.rank == F["rank"] < 20
+    k = G.rank
+    assert np.array_equal(G.perm, F["perm"])
+    assert np.array_equal(np.triu(G.U)[:k, :k], np.triu(F["U"])[:k, :k])
+
+
+@pytest.mark.parametrize("n,bs", [(100, 8), (100, 16), (100, 32), (100, 64), (300, 128)])
+def test_cholesky_classic_bitexact(D, oracle, n, bs):
+    # test/runtests.jl:38-59
+    rng = np.random.default_rng(102)
+    A = rng.random((n, n))
+    Cm = A @ A.T + 100.0 * np.eye(n)
+    G = D.cholesky_classic(Cm, -np.ones(n), np.ones(n), bs, bs, bs, bs)
+    F = oracle.cholesky_classic(Cm, -np.ones(n), np.ones(n), bs, bs, bs, bs)
+    assert np.array_equal(np.triu(G.U), np.triu(F["U"]))
+    d = np.sqrt(np.diag(Cm))
+    U = np.triu(G.U)
+    assert np.max(np.abs(Cm / np.outer(d, d) - U.T @ U)) < 1e-10
+
+
+# ---------------------------------------------------------------- points ---
+@pytest.mark.parametrize("n0", [0, 10_000, 2**20])
+def test_richtmyer_bitexact(D, oracle, n0):
+    q = D.get_sqrt_primes(50)
+    assert np.array_equal(D.richtmyer_mat(1000, q, n0), oracle.richtmyer_mat(1000, q, n0))
+
+
+@pytest.mark.parametrize("first", [0, 2048, 12345])
+def test_sobol_bitexact(D, oracle, first):
+    V = D.sobol_dirnums(20)
+    assert np.array_equal(D.sobol_mat(4096, V, first), oracle.sobol_points(V, first, 4096))
+
+
+# ------------------------------------------------------------- integrate ---
+def _case(z, c):
+    return {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(c + "/")}
+
+
+def _from_case(D, g, T=np.float64, precision=None):
+    opts = D.QMC_opts(T, m=int(g["m"]), n_reps=int(g["n_reps"]), max_pts=int(g["max_pts"]),
+                      max_abs_err=0.0, chol_block_size=int(g["bs1"]), chol_block_size2=int(g["bs2"]))
+    kw = dict(precision=precision, cdf_form=int(g["cdf_form"]))
+    if int(g["qmc_type"]) == 0:
+        kw.update(qmc_type="Richtmyer", shifts=g["shifts"])
+    else:
+        kw.update(qmc_type="Sobol", ushifts=g["ushifts"], sobol_dirnums=g["V"],
+                  sobol_first=int(g["sobol_first"]))
+    cls = D.QMCDataSparse if int(g["sparse"]) else D.QMCData
+    return cls(g["Sigma"], g["a_in"], g["b_in"], opts, **kw)
+
+
+DENSE_CASES = ["c1", "spd8", "sobol40", "erfc130"]
+
+
+@pytest.mark.parametrize("c", DENSE_CASES)
+def test_pnorm_fp64_matches_fixture(D, c):
+    z = np.load(os.path.join(GOLD, "oracle_cases.npz"))
+    g = _case(z, c)
+    Q = _from_case(D, g)
+    F = Q.C
+    assert np.array_equal(F.perm, g["perm"]) and np.array_equal(np.triu(F.U), np.triu(g["U"]))
+    P, err, npts, reps = D.qmc_pnorm(Q, return_reps=True)
+    assert npts == int(g["n_pts"])
+    np.testing.assert_allclose(reps, g["reps"], rtol=1e-12, atol=1e-300)
+    assert abs(P - float(g["P"])) <= 1e-12 * abs(float(g["P"]))
+    assert abs(err - float(g["err"])) <= 1e-9 * abs(float(g["err"])) + 1e-15
+
+
+@pytest.mark.parametrize("c", DENSE_CASES)
+def test_pnorm_fp32_simt_close_to_fp64(D, c):
+    # FP32 numerics (FP64 weight product): |P - P64| <= 2e-6 + 1e-5 |P|
+    z = np.load(os.path.join(GOLD, "oracle_cases.npz"))
+    g = _case(z, c)
+    Q = _from_case(D, g, np.float32, precision=L.PREC_FP32_SIMT)
+    P, err, npts, reps = D.qmc_pnorm(Q, return_reps=True)
+    P64 = float(g["P"])
+    assert abs(P - P64) <= 2e-6 + 1e-5 * abs(P64), (P, P64)
+    np.testing.assert_allclose(reps, g["reps"], rtol=1e-4, atol=2e-6)
+
+
+def test_pnorm_fp64_multi_group_vs_checker(D, oracle):
+    # d = 300 crosses several 64-wide groups; m not a multiple of the tile
+    n = 300
+    S = _spd(n, 300)
+    lo, up = W.bounds_quarter(S)
+    sh = np.random.default_rng(300).random((n - 1, 4))
+    opts = D.QMC_opts(m=700, n_reps=4, max_pts=1400, max_abs_err=0.0)
+    Q = D.QMCData(S, lo, up, opts, shifts=sh)
+    P, err, npts, reps = D.qmc_pnorm(Q, return_reps=True)
+    F = Q.C
+    Pc, ec, nc, rc = oracle.qmc_pnorm(F.U, F.a, F.b, m=700, n_reps=4, shifts=sh, max_pts=1400,
+                                      max_abs_err=0.0)
+    assert npts == nc == 1400
+    np.testing.assert_allclose(reps, rc, rtol=1e-12)
+
+
+def test_second_call_continues_sequence(D, oracle):
+    # qmc_pnorm! twice on the same QMCData: the generator state persists
+    n = 20
+    S = _spd(n, 20)
+    lo, up = W.bounds_quarter(S)
+    sh = np.random.default_rng(20).random((n - 1, 3))
+    opts = D.QMC_opts(m=256, n_reps=3, max_pts=512, max_abs_err=0.0)
+    Q = D.QMCData(S, lo, up, opts, shifts=sh)
+    D.qmc_pnorm(Q)
+    P2, _, n2, r2 = D.qmc_pnorm(Q, return_reps=True)
+    F = Q.C
+    _, _, _, rc = oracle.qmc_pnorm(F.U, F.a, F.b, m=256, n_reps=3, shifts=sh, max_pts=512,
+                                   max_abs_err=0.0, gen_base0=256)
+    assert n2 == 512
+    np.testing.assert_allclose(r2, rc, rtol=1e-12)
+
+
+def test_distributions_variant_gpu(D, oracle):
+    S = _spd(30, 31)
+    lo, up = W.bounds_quarter(S)
+    sh = np.random.default_rng(31).random((29, 6))
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=500, n_reps=6, max_pts=500), shifts=sh)
+    P1 = D.qmc_pnorm(Q)[0]
+    Qd = D.QMCData_Distributions(Q)
+    P2, _, _, r2 = D.qmc_pnorm(Qd, return_reps=True)
+    F = Q.C
+    _, _, _, rc = oracle.qmc_pnorm(F.U, F.a, F.b, m=500, n_reps=6, shifts=sh, cdf_form=1,
+                                   gen_base0=0)
+    np.testing.assert_allclose(r2, rc, rtol=1e-12)
+    assert abs(P1 - P2) < 1e-12
+
+
+def test_identity_known_answer_gpu(D):
+    n = 20
+    lo, up = W.bounds_quarter(np.eye(n))
+    for prec, tol in ((L.PREC_FP64, 1e-14), (L.PREC_FP32_SIMT, 1e-6)):
+        Q = D.QMCData(np.eye(n), lo, up, D.QMC_opts(m=512, n_reps=4), rng=np.random.default_rng(1),
+                      precision=prec)
+        P, err, _ = D.qmc_pnorm(Q)
+        assert abs(P - 0.25) < tol
+
+
+def test_equicorrelated_known_answer_gpu(D):
+    n = 256
+    S = W.fixed_dense(n)
+    lo, up = W.bounds_quarter(S)
+    ref = kat.equicorrelated(1.0, 1.0, lo, up)
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=4096, n_reps=12, max_pts=4096),
+                  rng=np.random.default_rng(256))
+    P, err, _ = D.qmc_pnorm(Q)
+    assert abs(P - ref) < max(3 * err, 1e-3)
+
+
+# ---------------------------------------------------------------- errors ---
+def test_error_statuses(D):
+    n = 6
+    lo, up = -np.ones(n), np.ones(n)
+    opts = D.QMC_opts(m=64, n_reps=2)
+    B = np.random.default_rng(1).standard_normal((n, 2))
+    with pytest.raises(D.DbgzError) as e:
+        D.QMCData(B @ B.T, lo, up, opts)
+    assert e.value.status == L.ERR_RANK_DEFICIENT
+    S = np.eye(n)
+    S[1, 2] = np.nan
+    with pytest.raises(D.DbgzError) as e:
+        D.QMCData(S, lo, up, opts)
+    assert e.value.status == L.ERR_NONFINITE_INPUT
+    with pytest.raises(D.DbgzError) as e:
+        D.QMCData(np.eye(n), up, lo, opts)
+    assert e.value.status == L.ERR_NONFINITE_INPUT
+    with pytest.raises(D.DbgzError) as e:
+        D.QMCData(np.eye(1), [-1.0], [1.0], opts)
+    assert e.value.status == L.ERR_DIMENSION
+    Q = D.QMCData(np.eye(n), lo, up, opts)
+    with pytest.raises(D.DbgzError) as e:
+        D.qmc_pnorm(Q, precision=17)
+    assert e.value.status == L.ERR_INVALID_ARGUMENT

@@ -1,0 +1,211 @@
+"""The CPU checker pinned against the reference's own assertions, its known
+answers and its published values (no GPU).  Each test cites the reference
+test or data it restates."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+from scipy.special import erfinv as sp_erfinv
+
+from dbgenzpaper_b200 import workloads as W
+from oracle import kat
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_det_erf_exp_accuracy(oracle):
+    for x in np.linspace(-7, 7, 1401):
+        r = math.erf(x)
+        v = oracle.det_erf(x)
+        assert abs(v - r) <= 5 * math.ulp(r if r != 0 else 1e-300) or v == r
+    for x in np.linspace(-700, 700, 1401):
+        r = math.exp(x)
+        assert abs(oracle.det_exp(x) - r) <= math.ulp(r)
+    assert oracle.det_erf(float("inf")) == 1.0 and oracle.det_erf(-float("inf")) == -1.0
+    assert math.isnan(oracle.det_erf(float("nan")))
+    assert oracle.det_exp(-float("inf")) == 0.0
+
+
+def test_erfinv_accuracy(oracle):
+    for u in np.concatenate([np.linspace(-0.999999, 0.999999, 801), [1 - 2e-16, -1 + 2e-16, 1e-300]]):
+        r = sp_erfinv(u)
+        assert abs(oracle.erfinv(u) - r) <= 4e-16 * abs(r) + 1e-300
+
+
+def test_cholesky_genz_reconstruction(oracle):
+    # test/runtests.jl:15-36 (n = 1024, A ~ U(0,1), C = A A' + 100 I)
+    rng = np.random.default_rng(101)
+    n = 1024
+    A = rng.random((n, n))
+    C = A @ A.T + 100.0 * np.eye(n)
+    F = oracle.cholesky_genz(C, -np.ones(n), np.ones(n))
+    U = np.triu(F["U"])
+    p = F["perm"]
+    d = np.sqrt(np.diag(C))
+    Ct = C / np.outer(d, d)
+    assert F["rank"] == n
+    assert sorted(p) == list(range(n))
+    assert np.max(np.abs(Ct[np.ix_(p, p)] - U.T @ U)) < 1e-10
+
+
+def test_cholesky_genz_reorders_by_probability(oracle):
+    # with Sigma = I the Genz order is ascending marginal probability mass
+    n = 12
+    rng = np.random.default_rng(5)
+    b = rng.uniform(0.1, 3.0, n)
+    F = oracle.cholesky_genz(np.eye(n), -np.full(n, np.inf), b, 4, 6)
+    for p0 in (0, 6):  # panel-restricted pivoting (bs2 = 6)
+        panel = F["perm"][p0:p0 + 6]
+        assert list(panel) == list(np.sort(np.arange(p0, p0 + 6))[np.argsort(b[p0:p0 + 6], kind="stable")])
+
+
+@pytest.mark.parametrize("bs", [8, 16, 32, 64])
+def test_cholesky_classic_reconstruction(oracle, bs):
+    # test/runtests.jl:38-59
+    rng = np.random.default_rng(102)
+    n = 100
+    A = rng.random((n, n))
+    C = A @ A.T + 100.0 * np.eye(n)
+    d = np.sqrt(np.diag(C))
+    Ct = C / np.outer(d, d)
+    F = oracle.cholesky_classic(C, -np.ones(n), np.ones(n), bs, bs, bs, bs)
+    U = np.triu(F["U"])
+    assert np.max(np.abs(Ct - U.T @ U)) < 1e-10
+
+
+def test_richtmyer_properties(oracle):
+    # test/runtests.jl:91-113
+    n_dim, n_pts = 1024, 1024
+    q = oracle.sqrt_primes(n_dim)
+    assert q.dtype == np.float64 and np.all((0 < q) & (q < 1))
+    X = oracle.richtmyer_mat(n_pts, q, 0)
+    assert len(np.unique(X[:, -1].astype(np.float32))) == n_pts
+    X2 = oracle.richtmyer_mat(n_pts, q, n_pts)
+    assert len(np.unique(X2[:, -1].astype(np.float32))) == n_pts
+    X3 = oracle.richtmyer_mat(n_pts, q, 2**20)
+    assert len(np.unique(X3[:, -1].astype(np.float32))) == n_pts
+    # X[i, j] = frac((n0 + i) q_j) exactly
+    i = np.arange(1, n_pts + 1, dtype=np.float64)
+    assert np.array_equal(X[:, 3], i * q[3] - np.floor(i * q[3]))
+
+
+def test_sobol_net_property(oracle):
+    import ctypes as C
+    from dbgenzpaper_b200 import _lib as L
+    dims = 50
+    V = np.zeros((dims, 32), dtype=np.uint32)
+    L.check(L.lib().dbgz_sobol_dirnums(dims, V.ctypes.data_as(C.POINTER(C.c_uint32))))
+    k = 10
+    X = oracle.sobol_points(V, 3 * 2**k, 2**k)  # an aligned block of 2^k points
+    for j in range(dims):
+        assert len(np.unique(X[:, j] >> (32 - k))) == 2**k
+    # first points of the van der Corput dimension
+    X0 = oracle.sobol_points(V[:1], 1, 4)[:, 0] / 2.0**32
+    assert list(X0) == [0.5, 0.75, 0.25, 0.375]
+
+
+def _prep(oracle, S, a, b, bs=(64, 512), sparse=False):
+    F = (oracle.cholesky_classic if sparse else oracle.cholesky_genz)(S, a, b, *bs)
+    return oracle.truncate_U(F["U"]), F
+
+
+def test_identity_known_answer(oracle):
+    n = 16
+    lo, up = W.bounds_quarter(np.eye(n))
+    U, F = _prep(oracle, np.eye(n), lo, up)
+    sh = np.random.default_rng(1).random((n - 1, 12))
+    P, err, npts, reps = oracle.qmc_pnorm(U, F["a"], F["b"], m=256, n_reps=12, shifts=sh)
+    assert abs(P - 0.25) < 1e-14 and err < 1e-13 and npts == 256
+
+
+def test_dense_vs_independent_integrator(oracle):
+    # test/runtests.jl:150-173 (MvNormalCDF replaced by scipy's Genz-Bretz)
+    rng = np.random.default_rng(42)
+    n = 8
+    S = W.rand_spd(n, 4.0, rng)
+    a, b = np.full(n, -np.inf), np.full(n, 2.0)
+    U, F = _prep(oracle, S, a, b)
+    sh = rng.random((n - 1, 12))
+    P, err, npts, _ = oracle.qmc_pnorm(U, F["a"], F["b"], m=2**11, n_reps=12, shifts=sh,
+                                       block_size_i=256, block_size_i2=64, block_size_j=128,
+                                       max_pts=2**13, max_abs_err=0.0)
+    ref = kat.scipy_mvn(S, a, b)
+    assert np.isfinite(P) and np.isfinite(err) and npts == 2**13
+    assert abs(P - ref) < 0.06           # the reference test's tolerance
+    assert abs(P - ref) < 3 * err + 1e-6  # and the QMC error bound
+
+
+def test_sparse_vs_independent_integrator(oracle):
+    # test/runtests.jl:175-201 (tridiagonal 1.8 / 0.25, b = 1.5)
+    n = 8
+    S = np.diag(np.full(n, 1.8)) + np.diag(np.full(n - 1, 0.25), 1) + np.diag(np.full(n - 1, 0.25), -1)
+    a, b = np.full(n, -np.inf), np.full(n, 1.5)
+    U, F = _prep(oracle, S, a, b, sparse=True)
+    sh = np.random.default_rng(21).random((n - 1, 12))
+    P, err, npts, _ = oracle.qmc_pnorm(U, F["a"], F["b"], m=2**11, n_reps=12, shifts=sh,
+                                       sparse=True, max_pts=2**13, max_abs_err=0.0)
+    ref = kat.scipy_mvn(S, a, b)
+    assert abs(P - ref) < 0.06 and abs(P - ref) < 3 * err + 1e-6
+
+
+def test_equicorrelated_published_value(oracle):
+    # Sigma_2 = 1 1' + I at n = 256: closed form (mwp.jl:80-116) against the
+    # reference's published estimate (data/sims/table_sparse_dense1.tex:10)
+    pub = json.load(open(os.path.join(GOLD, "published.json")))
+    row = pub["rows"][0]
+    n = row["n"]
+    S = W.fixed_dense(n)
+    lo, up = W.bounds_quarter(S)
+    assert abs(row["closed_form"] - kat.equicorrelated(1.0, 1.0, lo, up)) < 1e-12
+    for r in pub["rows"]:
+        assert abs(r["value"] - r["closed_form"]) < 3 * r["sd"] + 1e-4
+    U, F = _prep(oracle, S, lo, up)
+    sh = np.random.default_rng(256).random((n - 1, 12))
+    P, err, _, _ = oracle.qmc_pnorm(U, F["a"], F["b"], m=1024, n_reps=12, shifts=sh)
+    assert abs(P - row["closed_form"]) < max(3 * err, 3 * row["sd"])
+
+
+def test_distributions_variant_agrees(oracle):
+    # erf form vs erfc form on the same points (simulation_precision.jl:94-123)
+    S = W.rand_spd(30, 1.0, np.random.default_rng(30))
+    lo, up = W.bounds_quarter(S)
+    U, F = _prep(oracle, S, lo, up)
+    sh = np.random.default_rng(3).random((29, 12))
+    P1 = oracle.qmc_pnorm(U, F["a"], F["b"], m=512, n_reps=12, shifts=sh, cdf_form=0)[0]
+    P2 = oracle.qmc_pnorm(U, F["a"], F["b"], m=512, n_reps=12, shifts=sh, cdf_form=1)[0]
+    assert abs(P1 - P2) < 1e-13
+
+
+def test_golden_fixtures_reproduce(oracle):
+    z = np.load(os.path.join(GOLD, "oracle_cases.npz"))
+    names = sorted({k.split("/")[0] for k in z.files})
+    assert {"c1", "spd8", "sobol40", "tridiag8", "erfc130"} <= set(names)
+    for c in names:
+        g = lambda k: z[f"{c}/{k}"]
+        sparse = bool(g("sparse"))
+        U, F = _prep(oracle, g("Sigma"), g("a_in"), g("b_in"), (int(g("bs1")), int(g("bs2"))), sparse)
+        assert np.array_equal(U, g("U"), equal_nan=True) and np.array_equal(F["perm"], g("perm"))
+        kw = dict(m=int(g("m")), n_reps=int(g("n_reps")), max_pts=int(g("max_pts")), max_abs_err=0.0,
+                  cdf_form=int(g("cdf_form")), sparse=sparse)
+        if int(g("qmc_type")) == 0:
+            kw["shifts"] = g("shifts")
+        else:
+            kw.update(qmc_type=1, V=g("V"), ushifts=g("ushifts"), sobol_first=int(g("sobol_first")))
+        P, err, npts, reps = oracle.qmc_pnorm(U, F["a"], F["b"], **kw)
+        assert np.array_equal(reps, g("reps")) and P == float(g("P")) and npts == int(g("n_pts"))
+
+
+def test_continuation_matches_longer_run(oracle):
+    # a pass that starts at generator offset m equals the second pass of a
+    # two-pass run (next_points!, src/qmc_generators.jl:119-122)
+    S = W.rand_spd(12, 2.0, np.random.default_rng(12))
+    lo, up = W.bounds_quarter(S)
+    U, F = _prep(oracle, S, lo, up)
+    sh = np.random.default_rng(4).random((11, 4))
+    _, _, _, r2 = oracle.qmc_pnorm(U, F["a"], F["b"], m=300, n_reps=4, shifts=sh, max_pts=600,
+                                   max_abs_err=0.0)
+    _, _, _, r1 = oracle.qmc_pnorm(U, F["a"], F["b"], m=300, n_reps=4, shifts=sh)
+    _, _, _, rb = oracle.qmc_pnorm(U, F["a"], F["b"], m=300, n_reps=4, shifts=sh, gen_base0=300)
+    assert np.allclose(r2, 0.5 * (r1 + rb), rtol=1e-14, atol=0)
