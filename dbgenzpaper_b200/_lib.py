@@ -88,6 +88,8 @@ SIGNATURES = {
     "dbgz_problem_set_cdf_form": (C.c_int, [_vp, C.c_int]),
     "dbgz_problem_factor": (C.c_int, [_vp, _pd, _pi64, _pd, _pd, _pd, _pi64]),
     "dbgz_pnorm": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
+    "dbgz_pnorm_pass_noalloc": (C.c_int, [C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int64,
+                                          C.c_int64, C.c_int64, _vp, _vp]),
     "dbgz_cholesky_genz": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,
                                      C.c_int64, C.c_int64, _pi64, _pd, _pi64]),
     "dbgz_cholesky_classic": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,

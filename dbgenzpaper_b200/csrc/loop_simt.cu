@@ -21,223 +21,12 @@
 //     sub-block 1 (128 x 32 x 32 GEMM from shared memory).
 //   * p is FP64; per-tile sums go to partials[tile] and a finalize kernel
 //     reduces them per shift in a fixed order (deterministic results).
-#include "internal.cuh"
-#include "genz_step.cuh"
+#include "loop_simt_kernels.cuh"
 #include <algorithm>
 
+using namespace simt;
+
 namespace {
-
-constexpr int TS = 128;   // samples per tile
-constexpr int G = 64;     // y-indices per group
-constexpr int SB = 32;    // y-indices per sequential sub-block
-constexpr int KC = 16;    // K chunk of the group GEMM
-constexpr int NT = 256;   // threads per CTA
-
-template <typename T>
-struct TgtOf;
-template <>
-struct TgtOf<double> {
-  using type = TargetParams64;
-};
-template <>
-struct TgtOf<float> {
-  using type = TargetParams32;
-};
-
-template <typename T>
-struct SimtParams {
-  int64_t d, m, n_reps, tiles_per_shift, n_tiles, Dp;
-  dbgz::GenParams gen;
-  const T *U;  // d x d col-major
-  const typename TgtOf<T>::type *tgt;
-  double c1, dc1, up1;
-  int cdf_form;
-  T *yws;            // gridDim.x slots of Dp x TS
-  double *partials;  // n_tiles
-};
-
-template <typename T>
-struct SimtSmem {
-  T Ss[G][TS];                // group partial sums, [target][sample]
-  union {
-    struct {
-      T Ys[KC][TS];
-      T Us[KC][G + 4];
-    } gemm;
-    T Ysub[SB][TS];           // y's of the last sub-block
-  } u;
-  T Ublk[SB][SB + 1];         // U of the sub-block (and of the cross block)
-  double qv[SB];
-  T shv[SB];
-  typename TgtOf<T>::type tg[SB];
-  double red[NT / 32];
-};
-
-template <typename T>
-__device__ __forceinline__ T shift_at(const dbgz::GenParams &g, int64_t idx);
-template <>
-__device__ __forceinline__ double shift_at<double>(const dbgz::GenParams &g, int64_t idx) {
-  return g.shift64 ? g.shift64[idx] : 0.0;
-}
-template <>
-__device__ __forceinline__ float shift_at<float>(const dbgz::GenParams &g, int64_t idx) {
-  return g.shift32 ? g.shift32[idx] : 0.0f;
-}
-
-template <typename T, typename Step>
-__global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SimtSmem<T> &sm = *reinterpret_cast<SimtSmem<T> *>(smem_raw);
-  const int tid = threadIdx.x;
-  const int64_t d = P.d, nY = d - 1;
-  T *Yw = P.yws + (int64_t)blockIdx.x * P.Dp * TS;
-  const int64_t last_g0 = ((nY - 1) / G) * G;  // start of the last group
-
-  for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
-    const int64_t k = tile / P.tiles_per_shift;
-    const int64_t jt = tile - k * P.tiles_per_shift;
-    const int r = tid;  // sample row for the scalar threads (tid < TS)
-    const int64_t j = jt * TS + r;
-    Step st;
-    st.init(P.c1, P.dc1, P.up1);
-
-    for (int64_t g0 = 0; g0 < nY; g0 += G) {
-      const int ng = (int)(nY - g0 < (int64_t)G ? nY - g0 : (int64_t)G);
-      // ---- group GEMM: Ss[t][r] = sum_{l<g0} Y[l][r] U[l][g0+1+t] ----
-      {
-        const int tx = tid & 15, ty = tid >> 4;
-        T acc[8][4];
-#pragma unroll
-        for (int a = 0; a < 8; ++a)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
-        for (int64_t l0 = 0; l0 < g0; l0 += KC) {
-#pragma unroll
-          for (int e = 0; e < KC * TS / NT; ++e) {
-            int idx = tid + e * NT;
-            int kk = idx / TS, rr = idx % TS;
-            sm.u.gemm.Ys[kk][rr] = Yw[(l0 + kk) * TS + rr];
-          }
-#pragma unroll
-          for (int e = 0; e < KC * G / NT; ++e) {
-            int idx = tid + e * NT;
-            int t = idx / KC, kk = idx % KC;
-            int64_t tgt = g0 + 1 + t;
-            sm.u.gemm.Us[kk][t] = tgt < d ? P.U[tgt * d + l0 + kk] : T(0);
-          }
-          __syncthreads();
-#pragma unroll
-          for (int kk = 0; kk < KC; ++kk) {
-            T av[8], bv[4];
-#pragma unroll
-            for (int a = 0; a < 8; ++a) av[a] = sm.u.gemm.Ys[kk][ty * 8 + a];
-#pragma unroll
-            for (int b = 0; b < 4; ++b) bv[b] = sm.u.gemm.Us[kk][tx * 4 + b];
-#pragma unroll
-            for (int a = 0; a < 8; ++a)
-#pragma unroll
-              for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
-          }
-          __syncthreads();
-        }
-#pragma unroll
-        for (int a = 0; a < 8; ++a)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) sm.Ss[tx * 4 + b][ty * 8 + a] = acc[a][b];
-        __syncthreads();
-      }
-      // ---- sequential sub-blocks ----
-      for (int sb = 0; sb < ng; sb += SB) {
-        const int nsb = min(SB, ng - sb);
-        const int64_t l_base = g0 + sb;
-        // stage U of the sub-block and the per-dimension parameters
-        for (int e = tid; e < SB * SB; e += NT) {
-          int li = e % SB, ti = e / SB;
-          int64_t l = l_base + li, t = l_base + ti + 1;
-          sm.Ublk[li][ti] = (li <= ti && li < nsb && ti < nsb) ? P.U[t * d + l] : T(0);
-        }
-        if (tid < SB) {
-          int64_t l = l_base + tid;
-          if (tid < nsb) {
-            sm.qv[tid] = P.gen.q ? P.gen.q[l] : 0.0;
-            sm.shv[tid] = shift_at<T>(P.gen, k * nY + l);
-            sm.tg[tid] = P.tgt[l + 1];
-          }
-        }
-        __syncthreads();
-        if (tid < TS) {
-          // in-block dot in the reference's order (src/qmc.jl:394-403):
-          // acc = S[target] + y_{l_base} U[..] + ... + y_l U[l, l+1]
-#pragma unroll 1
-          for (int li = 0; li < nsb; ++li) {
-            const int64_t l = l_base + li;
-            T y = st.quantile(P.gen, d, j, k, l, sm.qv[li], sm.shv[li]);
-            sm.u.Ysub[li][r] = y;
-            if (g0 < last_g0) Yw[l * TS + r] = y;
-            T acc = sm.Ss[sb + li][r];
-#pragma unroll 4
-            for (int mi = 0; mi <= li; ++mi) acc = fma(sm.u.Ysub[mi][r], sm.Ublk[mi][li], acc);
-            const auto tg = sm.tg[li];
-            st.cdf(acc, tg.a, tg.b, tg.inv_u, P.cdf_form);
-          }
-        }
-        __syncthreads();
-        // cross update: Ss[sb+SB+t][r] += sum_li Ysub[li][r] U[l_base+li][l_base+SB+1+t]
-        if (sb + SB < ng) {
-          const int nt2 = min(SB, ng - sb - SB);
-          for (int e = tid; e < SB * SB; e += NT) {
-            int li = e % SB, ti = e / SB;
-            int64_t t = l_base + SB + ti + 1;
-            sm.Ublk[li][ti] = (ti < nt2) ? P.U[t * d + l_base + li] : T(0);
-          }
-          __syncthreads();
-          const int rr = tid & (TS - 1), half = tid / TS;  // 2 threads per sample
-#pragma unroll 4
-          for (int ti = half * 16; ti < half * 16 + 16; ++ti) {
-            T acc = sm.Ss[sb + SB + ti][rr];
-#pragma unroll
-            for (int li = 0; li < SB; ++li) acc = fma(sm.u.Ysub[li][rr], sm.Ublk[li][ti], acc);
-            sm.Ss[sb + SB + ti][rr] = acc;
-          }
-          __syncthreads();
-        }
-      }
-    }
-    // ---- per-tile sum of p (fixed order) ----
-    double pv = (tid < TS && j < P.m) ? st.p : 0.0;
-    for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
-    if ((tid & 31) == 0) sm.red[tid >> 5] = pv;
-    __syncthreads();
-    if (tid == 0) {
-      double sum = 0.0;
-      for (int w = 0; w < NT / 32; ++w) sum += sm.red[w];
-      P.partials[tile] = sum;
-    }
-    __syncthreads();
-  }
-}
-
-// Per shift: Neumaier-compensated sum of its tile sums in tile order, then
-// the running mean of src/qmc.jl:437-442.
-__global__ void k_finalize(const double *partials, int64_t tiles_per_shift, int64_t n_reps,
-                           int64_t n_pts0, int64_t m, double *reps) {
-  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= n_reps) return;
-  const double *pk = partials + k * tiles_per_shift;
-  double s = 0.0, c = 0.0;
-  for (int64_t t = 0; t < tiles_per_shift; ++t) {
-    double x = pk[t];
-    double tt = s + x;
-    if (fabs(s) >= fabs(x)) c += (s - tt) + x;
-    else c += (x - tt) + s;
-    s = tt;
-  }
-  s += c;
-  double inv_tot = 1.0 / (double)(n_pts0 + m);
-  double mean_rep = s * inv_tot;
-  double old_weight = (double)n_pts0 * inv_tot;
-  reps[k] = fma(reps[k], old_weight, mean_rep);
-}
 
 template <typename T, typename Step>
 int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {

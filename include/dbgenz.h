@@ -168,6 +168,40 @@ int dbgz_problem_factor(const dbgz_problem *p, double *U, int64_t *perm, double 
 int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err,
                int64_t *n_pts, double *qmc_reps);
 
+/* ---- allocation-free pass -------------------------------------------
+ * No counterpart in the reference.  Some callers cannot let a library
+ * allocate device memory: a host framework that owns every device buffer
+ * and hands them to the library (an XLA/JAX custom call, a Julia program
+ * whose GPU memory is CUDA.jl's pool), or a latency-critical caller for
+ * whom cudaMalloc/cudaFree would synchronise the whole device.  For them
+ * this entry point runs one FP64 integration pass of qmc_pnorm! (Richtmyer
+ * points, erf-form CDF: the loop of src/qmc.jl:315-444 for one pass) and
+ * allocates nothing.  Its scratch (per-target constants, per-CTA y
+ * workspace, per-tile partial sums) is one fixed 32 MiB array compiled
+ * into the library, which every GPU that loads the library holds until
+ * the process exits.
+ *   Inputs, device pointers: U (d x d truncated factor, column-major, as
+ *   dbgz_problem_factor returns it), a and b (permuted, scaled bounds,
+ *   length d), q (d-1 lattice generators, dbgz_sqrt_primes), shifts
+ *   ((d-1) x n_reps in [0,1]).  n_base is the generator position of the
+ *   pass (0 for the first pass, then m, 2m, ...).
+ *   Output, device pointer: qmc_reps (n_reps), each shift's mean over its
+ *   m points.
+ *   stream: a cudaStream_t (NULL: the legacy default stream) on the current
+ *   device; the call only enqueues work and returns.
+ * Limits: 2 <= d <= 8192 and ceil(m/128) * n_reps <= 131072; larger sizes
+ * return DBGZ_ERR_DIMENSION.  Large d runs on fewer CTAs (the workspace
+ * share of one CTA grows with d), so this is slower than dbgz_pnorm.
+ * The first call on a device looks up the array's device address with
+ * that device current (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the one array and leave their
+ * intermediate data in it: calls whose work overlaps on the GPU (other
+ * streams or host threads at the same time) race and corrupt each other's
+ * results, so serialise them. */
+int dbgz_pnorm_pass_noalloc(int64_t d, const double *U, const double *a, const double *b,
+                            const double *q, const double *shifts, int64_t m, int64_t n_reps,
+                            int64_t n_base, double *qmc_reps, void *stream);
+
 /* ---- primitives of the path (device compute, host buffers) ---------- */
 
 /* cholesky_genz!(M, a, b, bs1, bs2, bs3, bs4) (src/cholesky.jl:445-628):
