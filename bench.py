@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "d=1000 MVN P time at |err|<=1e-5 vs FP64: mixed-prec vs FP64 GPU; grad/fwd cost"
 UNIT = "ms"
-MIXED = "fp32_simt"   # best mixed-precision mode built into this library
+MIXED = "fp32_split_bf16"   # mixed-precision mode of the headline number
 
 
 def _peaks():
@@ -105,12 +105,12 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload(rank: int, world: int, quick: bool):
+def workload(rank: int, world: int, quick: bool, d=None, points=None):
     from dbgenzpaper_b200 import workloads as W
     if quick:
-        w = W.c3(d=200, m=2**12, n_reps=16)
+        w = W.c3(d=d or 200, m=points or 2**12, n_reps=16)
     else:
-        w = W.c3()
+        w = W.c3(d=d or 1000, m=points or 2**17)
     # weak scaling: every rank integrates its own 16 shifts of the same problem
     if world > 1:
         rng = np.random.default_rng(10_000 + rank)
@@ -198,6 +198,10 @@ def main():
     ap.add_argument("--precision", default=MIXED)
     ap.add_argument("--quick", action="store_true", help="small d=200 case for smoke runs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--d", type=int, default=None, help="dimension (default: 1000)")
+    ap.add_argument("--points", type=int, default=None, help="points per shift (default: 2^17)")
+    ap.add_argument("--only", action="store_true",
+                    help="time only --precision (no FP64/other modes/accuracy/e2e/CPU legs); for profiling")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -221,7 +225,7 @@ def main():
     ctx = D.get_context(local)
     lib.dbgz_set_profiling(ctx.handle, 1)
     prec_mixed = D.PRECISIONS[args.precision]
-    w = workload(rank, world, args.quick)
+    w = workload(rank, world, args.quick, args.d, args.points)
     d = w.d
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
@@ -265,9 +269,33 @@ def main():
         (P_mix, err_mix, npts, reps_mix), ms_mix, loop_ms, n_loop, n_kern = timed(
             Q, prec_mixed, args.steps, args.warmup)
     clocks = clk.summary()
+    if args.only:
+        if rank == 0:
+            print(json.dumps({"precision": args.precision, "ms_per_step": ms_mix, "loop_ms": loop_ms,
+                              "P": P_mix, "workload": w.name, "samples": w.samples}), flush=True)
+        return 0
     # FP64 GPU path on the same points and shifts
     k64 = max(2, args.steps // 2)
     (P64, err64, _, reps64), ms64, loop64_ms, _, _ = timed(Q, L.PREC_FP64, k64, 1)
+    # the other mixed modes, same points and shifts
+    other = {}
+    for name in ("fp32_tf32", "fp32_split_bf16", "fp32_simt"):
+        if name == args.precision:
+            continue
+        (Po, _, _, _), mso, lo_ms, _, _ = timed(Q, D.PRECISIONS[name], max(2, args.steps // 2), 1)
+        other[name] = {"ms_per_step": mso, "loop_ms": lo_ms, "P": Po}
+    # accuracy where P is O(0.1): the same covariance with the reference's own
+    # bound design (+-k sqrt(S_ii), P(independent) = 0.25), same points
+    from dbgenzpaper_b200 import workloads as W
+    wq = W.c3_quarter(d=w.d, m=w.m, n_reps=w.n_reps)
+    Qq = D.QMCData(wq.Sigma, wq.a, wq.b, D.QMC_opts(m=wq.m, n_reps=wq.n_reps, max_pts=wq.m, max_abs_err=0.0),
+                   qmc_type="Richtmyer", shifts=wq.shifts, device=local)
+    acc = {"workload": wq.name}
+    acc["P_fp64"], acc["err_fp64"], _ = D.qmc_pnorm(Qq, precision=L.PREC_FP64)
+    for name in ("fp32_split_bf16", "fp32_tf32", "fp32_simt"):
+        Pm = D.qmc_pnorm(Qq, precision=D.PRECISIONS[name])[0]
+        acc[name] = {"P": Pm, "abs_err": abs(Pm - acc["P_fp64"]), "rel_err": abs(Pm - acc["P_fp64"]) / acc["P_fp64"]}
+    Qq.close()
 
     # e2e: the public API from host buffers, upload and factorisation included
     def e2e_step():
@@ -311,6 +339,8 @@ def main():
             "P": P_mix, "P_fp64": P64, "abs_err_vs_fp64": abs(P_mix - P64),
             "rel_err_vs_fp64": abs(P_mix - P64) / abs(P64) if P64 else None,
             "qmc_3sem": err_mix,
+            "other_modes": other,
+            "accuracy_quarter_bounds": acc,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
                          "kernel": f"integration loop ({args.precision})",

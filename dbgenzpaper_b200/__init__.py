@@ -54,7 +54,7 @@ PRECISIONS = {
     "fp32_simt": L.PREC_FP32_SIMT,
 }
 # precision used for QMC_opts(np.float32)
-DEFAULT_FP32_PRECISION = L.PREC_FP32_SIMT
+DEFAULT_FP32_PRECISION = L.PREC_FP32_SPLIT_BF16
 
 
 class Context:

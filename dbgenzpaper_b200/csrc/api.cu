@@ -440,8 +440,6 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
     return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "pnorm: bad precision %d", precision);
   if (p->structure != DBGZ_STRUCTURE_DENSE)
     return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm: sparse structure not built into this library yet");
-  if (precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16)
-    return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm: tensor-core modes not built into this library yet");
   cudaSetDevice(ctx->device);
   const dbgz_opts &o = p->opts;
   const int64_t n_reps = o.n_reps, m = o.m;
@@ -477,7 +475,11 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
     pa.gen_base = p->gen_base;
     const int64_t l_before = ctx->launch_count;
     if (prof) cudaEventRecord(ctx->ev[2], ctx->stream);
-    DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
+    const bool tensor = precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16;
+    if (tensor)
+      DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
+    else
+      DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
     if (prof) cudaEventRecord(ctx->ev[3], ctx->stream);
     pr.loop_launches += ctx->launch_count - l_before;
     if (prof) cudaEventRecord(ctx->ev[4], ctx->stream);
@@ -485,8 +487,15 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
     if (prof) cudaEventRecord(ctx->ev[5], ctx->stream);
     DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(reps.data(), p->reps.p, sizeof(double) * n_reps,
                                        cudaMemcpyDeviceToHost, ctx->stream));
+    int dev_status = 0;
+    if (tensor)
+      DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
     if (prof) cudaEventRecord(ctx->ev[1], ctx->stream);
     DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (dev_status != 0)
+      return dbgz_fail(ctx, DBGZ_ERR_TIMEOUT, "pnorm: a bounded wait in the tensor-core loop gave up (status %d)",
+                       dev_status);
     if (prof) {
       pr.loop_ms += event_ms(ctx->ev[2], ctx->ev[3]);
       pr.finalize_ms += event_ms(ctx->ev[4], ctx->ev[5]);

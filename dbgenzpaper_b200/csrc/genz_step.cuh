@@ -110,6 +110,13 @@ struct StepFp64 {
 };
 
 // ---------------------------------------------------------------- FP32 ---
+// Phi(-x0) - Phi(-x1) = (erfc(x0) - erfc(x1)) / 2 for 0 <= x0 <= x1 (erf
+// units) in FP64: the FP32 difference of two close tail masses cancels.
+// Rarely taken; kept out of line so the unrolled loop stays small.
+static __device__ __noinline__ float same_tail_mass64(float x0, float x1) {
+  return (float)(0.5 * (erfc((double)x0) - erfc((double)x1)));
+}
+
 struct StepFp32 {
   float lo, up, dc;  // Phi(alpha), Phi(-beta), Phi(beta) - Phi(alpha)
   double p;
@@ -139,10 +146,13 @@ struct StepFp32 {
       w1 = (float)(2.0 * fmin(u, 1.0 - u));
     }
     const float kEps = (float)DBL_EPSILON;
-    float t = fmaf(w, dc, lo);
-    if (t <= 0.5f) return normcdfinvf(fmaxf(t, kEps));
-    float qq = fmaf(w1, dc, up);
-    return -normcdfinvf(fmaxf(qq, kEps));
+    // u = lo + w dc when that is <= 1/2, else 1 - u = up + (1 - w) dc;
+    // Phi^-1 is taken of the smaller one (one call site keeps the code small)
+    const float t = fmaf(w, dc, lo);
+    const bool lower = t <= 0.5f;
+    const float arg = lower ? t : fmaf(w1, dc, up);
+    const float y = normcdfinvf(fmaxf(arg, kEps));
+    return lower ? y : -y;
   }
   __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
     float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
@@ -152,12 +162,12 @@ struct StepFp32 {
     float d;
     if (xa >= 0.0f) {                   // both bounds in the upper tail
       d = ea - eb;
-      if (eb > 0.5f * ea) d = (float)(0.5 * (erfc((double)xa) - erfc((double)xb)));
+      if (eb > 0.5f * ea) d = same_tail_mass64(xa, xb);
       lo = 1.0f - ea;
       up = eb;
     } else if (xb <= 0.0f) {            // both bounds in the lower tail
       d = eb - ea;
-      if (ea > 0.5f * eb) d = (float)(0.5 * (erfc(-(double)xb) - erfc(-(double)xa)));
+      if (ea > 0.5f * eb) d = same_tail_mass64(-xb, -xa);
       lo = ea;
       up = 1.0f - eb;
     } else {                            // alpha < 0 < beta

@@ -109,5 +109,7 @@ struct PassArgs {
 };
 int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);
+int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
+                   int64_t n_tiles);
 int dbgz_finalize_pass(dbgz_problem *p, const double *partials, int64_t tiles_per_shift,
                        int64_t n_pts0, int64_t m, double *reps);

@@ -1,0 +1,610 @@
+// loop_umma.cu -- the dense Genz integration loop with the conditioning
+// contraction on tcgen05 tensor cores (split-BF16 or TF32, FP32 accumulate
+// in TMEM) and the sequential per-dimension step on CUDA cores.
+//
+// Replaces qmc_loop!(::QMCData) (reference src/qmc.jl:315-444) for
+// T = Float32-class precision; the per-sample step is genz_step.cuh's
+// StepFp32 (FP32 special functions, FP64 weight product, FP64 tails).
+//
+// Decomposition.  One CTA owns a tile of 128 samples (128 consecutive points
+// of one shift) = the 128 TMEM lanes = the M of every MMA.  y-indices are
+// processed in phases of P (= TMEM columns, 256) and, inside a phase, blocks
+// of 32:
+//   * phase start (phase > 0): S[:, phase targets] = Y[:, 0:L] U[0:L, phase]
+//     -- a K = L GEMM whose A operand (this tile's earlier y's) streams back
+//     from a per-CTA workspace in HBM/L2 and B (U^T panel) from the
+//     converted factor, both by TMA, into TMEM columns 0..P-1;
+//   * block b: the 128 sample threads read their 32 partial sums of the
+//     block's targets from TMEM (tcgen05.ld), run the 32 sequential steps
+//     with an in-register rank-1 update for the block's own triangle, and
+//     write their y's (split hi/lo BF16, or TF32) as the A tile of the next
+//     MMA in shared memory (and to the workspace by TMA store when later
+//     phases need them);
+//   * after block b: S[:, targets of blocks b+1..] += Y_b U[b rows, ...] on
+//     the tensor cores -- first the 32 columns the next block needs
+//     (committed to its own barrier so the sample threads can go on), then
+//     the rest of the phase, which overlaps with the next block's steps.
+// Warp roles: warps 0-3 sample threads, warp 4 TMEM owner + MMA issuer,
+// warp 5 TMA producer.  Every wait is bounded (sm100.cuh); a timeout sets
+// DBGZ_ERR_TIMEOUT in the status word and the CTA drains and leaves.
+#include <cuda.h>
+
+#include "internal.cuh"
+#include "genz_step.cuh"
+#include "sm100.cuh"
+
+namespace {
+
+using namespace sm100;
+
+constexpr int TS = 128;    // samples per tile = TMEM lanes = MMA M
+constexpr int BK = 32;     // y-indices per block
+constexpr int NT = 192;    // 4 sample warps + MMA warp + producer warp
+constexpr int kMmaWarp = 4, kProdWarp = 5;
+constexpr int kBarScalar = 1;  // named barrier of the 128 sample threads
+
+template <int MODE>
+struct Fmt;
+template <>
+struct Fmt<DBGZ_PREC_FP32_SPLIT_BF16> {
+  static constexpr int NPART = 2, ROWB = 64, ATOM = 512, LAYOUT = 4, NKS = 2, ESZ = 2;
+  static constexpr uint32_t IDESC_FMT = 1;  // BF16
+};
+template <>
+struct Fmt<DBGZ_PREC_FP32_TF32> {
+  static constexpr int NPART = 1, ROWB = 128, ATOM = 1024, LAYOUT = 2, NKS = 4, ESZ = 4;
+  static constexpr uint32_t IDESC_FMT = 2;  // TF32
+};
+
+struct __align__(64) UmmaParams {
+  CUtensorMap tm_u[2];  // U^T panel parts: rows = targets, K = y-index
+  CUtensorMap tm_y[2];  // Y workspace parts: rows = slot*128 + sample, K = y-index
+  int64_t d, nY, m, n_reps, tiles_per_shift, n_tiles;
+  int P;
+  dbgz::GenParams gen;
+  const float *U32;  // d x d column-major (in-block triangle)
+  const TargetParams32 *tgt;
+  double c1, dc1, up1;
+  double *partials;
+  int *status;
+};
+
+struct Phase {
+  int64_t L;
+  int Pr, nb;
+};
+__device__ __forceinline__ Phase phase_of(const UmmaParams &p, int64_t ph) {
+  Phase f;
+  f.L = ph * p.P;
+  int64_t w = p.nY - f.L;
+  if (w > p.P) w = p.P;
+  f.Pr = (int)((w + BK - 1) / BK) * BK;
+  f.nb = f.Pr / BK;
+  return f;
+}
+
+__device__ __forceinline__ void named_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+template <int MODE>
+struct Smem {
+  static constexpr int ABYTES = TS * Fmt<MODE>::ROWB * Fmt<MODE>::NPART;  // one A tile, all parts
+  static constexpr int APART = TS * Fmt<MODE>::ROWB;
+  // B stage bytes depend on P: P rows per part
+  static __host__ __device__ int bpart(int P) { return P * Fmt<MODE>::ROWB; }
+  static __host__ __device__ int bbytes(int P) { return bpart(P) * Fmt<MODE>::NPART; }
+  static __host__ __device__ int off_b(int) { return 2 * ABYTES; }
+  static __host__ __device__ int off_misc(int P) { return 2 * ABYTES + 2 * bbytes(P); }
+  static __host__ __device__ int total(int P) { return off_misc(P) + 12288 + 1024; }
+};
+
+struct Misc {
+  float ublk[BK][2 * BK + 1];  // U of the block's triangle, zero beyond column BK
+  TargetParams32 tg[BK];
+  double qv[BK];
+  float shv[BK];
+  double red[4];
+  uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
+  uint32_t tmem_base;
+  int abort;
+};
+
+__device__ __forceinline__ void set_abort(Misc *ms, int *status) {
+  ms->abort = 1;
+  atomicExch(status, DBGZ_ERR_TIMEOUT);
+}
+
+// Swizzled K-major offset of 16-byte chunk c of row r.
+template <int MODE>
+__device__ __forceinline__ uint32_t a_chunk_off(int r, int c) {
+  if (MODE == DBGZ_PREC_FP32_SPLIT_BF16)
+    return (uint32_t)((r >> 3) * 512 + (r & 7) * 64 + ((c ^ ((r & 7) >> 1)) << 4));
+  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t *>(&h);
+}
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t t;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
+  return t;
+}
+
+template <int MODE, int GEN>
+__global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ UmmaParams P) {
+  using F = Fmt<MODE>;
+  using SM = Smem<MODE>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *sm = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char *abuf = sm;                       // 2 A tiles
+  unsigned char *bst = sm + SM::off_b(P.P);       // 2 B stages
+  Misc *ms = reinterpret_cast<Misc *>(sm + SM::off_misc(P.P));
+  volatile int *abort = &ms->abort;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t nphase = (P.nY + P.P - 1) / P.P;
+  const int32_t slot_row = (int32_t)blockIdx.x * TS;
+  const int bpart = SM::bpart(P.P);
+
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&ms->a_full[i], 1);
+      mbar_init(&ms->a_free[i], 1);
+      mbar_init(&ms->b_full[i], 1);
+      mbar_init(&ms->b_free[i], 1);
+    }
+    mbar_init(&ms->bar_s, 1);
+    mbar_init(&ms->ws_ready, 1);
+    mbar_init(&ms->drain, 1);
+    ms->abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == kMmaWarp) {
+    tmem_alloc(&ms->tmem_base, (uint32_t)P.P);
+    tmem_relinquish();
+  }
+  if (warp == kProdWarp && lane == 0) {
+    prefetch_tmap(&P.tm_u[0]);
+    prefetch_tmap(&P.tm_y[0]);
+    if (F::NPART > 1) {
+      prefetch_tmap(&P.tm_u[1]);
+      prefetch_tmap(&P.tm_y[1]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = ms->tmem_base;
+
+  if (warp == kProdWarp) {
+    // ---------------------------------------------------------------- TMA
+    if (lane == 0) {
+      uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0}, ws_cnt = 0;
+      uint32_t ja = 0, jb = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
+        for (int64_t ph = 0; ph < nphase && ok; ++ph) {
+          const Phase f = phase_of(P, ph);
+          if (ph > 0) {
+            ok = mbar_wait(&ms->ws_ready, ws_cnt & 1, abort);
+            ++ws_cnt;
+            const int nbox = (f.Pr + 63) / 64;
+            for (int64_t kc = 0; kc < f.L / BK && ok; ++kc) {
+              const int ia = ja & 1, ib = jb & 1;
+              if (a_use[ia] > 0) ok = ok && mbar_wait(&ms->a_free[ia], (a_use[ia] - 1) & 1, abort);
+              if (b_use[ib] > 0) ok = ok && mbar_wait(&ms->b_free[ib], (b_use[ib] - 1) & 1, abort);
+              if (!ok) break;
+              mbar_arrive_expect_tx(&ms->a_full[ia], SM::ABYTES);
+              for (int pp = 0; pp < F::NPART; ++pp)
+                tma_load_2d(abuf + ia * SM::ABYTES + pp * SM::APART, &P.tm_y[pp], (int32_t)(kc * BK),
+                            slot_row, &ms->a_full[ia]);
+              mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
+              for (int pp = 0; pp < F::NPART; ++pp)
+                for (int i = 0; i < nbox; ++i)
+                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &P.tm_u[pp],
+                              (int32_t)(kc * BK), (int32_t)(f.L + 1 + 64 * i), &ms->b_full[ib]);
+              ++a_use[ia];
+              ++b_use[ib];
+              ++ja;
+              ++jb;
+            }
+          }
+          for (int b = 0; b < f.nb && ok; ++b) {
+            const int ia = ja & 1, ib = jb & 1;
+            ++a_use[ia];  // the sample threads fill this A tile
+            ++ja;
+            if (b_use[ib] > 0) ok = mbar_wait(&ms->b_free[ib], (b_use[ib] - 1) & 1, abort);
+            if (!ok) break;
+            if (b < f.nb - 1) {
+              const int rows = f.Pr - BK * (b + 1);
+              const int nbox = (rows + 63) / 64;
+              mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
+              for (int pp = 0; pp < F::NPART; ++pp)
+                for (int i = 0; i < nbox; ++i)
+                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &P.tm_u[pp],
+                              (int32_t)(f.L + BK * b), (int32_t)(f.L + 1 + BK * (b + 1) + 64 * i),
+                              &ms->b_full[ib]);
+            } else {
+              mbar_arrive(&ms->b_full[ib]);
+            }
+            ++b_use[ib];
+            ++jb;
+          }
+        }
+      }
+      if (!ok) {
+        set_abort(ms, P.status);
+        // let loads already issued land before the CTA leaves
+        for (int i = 0; i < 2; ++i) {
+          if (a_use[i] > 0) mbar_wait(&ms->a_full[i], (a_use[i] - 1) & 1, abort);
+          if (b_use[i] > 0) mbar_wait(&ms->b_full[i], (b_use[i] - 1) & 1, abort);
+        }
+      }
+    }
+  } else if (warp == kMmaWarp) {
+    // ---------------------------------------------------------------- MMA
+    if (lane == 0) {
+      uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0};
+      uint32_t ja = 0, jb = 0;
+      bool ok = true;
+      const uint32_t sbo = F::ATOM;
+      auto issue = [&](uint32_t d_col, int ncols, uint32_t a_addr, uint32_t b_addr, bool overwrite) {
+        // D[:, d_col .. d_col+ncols) (+)= A[128 x 32] * B[ncols x 32]^T; split
+        // BF16 as hi*hi + hi*lo + lo*hi.
+        for (int c0 = 0; c0 < ncols; c0 += 256) {
+          const int n = ncols - c0 < 256 ? ncols - c0 : 256;
+          const uint32_t idesc = instr_desc(F::IDESC_FMT, F::IDESC_FMT, 128, (uint32_t)n);
+          const uint32_t bo = (uint32_t)(c0 * F::ROWB);
+          for (int ks = 0; ks < F::NKS; ++ks) {
+            const uint32_t acc0 = (overwrite && ks == 0) ? 0u : 1u;
+            const uint64_t a0 = smem_desc(a_addr + 32 * ks, sbo, F::LAYOUT);
+            const uint64_t b0 = smem_desc(b_addr + bo + 32 * ks, sbo, F::LAYOUT);
+            if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
+              const uint64_t a1 = smem_desc(a_addr + SM::APART + 32 * ks, sbo, F::LAYOUT);
+              const uint64_t b1 = smem_desc(b_addr + bpart + bo + 32 * ks, sbo, F::LAYOUT);
+              mma_f16(tmem + d_col + c0, a0, b0, idesc, acc0);
+              mma_f16(tmem + d_col + c0, a0, b1, idesc, 1u);
+              mma_f16(tmem + d_col + c0, a1, b0, idesc, 1u);
+            } else {
+              mma_tf32(tmem + d_col + c0, a0, b0, idesc, acc0);
+            }
+          }
+        }
+      };
+      for (int64_t tile = blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
+        for (int64_t ph = 0; ph < nphase && ok; ++ph) {
+          const Phase f = phase_of(P, ph);
+          const int64_t nkc = ph > 0 ? f.L / BK : 0;
+          for (int64_t kc = 0; kc < nkc && ok; ++kc) {
+            const int ia = ja & 1, ib = jb & 1;
+            ok = mbar_wait(&ms->a_full[ia], a_use[ia] & 1, abort) &&
+                 mbar_wait(&ms->b_full[ib], b_use[ib] & 1, abort);
+            if (!ok) break;
+            tc_fence_after();
+            issue(0, f.Pr, smem_u32(abuf + ia * SM::ABYTES), smem_u32(bst + ib * SM::bbytes(P.P)),
+                  kc == 0);
+            mma_commit(&ms->a_free[ia]);
+            mma_commit(&ms->b_free[ib]);
+            if (kc == nkc - 1) mma_commit(&ms->bar_s);
+            ++a_use[ia];
+            ++b_use[ib];
+            ++ja;
+            ++jb;
+          }
+          for (int b = 0; b < f.nb && ok; ++b) {
+            const int ia = ja & 1, ib = jb & 1;
+            ok = mbar_wait(&ms->a_full[ia], a_use[ia] & 1, abort) &&
+                 mbar_wait(&ms->b_full[ib], b_use[ib] & 1, abort);
+            if (!ok) break;
+            tc_fence_after();
+            if (b < f.nb - 1) {
+              const bool first = (ph == 0 && b == 0);
+              const uint32_t aa = smem_u32(abuf + ia * SM::ABYTES);
+              const uint32_t bb = smem_u32(bst + ib * SM::bbytes(P.P));
+              issue((uint32_t)(BK * (b + 1)), BK, aa, bb, first);  // next block's columns
+              mma_commit(&ms->bar_s);
+              const int rest = f.Pr - BK * (b + 2);
+              if (rest > 0) issue((uint32_t)(BK * (b + 2)), rest, aa, bb + BK * F::ROWB, first);
+              mma_commit(&ms->a_free[ia]);
+              mma_commit(&ms->b_free[ib]);
+            } else {
+              mbar_arrive(&ms->a_free[ia]);
+              mbar_arrive(&ms->b_free[ib]);
+            }
+            ++a_use[ia];
+            ++b_use[ib];
+            ++ja;
+            ++jb;
+          }
+        }
+      }
+      if (!ok) set_abort(ms, P.status);
+      mma_commit(&ms->drain);
+      if (!mbar_wait(&ms->drain, 0, abort)) {
+        // abort was raised elsewhere: still give the tensor cores time to finish
+        const uint64_t t0 = globaltimer();
+        while (!mbar_try_wait(&ms->drain, 0) && globaltimer() - t0 < kWaitLimitNs) {
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------------ sample threads
+    const int r = tid;  // sample row = TMEM lane
+    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+    uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
+    const bool need_ws = nphase > 1;
+    for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
+      const int64_t k_shift = tile / P.tiles_per_shift;
+      const int64_t jt = tile - k_shift * P.tiles_per_shift;
+      const int64_t j = jt * TS + r;
+      dbgz::StepFp32 st;
+      st.init(P.c1, P.dc1, P.up1);
+      dbgz::GenParams gen = P.gen;
+      gen.qmc_type = GEN;  // compile-time generator: only one point path in the code
+      for (int64_t ph = 0; ph < nphase; ++ph) {
+        const Phase f = phase_of(P, ph);
+        if (ph > 0) {
+          for (int64_t kc = 0; kc < f.L / BK; ++kc) {
+            ++a_use[ja & 1];
+            ++ja;
+          }
+        }
+        for (int b = 0; b < f.nb; ++b) {
+          const int ia = ja & 1;
+          const int64_t lbase = f.L + BK * b;
+          const int nval = (int)((P.nY - lbase) < BK ? (P.nY - lbase) : BK);
+          // stage the block's U triangle and per-dimension parameters
+          named_sync(kBarScalar, TS);
+          for (int e = r; e < BK * 2 * BK; e += TS) {
+            const int li = e % BK, ti = e / BK;
+            ms->ublk[li][ti] =
+                (li <= ti && ti < nval) ? P.U32[(lbase + ti + 1) * P.d + lbase + li] : 0.f;
+          }
+          if (r < BK && r < nval) {
+            ms->tg[r] = P.tgt[lbase + r + 1];
+            ms->qv[r] = P.gen.q ? P.gen.q[lbase + r] : 0.0;
+            ms->shv[r] = P.gen.shift32 ? P.gen.shift32[k_shift * P.nY + lbase + r] : 0.f;
+          }
+          // partial sums of the block's targets, accumulated by the tensor cores
+          float s[BK];
+          bool ok = true;
+          if (ph == 0 && b == 0) {
+#pragma unroll
+            for (int t = 0; t < BK; ++t) s[t] = 0.f;
+          } else {
+            ok = mbar_wait(&ms->bar_s, s_cnt & 1, abort);
+            ++s_cnt;
+            tc_fence_after();
+            uint32_t v[BK];
+            tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(BK * b), v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int t = 0; t < BK; ++t) s[t] = __uint_as_float(v[t]);
+          }
+          // the A tile must be free: its previous MMA done, its previous store read
+          if (a_use[ia] > 0) ok = mbar_wait(&ms->a_free[ia], (a_use[ia] - 1) & 1, abort) && ok;
+          if (r == 0) bulk_wait_read_all();
+          if (!ok) set_abort(ms, P.status);
+          named_sync(kBarScalar, TS);
+          if (*abort) goto done;
+          {
+            // 4 chunks of 8 sequential steps.  s[] is kept in a frame that
+            // rotates by 8 per chunk, so that every register index is static:
+            // in chunk ch, s[t] is the partial sum of target lbase + 8 ch + t + 1.
+            unsigned char *A = abuf + ia * SM::ABYTES;
+#pragma unroll 1
+            for (int ch = 0; ch < BK / 8; ++ch) {
+              uint32_t hi[4], lo[4];
+              float ys[8];
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                const int li = 8 * ch + k;
+                float y = 0.f;
+                if (li < nval) {
+                  const int64_t l = lbase + li;
+                  y = st.quantile(gen, P.d, j, k_shift, l, ms->qv[li], ms->shv[li]);
+                  const float *urow = &ms->ublk[li][8 * ch];
+#pragma unroll
+                  for (int t = k; t < BK; ++t) s[t] = fmaf(y, urow[t], s[t]);
+                  const TargetParams32 tg = ms->tg[li];
+                  st.cdf(s[k], tg.a, tg.b, tg.inv_u, 0);
+                }
+                ys[k] = y;
+              }
+              if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  const __nv_bfloat162 h = __floats2bfloat162_rn(ys[2 * e], ys[2 * e + 1]);
+                  const float2 hf = __bfloat1622float2(h);
+                  hi[e] = *reinterpret_cast<const uint32_t *>(&h);
+                  lo[e] = pack_bf16x2(ys[2 * e] - hf.x, ys[2 * e + 1] - hf.y);
+                }
+                const uint32_t off = a_chunk_off<MODE>(r, ch);
+                *reinterpret_cast<uint4 *>(A + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<uint4 *>(A + SM::APART + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+              } else {
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2) {
+                  const uint32_t off = a_chunk_off<MODE>(r, 2 * ch + h2);
+                  *reinterpret_cast<uint4 *>(A + off) =
+                      make_uint4(to_tf32(ys[4 * h2]), to_tf32(ys[4 * h2 + 1]), to_tf32(ys[4 * h2 + 2]),
+                                 to_tf32(ys[4 * h2 + 3]));
+                }
+              }
+#pragma unroll
+              for (int t = 0; t < BK - 8; ++t) s[t] = s[t + 8];
+#pragma unroll
+              for (int t = BK - 8; t < BK; ++t) s[t] = 0.f;
+            }
+          }
+          fence_proxy_async_smem();
+          tc_fence_before();
+          named_sync(kBarScalar, TS);
+          if (r == 0) {
+            mbar_arrive(&ms->a_full[ia]);
+            if (need_ws && ph < nphase - 1) {
+              for (int pp = 0; pp < F::NPART; ++pp)
+                tma_store_2d(&P.tm_y[pp], (int32_t)lbase, slot_row, abuf + ia * SM::ABYTES + pp * SM::APART);
+              bulk_commit();
+              if (b == f.nb - 1) {
+                bulk_wait_all();
+                mbar_arrive(&ms->ws_ready);
+                ++ws_cnt;
+              }
+            }
+          }
+          ++a_use[ia];
+          ++ja;
+        }
+      }
+      // per-tile sum of p in a fixed order
+      {
+        double pv = (j < P.m) ? st.p : 0.0;
+        for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
+        if (lane == 0) ms->red[warp] = pv;
+        named_sync(kBarScalar, TS);
+        if (r == 0) P.partials[tile] = ((ms->red[0] + ms->red[1]) + ms->red[2]) + ms->red[3];
+      }
+    }
+  done:
+    if (r == 0) bulk_wait_all();
+    (void)ws_cnt;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    tc_fence_after();
+    tmem_dealloc(tmem, (uint32_t)P.P);
+  }
+}
+
+// U^T panels: Ut[t * ldU + l] = U[l, t] for l < t (strict upper), else 0.
+template <int MODE>
+__global__ void k_make_ut(const double *U, int64_t d, int64_t ldU, void *out0, void *out1) {
+  const int64_t t = blockIdx.y;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < ldU; l += (int64_t)gridDim.x * blockDim.x) {
+    const double u = (l < t && t < d) ? U[t * d + l] : 0.0;
+    if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
+      const __nv_bfloat16 h = __double2bfloat16(u);
+      const __nv_bfloat16 lo = __double2bfloat16(u - (double)__bfloat162float(h));
+      reinterpret_cast<__nv_bfloat16 *>(out0)[t * ldU + l] = h;
+      reinterpret_cast<__nv_bfloat16 *>(out1)[t * ldU + l] = lo;
+    } else {
+      reinterpret_cast<uint32_t *>(out0)[t * ldU + l] = to_tf32((float)u);
+    }
+  }
+}
+
+typedef CUresult (*EncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                            const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                            CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn() {
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeFn)p;
+  }
+  return fn;
+}
+
+template <int MODE>
+int encode_2d(dbgz_ctx *ctx, CUtensorMap *m, void *base, uint64_t inner, uint64_t rows, uint32_t box_rows) {
+  using F = Fmt<MODE>;
+  EncodeFn enc = encode_fn();
+  if (!enc) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  cuuint64_t dims[2] = {inner, rows};
+  cuuint64_t strides[1] = {inner * F::ESZ};
+  cuuint32_t box[2] = {(cuuint32_t)BK, box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(m, F::ESZ == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base,
+                   dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   F::ESZ == 2 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return DBGZ_OK;
+}
+
+template <int MODE>
+int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
+  using F = Fmt<MODE>;
+  using SM = Smem<MODE>;
+  dbgz_ctx *ctx = p->ctx;
+  const int64_t d = pa.d, nY = d - 1;
+  const int64_t Dp = ((nY + 63) / 64) * 64;
+  // converted factor (built on first use for this precision)
+  DevBuf &u0 = MODE == DBGZ_PREC_FP32_TF32 ? p->Utf : p->Uhi;
+  if (!u0.p || p->ldU != Dp) {
+    p->ldU = Dp;
+    DBGZ_TRY(dbgz_ensure(ctx, u0, (size_t)d * Dp * F::ESZ));
+    if (F::NPART > 1) DBGZ_TRY(dbgz_ensure(ctx, p->Ulo, (size_t)d * Dp * F::ESZ));
+    dim3 g((unsigned)((Dp + 255) / 256), (unsigned)d);
+    k_make_ut<MODE><<<g, 256, 0, ctx->stream>>>((const double *)p->U.p, d, Dp, u0.p,
+                                                F::NPART > 1 ? p->Ulo.p : nullptr);
+    dbgz_count_launch(ctx);
+    DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  }
+  if (!p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
+  const int Pw = 256;
+  const int smem = SM::total(Pw);
+  auto kern = pa.qmc_type == DBGZ_QMC_SOBOL ? k_genz_umma<MODE, DBGZ_QMC_SOBOL> : k_genz_umma<MODE, DBGZ_QMC_RICHTMYER>;
+  DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  int per_sm = 0;
+  DBGZ_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+  per_sm = std::min(per_sm, 512 / Pw);
+  if (per_sm < 1) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor-core loop does not fit on an SM");
+  const int64_t grid = std::min<int64_t>(n_tiles, (int64_t)per_sm * ctx->num_sms);
+  const int64_t nphase = (nY + Pw - 1) / Pw;
+  UmmaParams P{};
+  P.d = d;
+  P.nY = nY;
+  P.m = pa.m;
+  P.n_reps = pa.n_reps;
+  P.tiles_per_shift = (pa.m + TS - 1) / TS;
+  P.n_tiles = n_tiles;
+  P.P = Pw;
+  P.gen.qmc_type = pa.qmc_type;
+  P.gen.n_bits = pa.n_bits;
+  P.gen.gen_base = pa.gen_base;
+  P.gen.sobol_first = pa.sobol_first;
+  P.gen.q = (const double *)p->q.p;
+  P.gen.shift64 = (const double *)p->shifts.p;
+  P.gen.shift32 = (const float *)p->shifts32.p;
+  P.gen.V = (const uint32_t *)p->V.p;
+  P.gen.ushift = (const uint64_t *)p->ushifts.p;
+  P.U32 = (const float *)p->U32.p;
+  P.tgt = (const TargetParams32 *)p->tgt32.p;
+  P.c1 = pa.c1;
+  P.dc1 = pa.dc1;
+  P.up1 = 1.0 - pa.c1 - pa.dc1;
+  P.partials = partials;
+  P.status = ctx->d_status;
+  DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_u[0], u0.p, (uint64_t)Dp, (uint64_t)d, 64));
+  if (F::NPART > 1) DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_u[1], p->Ulo.p, (uint64_t)Dp, (uint64_t)d, 64));
+  // Y workspace: one 128-row slot per CTA, parts side by side
+  const size_t part_bytes = (size_t)grid * TS * Dp * F::ESZ;
+  (void)nphase;
+  DBGZ_TRY(dbgz_ensure(ctx, p->yws, part_bytes * F::NPART));
+  for (int pp = 0; pp < F::NPART; ++pp)
+    DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_y[pp], (char *)p->yws.p + pp * part_bytes, (uint64_t)Dp,
+                             (uint64_t)grid * TS, TS));
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+  kern<<<(unsigned)grid, NT, smem, ctx->stream>>>(P);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+}  // namespace
+
+int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials, int64_t n_tiles) {
+  if (precision == DBGZ_PREC_FP32_SPLIT_BF16)
+    return launch_umma<DBGZ_PREC_FP32_SPLIT_BF16>(p, pa, partials, n_tiles);
+  return launch_umma<DBGZ_PREC_FP32_TF32>(p, pa, partials, n_tiles);
+}

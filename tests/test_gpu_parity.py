@@ -250,3 +250,51 @@ def test_error_statuses(D):
     with pytest.raises(D.DbgzError) as e:
         D.qmc_pnorm(Q, precision=17)
     assert e.value.status == L.ERR_INVALID_ARGUMENT
+
+
+# ------------------------------------------------------- tensor-core loop ---
+# FP32 numerics with the contraction on tcgen05: split BF16 (3 products) is
+# held to the FP32-SIMT bar; TF32 (one product, 10-bit mantissa operands) to
+# a looser one.
+TC_TOL = {L.PREC_FP32_SPLIT_BF16: (5e-6, 2e-5), L.PREC_FP32_TF32: (1e-4, 2e-3)}
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
+@pytest.mark.parametrize("c", DENSE_CASES)
+def test_pnorm_tensor_core_fixture(D, c, prec):
+    z = np.load(os.path.join(GOLD, "oracle_cases.npz"))
+    g = _case(z, c)
+    Q = _from_case(D, g, np.float32, precision=prec)
+    P, err, npts, reps = D.qmc_pnorm(Q, return_reps=True)
+    P64 = float(g["P"])
+    at, rt = TC_TOL[prec]
+    assert npts == int(g["n_pts"])
+    assert abs(P - P64) <= at + rt * abs(P64), (P, P64, abs(P - P64))
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
+@pytest.mark.parametrize("n,m,n_reps", [(300, 777, 3), (600, 512, 2), (1000, 256, 2), (257, 300, 2)])
+def test_pnorm_tensor_core_phases(D, n, m, n_reps, prec):
+    # several 256-wide phases: the phase-start GEMM reads this tile's earlier
+    # y's back from the workspace; partial tiles and a partial last block
+    S = _spd(n, n + 7)
+    lo, up = W.bounds_quarter(S)
+    sh = np.random.default_rng(n).random((n - 1, n_reps))
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=m, n_reps=n_reps, max_pts=m, max_abs_err=0.0), shifts=sh)
+    P64, _, _, r64 = D.qmc_pnorm(Q, precision=L.PREC_FP64, return_reps=True)
+    Ps, _, _, rs = D.qmc_pnorm(Q, precision=L.PREC_FP32_SIMT, return_reps=True)
+    Pt, _, _, rt_ = D.qmc_pnorm(Q, precision=prec, return_reps=True)
+    at, rt = TC_TOL[prec]
+    assert abs(Ps - P64) <= 5e-6 + 2e-5 * abs(P64), (Ps, P64)
+    assert abs(Pt - P64) <= at + rt * abs(P64), (Pt, P64, abs(Pt - P64) / abs(P64))
+    np.testing.assert_allclose(rt_, r64, rtol=10 * rt, atol=10 * at)
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
+def test_identity_known_answer_tensor_core(D, prec):
+    n = 40
+    lo, up = W.bounds_quarter(np.eye(n))
+    Q = D.QMCData(np.eye(n), lo, up, D.QMC_opts(m=1000, n_reps=4), rng=np.random.default_rng(2),
+                  precision=prec)
+    P, err, _ = D.qmc_pnorm(Q)
+    assert abs(P - 0.25) < 1e-6
