@@ -4,6 +4,7 @@
 #include <cuda_bf16.h>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstdarg>
 #include <string>
 #include <vector>

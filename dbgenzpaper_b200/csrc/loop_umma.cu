@@ -555,9 +555,22 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   auto kern = pa.qmc_type == DBGZ_QMC_SOBOL ? k_genz_umma<MODE, DBGZ_QMC_SOBOL> : k_genz_umma<MODE, DBGZ_QMC_RICHTMYER>;
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  int per_sm = 0;
-  DBGZ_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
-  per_sm = std::min(per_sm, 512 / Pw);
+  // CTAs per SM from the kernel's own resources: TMEM columns (512 / P),
+  // registers and shared memory.  (The runtime occupancy query returns 1 for
+  // this kernel although two CTAs fit; if they did not, the extra CTAs would
+  // only start later.)
+  cudaFuncAttributes fa;
+  DBGZ_CUDA_TRY(ctx, cudaFuncGetAttributes(&fa, kern));
+  int smem_per_sm = 0, regs_per_sm = 0;
+  cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
+  cudaDeviceGetAttribute(&regs_per_sm, cudaDevAttrMaxRegistersPerMultiprocessor, ctx->device);
+  const int regs_cta = ((fa.numRegs + 7) / 8) * 8 * NT;
+  int per_sm = 512 / Pw;
+  per_sm = std::min(per_sm, smem_per_sm / (smem + 1024));
+  per_sm = std::min(per_sm, regs_per_sm / std::max(regs_cta, 1));
+  if (getenv("DBGZ_DEBUG"))
+    fprintf(stderr, "dbgz: tensor-core loop %d CTA/SM (smem %d of %d B, regs %d x %d of %d)\n", per_sm, smem,
+            smem_per_sm, fa.numRegs, NT, regs_per_sm);
   if (per_sm < 1) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor-core loop does not fit on an SM");
   const int64_t grid = std::min<int64_t>(n_tiles, (int64_t)per_sm * ctx->num_sms);
   const int64_t nphase = (nY + Pw - 1) / Pw;
