@@ -40,6 +40,9 @@ sys.path.insert(0, ROOT)
 METRIC = "d=1000 MVN P time at |err|<=1e-5 vs FP64: mixed-prec vs FP64 GPU; grad/fwd cost"
 UNIT = "ms"
 MIXED = "fp32_split_bf16"   # mixed-precision mode of the headline number
+# DRAM bytes of one 2^21-sample launch of the split-BF16 loop at d=1000 (ncu capture of a
+# 131,072-sample launch: 0.274 GB read + 0.351 GB written, scaled by the sample count)
+TRAFFIC_PER_LAUNCH = 16 * (274.25e6 + 350.67e6)
 
 
 def _peaks():
@@ -342,7 +345,10 @@ def main():
             "other_modes": other,
             "accuracy_quarter_bounds": acc,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if w.samples == 2**21 else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                                           "the split-BF16 loop at 8192 points x 16 shifts, scaled by 16 "
+                                           "to the 2^17-point launch",
                          "kernel": f"integration loop ({args.precision})",
                          "flops_per_launch": flops, "launch_ms": loop_ms,
                          "peak_source": f"{peak_kind} bf16_tflops (burst)"},

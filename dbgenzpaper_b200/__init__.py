@@ -217,6 +217,12 @@ class QMCData:
                                       method, sv)
         return self._chol
 
+    def truncate_band(self, bandwidth: int) -> None:
+        """Drop factor entries more than `bandwidth` above the diagonal (the
+        banded workload's truncation; no counterpart in the reference)."""
+        L.check(L.lib().dbgz_problem_truncate_band(self.handle, int(bandwidth)), self.ctx.handle)
+        self._chol = None
+
     @property
     def a(self):
         return self.C.a

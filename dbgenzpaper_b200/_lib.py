@@ -86,6 +86,7 @@ SIGNATURES = {
                                C.c_int, C.c_int, _pd, _pu64, _pu32, C.c_int64, C.POINTER(_vp)]),
     "dbgz_problem_free": (C.c_int, [_vp]),
     "dbgz_problem_set_cdf_form": (C.c_int, [_vp, C.c_int]),
+    "dbgz_problem_truncate_band": (C.c_int, [_vp, C.c_int64]),
     "dbgz_problem_factor": (C.c_int, [_vp, _pd, _pi64, _pd, _pd, _pd, _pi64]),
     "dbgz_pnorm": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
     "dbgz_pnorm_pass_noalloc": (C.c_int, [C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int64,

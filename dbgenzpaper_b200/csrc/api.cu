@@ -369,7 +369,8 @@ int dbgz_problem_free(dbgz_problem *p) {
   }
   DevBuf *bufs[] = {&p->U, &p->a, &p->b, &p->perm, &p->scale, &p->q, &p->shifts, &p->shifts32,
                     &p->V, &p->ushifts, &p->tgt64, &p->tgt32, &p->U32, &p->Uhi, &p->Ulo,
-                    &p->Utf, &p->yws, &p->partials, &p->reps};
+                    &p->Utf, &p->yws, &p->partials, &p->reps, &p->csc_colptr, &p->csc_row,
+                    &p->csc_val64, &p->csc_val32};
   for (DevBuf *b : bufs) dbgz_release(*b);
   delete p;
   return DBGZ_OK;
@@ -381,6 +382,20 @@ int dbgz_problem_set_cdf_form(dbgz_problem *p, int cdf_form) {
     return dbgz_fail(p->ctx, DBGZ_ERR_INVALID_ARGUMENT, "set_cdf_form: bad form %d", cdf_form);
   if (p->cdf_form != cdf_form) p->c1_ready = false;
   p->cdf_form = cdf_form;
+  return DBGZ_OK;
+}
+
+int dbgz_problem_truncate_band(dbgz_problem *p, int64_t bandwidth) {
+  if (!p || bandwidth < 1) return DBGZ_ERR_INVALID_ARGUMENT;
+  dbgz_ctx *ctx = p->ctx;
+  cudaSetDevice(ctx->device);
+  p->band = bandwidth;
+  DBGZ_TRY(dbgz_band_dev(ctx, p->d, (double *)p->U.p, bandwidth));
+  DevBuf *derived[] = {&p->U32, &p->Uhi, &p->Ulo, &p->Utf, &p->csc_colptr, &p->csc_row, &p->csc_val64,
+                       &p->csc_val32};
+  for (DevBuf *b : derived) dbgz_release(*b);
+  p->ldU = 0;
+  DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return DBGZ_OK;
 }
 
@@ -438,8 +453,6 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
   dbgz_ctx *ctx = p->ctx;
   if (precision < DBGZ_PREC_FP64 || precision > DBGZ_PREC_FP32_SIMT)
     return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "pnorm: bad precision %d", precision);
-  if (p->structure != DBGZ_STRUCTURE_DENSE)
-    return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm: sparse structure not built into this library yet");
   cudaSetDevice(ctx->device);
   const dbgz_opts &o = p->opts;
   const int64_t n_reps = o.n_reps, m = o.m;
@@ -475,8 +488,11 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
     pa.gen_base = p->gen_base;
     const int64_t l_before = ctx->launch_count;
     if (prof) cudaEventRecord(ctx->ev[2], ctx->stream);
-    const bool tensor = precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16;
-    if (tensor)
+    const bool sparse = p->structure == DBGZ_STRUCTURE_SPARSE;
+    const bool tensor = !sparse && (precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16);
+    if (sparse)
+      DBGZ_TRY(dbgz_loop_sparse(p, pa, precision, (double *)p->partials.p, n_tiles));
+    else if (tensor)
       DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
     else
       DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));

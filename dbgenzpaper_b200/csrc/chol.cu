@@ -307,6 +307,12 @@ __global__ void k_truncate(double *U, int64_t nn, double min_val) {
     if (fabs(U[t]) < min_val) U[t] = 0.0;
 }
 
+__global__ void k_band(double *U, int64_t d, int64_t band) {
+  const int64_t t = blockIdx.y;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < t - band; l += (int64_t)gridDim.x * blockDim.x)
+    U[t * d + l] = 0.0;
+}
+
 __global__ void k_targets(const double *U, int64_t n, const double *a, const double *b,
                           TargetParams64 *t64, TargetParams32 *t32) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -468,6 +474,14 @@ int dbgz_truncate_dev(dbgz_ctx *ctx, int64_t n, double *U, double eps_T) {
   int64_t nn = n * n;
   int blocks = (int)std::min<int64_t>((nn + 255) / 256, 4096);
   k_truncate<<<blocks, 256, 0, ctx->stream>>>(U, nn, min_val);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+int dbgz_band_dev(dbgz_ctx *ctx, int64_t d, double *U, int64_t band) {
+  dim3 g((unsigned)std::max<int64_t>(1, (d + 255) / 256), (unsigned)d);
+  k_band<<<g, 256, 0, ctx->stream>>>(U, d, band);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   return DBGZ_OK;

@@ -74,6 +74,9 @@ struct dbgz_problem {
   DevBuf tgt64, tgt32, U32;
   DevBuf Uhi, Ulo, Utf;  // tensor-core operands of the contraction
   int64_t ldU = 0;       // padded leading dimension of Uhi/Ulo/Utf
+  // sparse (banded) structure: CSC of the strict upper factor
+  DevBuf csc_colptr, csc_row, csc_val64, csc_val32;
+  int64_t nnz = 0, bandwidth = 0, band = 0;  // band > 0: entries beyond it dropped
   // workspaces
   DevBuf yws, partials, reps;
   double c1 = 0, dc1 = 0;
@@ -88,6 +91,7 @@ int dbgz_chol_classic_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double
                           int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4, double *scale);
 int dbgz_truncate_dev(dbgz_ctx *ctx, int64_t n, double *U, double eps_T);
 int dbgz_make_targets(dbgz_problem *p);
+int dbgz_band_dev(dbgz_ctx *ctx, int64_t d, double *U, int64_t band);
 int dbgz_make_U32(dbgz_problem *p);
 
 // ---- points (points.cu) --------------------------------------------------
@@ -112,5 +116,8 @@ int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *p
                    int64_t n_tiles);
 int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);
+int dbgz_loop_sparse(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
+                     int64_t n_tiles);
+int dbgz_build_csc(dbgz_problem *p);
 int dbgz_finalize_pass(dbgz_problem *p, const double *partials, int64_t tiles_per_shift,
                        int64_t n_pts0, int64_t m, double *reps);

@@ -154,6 +154,14 @@ int dbgz_problem_free(dbgz_problem *p);
  * switches the form of one problem instead of copying it. */
 int dbgz_problem_set_cdf_form(dbgz_problem *p, int cdf_form);
 
+/* Drops the factor's entries more than `bandwidth` above the diagonal
+ * (U[l,t] = 0 for t - l > bandwidth) and rebuilds the derived operands.
+ * No counterpart in the reference: QMCDataSparse keeps every entry that
+ * survives the eps/(9d) truncation (src/qmc.jl:270-272); the banded
+ * workload at d = 10^4 (AR(1) covariance, whose factor is dense with
+ * geometric decay) specifies this band truncation on top of it. */
+int dbgz_problem_truncate_band(dbgz_problem *p, int64_t bandwidth);
+
 /* Reads back the factorisation held by a prepared problem: U (d x d,
  * upper triangle meaningful, as CholeskyGenz.U), perm, permuted and scaled
  * a and b, scale_vec, rank (src/cholesky.jl:5-14).  Any pointer may be

@@ -298,3 +298,55 @@ def test_identity_known_answer_tensor_core(D, prec):
                   precision=prec)
     P, err, _ = D.qmc_pnorm(Q)
     assert abs(P - 0.25) < 1e-6
+
+
+# ---------------------------------------------------------- sparse / banded ---
+def test_pnorm_sparse_fixture(D):
+    z = np.load(os.path.join(GOLD, "oracle_cases.npz"))
+    g = _case(z, "tridiag8")
+    Q = _from_case(D, g)
+    P, err, npts, reps = D.qmc_pnorm(Q, return_reps=True)
+    assert npts == int(g["n_pts"])
+    np.testing.assert_allclose(reps, g["reps"], rtol=1e-12, atol=1e-300)
+    Q32 = _from_case(D, g, np.float32, precision=L.PREC_FP32_SIMT)
+    P32 = D.qmc_pnorm(Q32)[0]
+    assert abs(P32 - float(g["P"])) <= 2e-6 + 1e-5 * abs(float(g["P"]))
+
+
+def _ar1(n, rho=0.9):
+    i = np.arange(n)
+    return rho ** np.abs(i[:, None] - i[None, :])
+
+
+@pytest.mark.parametrize("n,band,qmc", [(60, None, "Richtmyer"), (300, 16, "Richtmyer"),
+                                         (300, 64, "Sobol"), (600, None, "Richtmyer")])
+def test_pnorm_sparse_vs_checker(D, oracle, n, band, qmc):
+    # classic factor, CSC of the strict upper triangle (optionally band-limited);
+    # n = 600 without a band exceeds the shared-memory ring (global ring path)
+    S = _spd(n, n) if band is None else _ar1(n)
+    rng = np.random.default_rng(n + 1)
+    a = np.full(n, -np.inf) if band else W.bounds_quarter(S)[0]
+    b = rng.uniform(-0.5, 2.5, n) if band else W.bounds_quarter(S)[1]
+    m, n_reps = 500, 3
+    kw = {}
+    if qmc == "Richtmyer":
+        kw["shifts"] = rng.random((n - 1, n_reps))
+    else:
+        kw["ushifts"] = rng.integers(0, 2**64, size=(n - 1, n_reps), dtype=np.uint64)
+    Q = D.QMCDataSparse(S, a, b, D.QMC_opts(m=m, n_reps=n_reps, max_pts=m, max_abs_err=0.0), qmc_type=qmc, **kw)
+    if band:
+        Q.truncate_band(band)
+    F = Q.C
+    U = F.U.copy()
+    if band:
+        assert np.all(np.triu(U, band + 1) == 0)
+    P, err, npts, reps = D.qmc_pnorm(Q, precision=L.PREC_FP64, return_reps=True)
+    okw = dict(m=m, n_reps=n_reps, sparse=True, max_pts=m)
+    if qmc == "Richtmyer":
+        okw["shifts"] = kw["shifts"]
+    else:
+        okw.update(qmc_type=oracle.SOBOL, V=D.sobol_dirnums(n - 1), ushifts=kw["ushifts"], sobol_first=Q.sobol_first)
+    Pc, ec, nc, rc = oracle.qmc_pnorm(U, F.a, F.b, **okw)
+    np.testing.assert_allclose(reps, rc, rtol=1e-12, atol=1e-300)
+    P32, _, _, r32 = D.qmc_pnorm(Q, precision=L.PREC_FP32_SIMT, return_reps=True)
+    assert abs(P32 - Pc) <= 5e-6 + 2e-5 * abs(Pc), (P32, Pc)
