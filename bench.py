@@ -287,6 +287,22 @@ def main():
             continue
         (Po, _, _, _), mso, lo_ms, _, _ = timed(Q, D.PRECISIONS[name], max(2, args.steps // 2), 1)
         other[name] = {"ms_per_step": mso, "loop_ms": lo_ms, "P": Po}
+
+    # gradient: estimate + adjoint on the same points (dbgz_pnorm_grad), timed
+    # on the device like the forward step (host-side D2H of dU included)
+    def grad_step(Qg, precision):
+        flush.zero_()
+        torch.cuda.synchronize()
+        r = D.qmc_pnorm_grad(Qg, precision=precision)
+        lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+        return r, prof.pnorm_ms, prof.kernel_launches
+
+    grad_step(Q, prec_mixed)
+    kg = max(2, args.steps // 2)
+    g_ms = [grad_step(Q, prec_mixed)[1] for _ in range(kg)]
+    grad = {"precision": args.precision, "ms_per_step": statistics.mean(g_ms),
+            "over_fwd": statistics.mean(g_ms) / ms_mix, "steps": kg,
+            "outputs": "P, dP/da, dP/db (original order), dP/dU (factor coordinates)"}
     # accuracy where P is O(0.1): the same covariance with the reference's own
     # bound design (+-k sqrt(S_ii), P(independent) = 0.25), same points
     from dbgenzpaper_b200 import workloads as W
@@ -298,6 +314,12 @@ def main():
     for name in ("fp32_split_bf16", "fp32_tf32", "fp32_simt"):
         Pm = D.qmc_pnorm(Qq, precision=D.PRECISIONS[name])[0]
         acc[name] = {"P": Pm, "abs_err": abs(Pm - acc["P_fp64"]), "rel_err": abs(Pm - acc["P_fp64"]) / acc["P_fp64"]}
+    g64 = D.qmc_pnorm_grad(Qq, precision=L.PREC_FP64)
+    gm = D.qmc_pnorm_grad(Qq, precision=prec_mixed)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    acc["grad_" + args.precision] = {"rel_err_dP_da": rel(gm[3], g64[3]), "rel_err_dP_db": rel(gm[4], g64[4]),
+                                     "rel_err_dP_dU": rel(gm[5], g64[5]), "norm": "Frobenius, vs FP64 adjoint"}
+    del g64, gm
     Qq.close()
 
     # e2e: the public API from host buffers, upload and factorisation included
@@ -343,6 +365,7 @@ def main():
             "rel_err_vs_fp64": abs(P_mix - P64) / abs(P64) if P64 else None,
             "qmc_3sem": err_mix,
             "other_modes": other,
+            "grad": grad,
             "accuracy_quarter_bounds": acc,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if w.samples == 2**21 else None,

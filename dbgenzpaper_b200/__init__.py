@@ -41,7 +41,7 @@ from . import _lib as L
 
 __all__ = [
     "QMCOpts", "QMC_opts", "QMCData", "QMCDataSparse", "QMCData_Distributions",
-    "qmc_pnorm", "CholeskyGenz", "cholesky_genz", "cholesky_classic",
+    "qmc_pnorm", "qmc_pnorm_grad", "CholeskyGenz", "cholesky_genz", "cholesky_classic",
     "get_sqrt_primes", "richtmyer_mat", "sobol_mat", "sobol_dirnums", "Context",
     "get_context", "DbgzError", "PRECISIONS",
 ]
@@ -289,6 +289,23 @@ def qmc_pnorm(D, use_AppleBLAS=None, *, precision: Optional[int] = None, return_
     L.check(st, base.ctx.handle)
     out = (res.value, err.value, int(npts.value))
     return out + (reps,) if return_reps else out
+
+
+def qmc_pnorm_grad(D, *, precision: Optional[int] = None, want_U: bool = True):
+    """Estimate and exact gradient on the current point set (no counterpart
+    in the reference): -> (P, err, n_pts, dP_da, dP_db, dP_dU).
+
+    dP_da/dP_db are in the original variable order and scale; dP_dU is with
+    respect to the factor in the permuted, scaled coordinates of ``D.C``."""
+    base = D.D if isinstance(D, QMCData_Distributions) else D
+    prec = base.resolved_precision() if precision is None else int(precision)
+    n = base.n
+    res, err, npts = C.c_double(), C.c_double(), C.c_int64()
+    da, db = np.zeros(n), np.zeros(n)
+    dU = np.zeros((n, n), order="F") if want_U else None
+    L.check(L.lib().dbgz_pnorm_grad(base.handle, prec, C.byref(res), C.byref(err), C.byref(npts), L.ptr(da),
+                                    L.ptr(db), L.ptr(dU)), base.ctx.handle)
+    return res.value, err.value, int(npts.value), da, db, dU
 
 
 # ---- primitives -------------------------------------------------------------

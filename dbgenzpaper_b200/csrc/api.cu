@@ -416,7 +416,7 @@ int dbgz_problem_factor(const dbgz_problem *p, double *U, int64_t *perm, double 
   return DBGZ_OK;
 }
 
-static int first_dim_cdf(dbgz_problem *p) {
+int dbgz_first_dim_cdf(dbgz_problem *p) {
   if (p->c1_ready) return DBGZ_OK;
   dbgz_ctx *ctx = p->ctx;
   double a0, b0, u00;
@@ -456,7 +456,7 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
   cudaSetDevice(ctx->device);
   const dbgz_opts &o = p->opts;
   const int64_t n_reps = o.n_reps, m = o.m;
-  DBGZ_TRY(first_dim_cdf(p));
+  DBGZ_TRY(dbgz_first_dim_cdf(p));
   if (precision != DBGZ_PREC_FP64 && !p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
   const int64_t tps = (m + 127) / 128;
   const int64_t n_tiles = tps * n_reps;

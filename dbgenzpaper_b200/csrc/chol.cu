@@ -313,6 +313,14 @@ __global__ void k_band(double *U, int64_t d, int64_t band) {
     U[t * d + l] = 0.0;
 }
 
+// Ub[i + j d] = U[(d-1-j) + (d-1-i) d]: the anti-transpose (coefficients of
+// the adjoint recurrence, policies.cuh)
+__global__ void k_anti_transpose(const double *U, int64_t d, double *Ub) {
+  const int64_t j = blockIdx.y;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < d; i += (int64_t)gridDim.x * blockDim.x)
+    Ub[j * d + i] = U[(d - 1 - i) * d + (d - 1 - j)];
+}
+
 __global__ void k_targets(const double *U, int64_t n, const double *a, const double *b,
                           TargetParams64 *t64, TargetParams32 *t32) {
   int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -507,6 +515,21 @@ int dbgz_make_U32(dbgz_problem *p) {
   int blocks = (int)std::min<int64_t>((nn + 255) / 256, 4096);
   k_to_f32<<<blocks, 256, 0, ctx->stream>>>((const double *)p->U.p, (float *)p->U32.p, nn);
   dbgz_count_launch(p->ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
+}
+
+int dbgz_make_Ub(dbgz_problem *p) {
+  dbgz_ctx *ctx = p->ctx;
+  const int64_t d = p->d, nn = d * d;
+  DBGZ_TRY(dbgz_ensure(ctx, p->Ub, sizeof(double) * nn));
+  DBGZ_TRY(dbgz_ensure(ctx, p->Ub32, sizeof(float) * nn));
+  dim3 g((unsigned)((d + 255) / 256), (unsigned)d);
+  k_anti_transpose<<<g, 256, 0, ctx->stream>>>((const double *)p->U.p, d, (double *)p->Ub.p);
+  dbgz_count_launch(ctx);
+  int blocks = (int)std::min<int64_t>((nn + 255) / 256, 4096);
+  k_to_f32<<<blocks, 256, 0, ctx->stream>>>((const double *)p->Ub.p, (float *)p->Ub32.p, nn);
+  dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   return DBGZ_OK;
 }

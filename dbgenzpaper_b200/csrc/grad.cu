@@ -1,0 +1,211 @@
+// grad.cu -- dbgz_pnorm_grad: the estimate and its adjoint on one point set.
+//
+// No counterpart in the reference (it has no gradient).  One pass of m
+// points x n_reps shifts runs the forward loop with the STORE policy
+// (y_l, s_t, dc_t and p of every sample kept in HBM, [index][sample]), then
+// the same loop kernel runs the adjoint recurrence on the anti-transposed
+// factor (policies.cuh).  Per-variable terms (dP/da_t, dP/db_t, dP/dU_tt)
+// come out as per-(tile, warp) partial sums reduced here in a fixed order;
+// the off-diagonal dP/dU[l, t] = mean over samples of y_l * (p sbar_t) is one
+// plain GEMM of the two stored arrays (cuBLAS: FP64 DGEMM for the FP64 path,
+// TF32 tensor-core GEMM with FP32 accumulation for the FP32 paths).
+#include <cublas_v2.h>
+
+#include <cmath>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace {
+
+// sum over rows (tile * 4 + warp) of part[row * d + t], rows in order
+__global__ void k_reduce_partials(const double *ga, const double *gb, const double *gu, int64_t rows, int64_t d,
+                                  double *out) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= d) return;
+  double a = 0.0, b = 0.0, u = 0.0;
+  for (int64_t r = 0; r < rows; ++r) {
+    a += ga[r * d + t];
+    b += gb[r * d + t];
+    u += gu[r * d + t];
+  }
+  out[t] = a;
+  out[d + t] = b;
+  out[2 * d + t] = u;
+}
+
+struct CublasHandle {
+  cublasHandle_t h = nullptr;
+  int device = -1;
+  ~CublasHandle() {
+    if (h) cublasDestroy(h);
+  }
+};
+thread_local CublasHandle g_cublas;
+
+int get_cublas(dbgz_ctx *ctx, cublasHandle_t *out) {
+  if (!g_cublas.h || g_cublas.device != ctx->device) {
+    if (g_cublas.h) cublasDestroy(g_cublas.h);
+    g_cublas.h = nullptr;
+    if (cublasCreate(&g_cublas.h) != CUBLAS_STATUS_SUCCESS)
+      return dbgz_fail(ctx, DBGZ_ERR_CUDA, "cublasCreate failed");
+    g_cublas.device = ctx->device;
+  }
+  if (cublasSetStream(g_cublas.h, ctx->stream) != CUBLAS_STATUS_SUCCESS)
+    return dbgz_fail(ctx, DBGZ_ERR_CUDA, "cublasSetStream failed");
+  *out = g_cublas.h;
+  return DBGZ_OK;
+}
+
+}  // namespace
+
+extern "C" int dbgz_first_dim_cdf(dbgz_problem *p);  // api.cu
+
+extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, double *err, int64_t *n_pts,
+                               double *dP_da, double *dP_db, double *dP_dU) {
+  if (!p || !result || !err || !n_pts) return DBGZ_ERR_INVALID_ARGUMENT;
+  dbgz_ctx *ctx = p->ctx;
+  if (precision < DBGZ_PREC_FP64 || precision > DBGZ_PREC_FP32_SIMT)
+    return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "pnorm_grad: bad precision %d", precision);
+  if (p->structure != DBGZ_STRUCTURE_DENSE)
+    return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm_grad: the adjoint is built for the dense structure");
+  if (p->cdf_form != DBGZ_CDF_ERF)
+    return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm_grad: the adjoint is built for the erf-form CDF");
+  cudaSetDevice(ctx->device);
+  const dbgz_opts &o = p->opts;
+  const int64_t d = p->d, m = o.m, n_reps = o.n_reps;
+  const int64_t tps = (m + 127) / 128, n_tiles = tps * n_reps, N = n_tiles * 128;
+  const size_t esz = precision == DBGZ_PREC_FP64 ? 8 : 4;
+  DBGZ_TRY(dbgz_first_dim_cdf(p));
+  if (precision != DBGZ_PREC_FP64 && !p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
+  if (!p->Ub.p) DBGZ_TRY(dbgz_make_Ub(p));
+  // one allocation for the pass: 4 state arrays, p, 3 partial arrays, sums, dU
+  const size_t arr = esz * (size_t)d * N;
+  const size_t part = sizeof(double) * (size_t)n_tiles * 4 * d;
+  const size_t total = 4 * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d + esz * (size_t)d * d + 4096;
+  DBGZ_TRY(dbgz_ensure(ctx, p->grad_buf, total));
+  char *base = (char *)p->grad_buf.p;
+  auto take = [&](size_t bytes) {
+    char *r = base;
+    base += (bytes + 255) & ~size_t(255);
+    return r;
+  };
+  GradArrays ga;
+  ga.N = N;
+  ga.y = take(arr);
+  ga.s = take(arr);
+  ga.dc = take(arr);
+  ga.sbar = take(arr);
+  ga.p = (double *)take(8 * (size_t)N);
+  ga.ga = (double *)take(part);
+  ga.gb = (double *)take(part);
+  ga.gu = (double *)take(part);
+  ga.dc1 = p->dc1;
+  double *sums = (double *)take(3 * 8 * (size_t)d);
+  void *dU = take(esz * (size_t)d * d);
+  // rows the passes leave unwritten enter the dU GEMM: clear them
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync((char *)ga.y + esz * (size_t)(d - 1) * N, 0, esz * N, ctx->stream));
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ga.sbar, 0, esz * N, ctx->stream));
+
+  DBGZ_TRY(dbgz_ensure(ctx, p->partials, sizeof(double) * n_tiles));
+  DBGZ_TRY(dbgz_ensure(ctx, p->reps, sizeof(double) * n_reps));
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(p->reps.p, 0, sizeof(double) * n_reps, ctx->stream));
+  const bool prof = ctx->profiling;
+  const int64_t launches0 = ctx->launch_count;
+  if (prof) cudaEventRecord(ctx->ev[0], ctx->stream);
+
+  PassArgs pa{};
+  pa.d = d;
+  pa.m = m;
+  pa.n_reps = n_reps;
+  pa.sobol_first = p->sobol_first;
+  pa.n_bits = (int)o.n_bits;
+  pa.qmc_type = p->qmc_type;
+  pa.cdf_form = p->cdf_form;
+  pa.c1 = p->c1;
+  pa.dc1 = p->dc1;
+  pa.gen_base = p->gen_base;
+  pa.grad = ga;
+  const bool tensor = precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16;
+  // forward, keeping the state
+  pa.kind = kLoopForwardStore;
+  if (tensor) DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
+  else DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
+  DBGZ_TRY(dbgz_finalize_pass(p, (const double *)p->partials.p, tps, 0, m, (double *)p->reps.p));
+  // adjoint on the anti-transposed factor
+  pa.kind = kLoopAdjoint;
+  if (tensor) DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
+  else DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
+  k_reduce_partials<<<(unsigned)((d + 127) / 128), 128, 0, ctx->stream>>>(ga.ga, ga.gb, ga.gu, n_tiles * 4, d, sums);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  // dU[l, t] = sum_n y[l][n] (p sbar)[t][n]: (d x N) x (N x d), sample-contiguous rows
+  if (dP_dU) {
+    cublasHandle_t h;
+    DBGZ_TRY(get_cublas(ctx, &h));
+    cublasStatus_t cs;
+    if (precision == DBGZ_PREC_FP64) {
+      const double one = 1.0, zero = 0.0;
+      cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, (int)N, &one, (const double *)ga.y, (int)N,
+                       (const double *)ga.sbar, (int)N, &zero, (double *)dU, (int)d);
+    } else {
+      const float one = 1.0f, zero = 0.0f;
+      cs = cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, (int)N, &one, ga.y, CUDA_R_32F, (int)N,
+                        ga.sbar, CUDA_R_32F, (int)N, &zero, dU, CUDA_R_32F, (int)d, CUBLAS_COMPUTE_32F_FAST_TF32,
+                        CUBLAS_GEMM_DEFAULT);
+    }
+    if (cs != CUBLAS_STATUS_SUCCESS) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
+  }
+  std::vector<double> reps(n_reps), hs(3 * d), scale(d), hU;
+  std::vector<int64_t> perm(d);
+  int dev_status = 0;
+  cudaMemcpyAsync(reps.data(), p->reps.p, 8 * n_reps, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(hs.data(), sums, 8 * 3 * d, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(perm.data(), p->perm.p, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(scale.data(), p->scale.p, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
+  if (tensor) cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (dP_dU) {
+    hU.resize((size_t)d * d * (esz / 4));
+    cudaMemcpyAsync(hU.data(), dU, esz * (size_t)d * d, cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  if (prof) cudaEventRecord(ctx->ev[1], ctx->stream);
+  DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (dev_status != 0)
+    return dbgz_fail(ctx, DBGZ_ERR_TIMEOUT, "pnorm_grad: a bounded wait in the tensor-core loop gave up");
+  if (prof) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->prof.pnorm_ms = ms;
+    ctx->prof.kernel_launches = ctx->launch_count - launches0;
+    ctx->prof.loop_launches = 2;
+  }
+  double res = 0.0;
+  for (double v : reps) res += v;
+  res /= (double)n_reps;
+  double acc = 0.0;
+  for (double v : reps) acc += (v - res) * (v - res) / (double)n_reps;
+  *result = res;
+  *err = 3.0 * std::sqrt(acc / (double)(n_reps - 1));
+  *n_pts = m;
+  const double inv = 1.0 / ((double)m * (double)n_reps);
+  for (int64_t t = 0; t < d; ++t) {
+    const int64_t orig = perm[t];
+    if (dP_da) dP_da[orig] = hs[t] * inv / scale[orig];
+    if (dP_db) dP_db[orig] = hs[d + t] * inv / scale[orig];
+  }
+  if (dP_dU) {
+    for (int64_t t = 0; t < d; ++t)
+      for (int64_t l = 0; l < d; ++l) {
+        double v = 0.0;
+        if (l < t) {
+          const size_t ix = (size_t)t * d + l;  // column t, row l of the GEMM result
+          v = (esz == 8 ? reinterpret_cast<const double *>(hU.data())[ix]
+                        : (double)reinterpret_cast<const float *>(hU.data())[ix]) * inv;
+        } else if (l == t) {
+          v = hs[2 * d + t] * inv;
+        }
+        dP_dU[(size_t)t * d + l] = v;
+      }
+  }
+  return DBGZ_OK;
+}

@@ -74,6 +74,11 @@ struct dbgz_problem {
   DevBuf tgt64, tgt32, U32;
   DevBuf Uhi, Ulo, Utf;  // tensor-core operands of the contraction
   int64_t ldU = 0;       // padded leading dimension of Uhi/Ulo/Utf
+  // the same for the anti-transposed factor Ub[i, j] = U[d-1-j, d-1-i]
+  // (coefficients of the adjoint recurrence, policies.cuh)
+  DevBuf Ub, Ub32, Ubhi, Ublo, Ubtf;
+  int64_t ldUb = 0;
+  DevBuf grad_buf;       // forward state and partial gradients of dbgz_pnorm_grad
   // sparse (banded) structure: CSC of the strict upper factor
   DevBuf csc_colptr, csc_row, csc_val64, csc_val32;
   int64_t nnz = 0, bandwidth = 0, band = 0;  // band > 0: entries beyond it dropped
@@ -93,6 +98,7 @@ int dbgz_truncate_dev(dbgz_ctx *ctx, int64_t n, double *U, double eps_T);
 int dbgz_make_targets(dbgz_problem *p);
 int dbgz_band_dev(dbgz_ctx *ctx, int64_t d, double *U, int64_t band);
 int dbgz_make_U32(dbgz_problem *p);
+int dbgz_make_Ub(dbgz_problem *p);
 
 // ---- points (points.cu) --------------------------------------------------
 int dbgz_richtmyer_dev(dbgz_ctx *ctx, int64_t m, int64_t n, const double *q, int64_t n0,
@@ -101,7 +107,21 @@ int dbgz_sobol_dev(dbgz_ctx *ctx, int64_t m, int64_t dims, const uint32_t *V, in
                    uint32_t *X);
 
 // ---- integration loop (loop_simt.cu) ---------------------------------------
+// Which sequential step the loops run (policies.cuh).
+enum LoopKind { kLoopForward = 0, kLoopForwardStore = 1, kLoopAdjoint = 2 };
+
+// Forward state kept for the adjoint and the adjoint's outputs (device
+// arrays; element type float or double per precision).
+struct GradArrays {
+  int64_t N = 0;  // samples of the pass (n_tiles * 128)
+  void *y = nullptr, *s = nullptr, *dc = nullptr, *sbar = nullptr;
+  double *p = nullptr, *ga = nullptr, *gb = nullptr, *gu = nullptr;
+  double dc1 = 0.0;
+};
+
 struct PassArgs {
+  int kind = kLoopForward;
+  GradArrays grad;
   int64_t d;
   int64_t m;          // points per pass
   int64_t n_reps;

@@ -28,7 +28,7 @@ using namespace simt;
 
 namespace {
 
-template <typename T, typename Step>
+template <typename T, typename Policy>
 int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
   dbgz_ctx *ctx = p->ctx;
   const int64_t d = pa.d;
@@ -53,15 +53,26 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.up1 = 1.0 - pa.c1 - pa.dc1;
   P.cdf_form = pa.cdf_form;
   P.partials = partials;
+  const bool adj = pa.kind == kLoopAdjoint;
   if (sizeof(T) == 8) {
-    P.U = (const T *)p->U.p;
+    P.U = (const T *)(adj ? p->Ub.p : p->U.p);
     P.tgt = (const typename TgtOf<T>::type *)p->tgt64.p;
   } else {
-    P.U = (const T *)p->U32.p;
+    P.U = (const T *)(adj ? p->Ub32.p : p->U32.p);
     P.tgt = (const typename TgtOf<T>::type *)p->tgt32.p;
   }
+  P.io.N = pa.grad.N;
+  P.io.y = (T *)pa.grad.y;
+  P.io.s = (T *)pa.grad.s;
+  P.io.dc = (T *)pa.grad.dc;
+  P.io.sbar = (T *)pa.grad.sbar;
+  P.io.p = pa.grad.p;
+  P.io.ga = pa.grad.ga;
+  P.io.gb = pa.grad.gb;
+  P.io.gu = pa.grad.gu;
+  P.io.dc1 = pa.grad.dc1;
   const size_t smem = sizeof(SimtSmem<T>);
-  auto kern = k_genz_simt<T, Step>;
+  auto kern = k_genz_simt<T, Policy>;
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   DBGZ_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
@@ -75,13 +86,27 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   return DBGZ_OK;
 }
 
+template <typename T, int GEN>
+int launch_kind(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
+  switch (pa.kind) {
+    case kLoopForwardStore: return launch_simt<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
+    case kLoopAdjoint: return launch_simt<T, pol::Adjoint<T, GEN>>(p, pa, partials, n_tiles);
+    default: return launch_simt<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
+  }
+}
+
+template <typename T>
+int launch_gen(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
+  if (pa.qmc_type == DBGZ_QMC_SOBOL) return launch_kind<T, DBGZ_QMC_SOBOL>(p, pa, partials, n_tiles);
+  return launch_kind<T, DBGZ_QMC_RICHTMYER>(p, pa, partials, n_tiles);
+}
+
 }  // namespace
 
 int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles) {
-  if (precision == DBGZ_PREC_FP64)
-    return launch_simt<double, dbgz::StepFp64>(p, pa, partials, n_tiles);
-  return launch_simt<float, dbgz::StepFp32>(p, pa, partials, n_tiles);
+  if (precision == DBGZ_PREC_FP64) return launch_gen<double>(p, pa, partials, n_tiles);
+  return launch_gen<float>(p, pa, partials, n_tiles);
 }
 
 int dbgz_finalize_pass(dbgz_problem *p, const double *partials, int64_t tiles_per_shift,

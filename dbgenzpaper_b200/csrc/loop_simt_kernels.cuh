@@ -4,6 +4,7 @@
 #pragma once
 #include "internal.cuh"
 #include "genz_step.cuh"
+#include "policies.cuh"
 
 namespace simt {
 
@@ -28,12 +29,13 @@ template <typename T>
 struct SimtParams {
   int64_t d, m, n_reps, tiles_per_shift, n_tiles, Dp;
   dbgz::GenParams gen;
-  const T *U;  // d x d col-major
+  const T *U;  // d x d col-major coefficient array (policies.cuh)
   const typename TgtOf<T>::type *tgt;
   double c1, dc1, up1;
   int cdf_form;
   T *yws;            // gridDim.x slots of Dp x TS
   double *partials;  // n_tiles
+  pol::GradIO<T> io;
 };
 
 template <typename T>
@@ -44,27 +46,15 @@ struct SimtSmem {
       T Ys[KC][TS];
       T Us[KC][G + 4];
     } gemm;
-    T Ysub[SB][TS];           // y's of the last sub-block
+    T Ysub[SB][TS];           // emitted values of the last sub-block
   } u;
-  T Ublk[SB][SB + 1];         // U of the sub-block (and of the cross block)
-  double qv[SB];
-  T shv[SB];
-  typename TgtOf<T>::type tg[SB];
+  T Ublk[SB][SB + 1];         // coefficients of the sub-block (and of the cross block)
+  pol::Staged<T> sg;
   double red[NT / 32];
 };
 
-template <typename T>
-__device__ __forceinline__ T shift_at(const dbgz::GenParams &g, int64_t idx);
-template <>
-__device__ __forceinline__ double shift_at<double>(const dbgz::GenParams &g, int64_t idx) {
-  return g.shift64 ? g.shift64[idx] : 0.0;
-}
-template <>
-__device__ __forceinline__ float shift_at<float>(const dbgz::GenParams &g, int64_t idx) {
-  return g.shift32 ? g.shift32[idx] : 0.0f;
-}
-
-template <typename T, typename Step>
+// Policy: pol::Forward<...> or pol::Adjoint<...> (policies.cuh).
+template <typename T, typename Policy>
 __global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SimtSmem<T> &sm = *reinterpret_cast<SimtSmem<T> *>(smem_raw);
@@ -74,16 +64,15 @@ __global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
   const int64_t last_g0 = ((nY - 1) / G) * G;  // start of the last group
 
   for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
-    const int64_t k = tile / P.tiles_per_shift;
-    const int64_t jt = tile - k * P.tiles_per_shift;
     const int r = tid;  // sample row for the scalar threads (tid < TS)
-    const int64_t j = jt * TS + r;
-    Step st;
-    st.init(P.c1, P.dc1, P.up1);
+    const int64_t k = tile / P.tiles_per_shift;
+    const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
+    Policy pl;
+    if (tid < TS) pl.tile_begin(P.gen, d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, P.cdf_form, P.io);
 
     for (int64_t g0 = 0; g0 < nY; g0 += G) {
       const int ng = (int)(nY - g0 < (int64_t)G ? nY - g0 : (int64_t)G);
-      // ---- group GEMM: Ss[t][r] = sum_{l<g0} Y[l][r] U[l][g0+1+t] ----
+      // ---- group GEMM: Ss[t][r] = sum_{l<g0} V[l][r] C[l][g0+t] ----
       {
         const int tx = tid & 15, ty = tid >> 4;
         T acc[8][4];
@@ -130,39 +119,30 @@ __global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
       for (int sb = 0; sb < ng; sb += SB) {
         const int nsb = min(SB, ng - sb);
         const int64_t l_base = g0 + sb;
-        // stage U of the sub-block and the per-dimension parameters
         for (int e = tid; e < SB * SB; e += NT) {
           int li = e % SB, ti = e / SB;
           int64_t l = l_base + li, t = l_base + ti + 1;
           sm.Ublk[li][ti] = (li <= ti && li < nsb && ti < nsb) ? P.U[t * d + l] : T(0);
         }
-        if (tid < SB) {
-          int64_t l = l_base + tid;
-          if (tid < nsb) {
-            sm.qv[tid] = P.gen.q ? P.gen.q[l] : 0.0;
-            sm.shv[tid] = shift_at<T>(P.gen, k * nY + l);
-            sm.tg[tid] = P.tgt[l + 1];
-          }
-        }
+        if (tid < TS) pl.stage(sm.sg, P.tgt, tid, l_base, nsb);
         __syncthreads();
         if (tid < TS) {
           // in-block dot in the reference's order (src/qmc.jl:394-403):
-          // acc = S[target] + y_{l_base} U[..] + ... + y_l U[l, l+1]
+          // acc = S[target] + v_{l_base} C[..] + ... + v_l C[l, l]
 #pragma unroll 1
           for (int li = 0; li < nsb; ++li) {
             const int64_t l = l_base + li;
-            T y = st.quantile(P.gen, d, j, k, l, sm.qv[li], sm.shv[li]);
-            sm.u.Ysub[li][r] = y;
-            if (g0 < last_g0) Yw[l * TS + r] = y;
+            T v = pl.emit(sm.sg, li, l);
+            sm.u.Ysub[li][r] = v;
+            if (g0 < last_g0) Yw[l * TS + r] = v;
             T acc = sm.Ss[sb + li][r];
 #pragma unroll 4
             for (int mi = 0; mi <= li; ++mi) acc = fma(sm.u.Ysub[mi][r], sm.Ublk[mi][li], acc);
-            const auto tg = sm.tg[li];
-            st.cdf(acc, tg.a, tg.b, tg.inv_u, P.cdf_form);
+            pl.consume(sm.sg, acc, li, l);
           }
         }
         __syncthreads();
-        // cross update: Ss[sb+SB+t][r] += sum_li Ysub[li][r] U[l_base+li][l_base+SB+1+t]
+        // cross update: Ss[sb+SB+t][r] += sum_li Ysub[li][r] C[l_base+li][l_base+SB+t]
         if (sb + SB < ng) {
           const int nt2 = min(SB, ng - sb - SB);
           for (int e = tid; e < SB * SB; e += NT) {
@@ -183,8 +163,9 @@ __global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
         }
       }
     }
-    // ---- per-tile sum of p (fixed order) ----
-    double pv = (tid < TS && j < P.m) ? st.p : 0.0;
+    // ---- per-tile end and sum of p (fixed order) ----
+    if (tid < TS) pl.tile_end(P.tgt, tid, 0, tile, j < P.m);
+    double pv = (tid < TS) ? pl.tile_value(j < P.m) : 0.0;
     for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
     if ((tid & 31) == 0) sm.red[tid >> 5] = pv;
     __syncthreads();

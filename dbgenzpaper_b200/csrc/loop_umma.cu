@@ -32,6 +32,7 @@
 #include "internal.cuh"
 #include "genz_step.cuh"
 #include "sm100.cuh"
+#include "policies.cuh"
 
 namespace {
 
@@ -67,6 +68,7 @@ struct __align__(64) UmmaParams {
   double c1, dc1, up1;
   double *partials;
   int *status;
+  pol::GradIO<float> io;
 };
 
 struct Phase {
@@ -100,10 +102,8 @@ struct Smem {
 };
 
 struct Misc {
-  float ublk[BK][2 * BK + 1];  // U of the block's triangle, zero beyond column BK
-  TargetParams32 tg[BK];
-  double qv[BK];
-  float shv[BK];
+  float ublk[BK][2 * BK + 1];  // coefficients of the block's triangle, zero beyond column BK
+  pol::Staged<float> sg;
   double red[4];
   uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
   uint32_t tmem_base;
@@ -133,7 +133,8 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return t;
 }
 
-template <int MODE, int GEN>
+// Policy: pol::Forward<float, GEN, STORE> or pol::Adjoint<float, GEN>.
+template <int MODE, typename Policy>
 __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ UmmaParams P) {
   using F = Fmt<MODE>;
   using SM = Smem<MODE>;
@@ -339,10 +340,8 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       const int64_t k_shift = tile / P.tiles_per_shift;
       const int64_t jt = tile - k_shift * P.tiles_per_shift;
       const int64_t j = jt * TS + r;
-      dbgz::StepFp32 st;
-      st.init(P.c1, P.dc1, P.up1);
-      dbgz::GenParams gen = P.gen;
-      gen.qmc_type = GEN;  // compile-time generator: only one point path in the code
+      Policy pl;
+      pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
       for (int64_t ph = 0; ph < nphase; ++ph) {
         const Phase f = phase_of(P, ph);
         if (ph > 0) {
@@ -362,11 +361,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
             ms->ublk[li][ti] =
                 (li <= ti && ti < nval) ? P.U32[(lbase + ti + 1) * P.d + lbase + li] : 0.f;
           }
-          if (r < BK && r < nval) {
-            ms->tg[r] = P.tgt[lbase + r + 1];
-            ms->qv[r] = P.gen.q ? P.gen.q[lbase + r] : 0.0;
-            ms->shv[r] = P.gen.shift32 ? P.gen.shift32[k_shift * P.nY + lbase + r] : 0.f;
-          }
+          pl.stage(ms->sg, P.tgt, r, lbase, nval);
           // partial sums of the block's targets, accumulated by the tensor cores
           float s[BK];
           bool ok = true;
@@ -404,12 +399,11 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 float y = 0.f;
                 if (li < nval) {
                   const int64_t l = lbase + li;
-                  y = st.quantile(gen, P.d, j, k_shift, l, ms->qv[li], ms->shv[li]);
+                  y = pl.emit(ms->sg, li, l);
                   const float *urow = &ms->ublk[li][8 * ch];
 #pragma unroll
                   for (int t = k; t < BK; ++t) s[t] = fmaf(y, urow[t], s[t]);
-                  const TargetParams32 tg = ms->tg[li];
-                  st.cdf(s[k], tg.a, tg.b, tg.inv_u, 0);
+                  pl.consume(ms->sg, s[k], li, l);
                 }
                 ys[k] = y;
               }
@@ -459,9 +453,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           ++ja;
         }
       }
-      // per-tile sum of p in a fixed order
+      // per-tile end and sum of p in a fixed order
       {
-        double pv = (j < P.m) ? st.p : 0.0;
+        pl.tile_end(P.tgt, r, warp, tile, j < P.m);
+        double pv = pl.tile_value(j < P.m);
         for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
         if (lane == 0) ms->red[warp] = pv;
         named_sync(kBarScalar, TS);
@@ -530,6 +525,19 @@ int encode_2d(dbgz_ctx *ctx, CUtensorMap *m, void *base, uint64_t inner, uint64_
   return DBGZ_OK;
 }
 
+template <int MODE, int GEN>
+auto pick_kind(const PassArgs &pa) -> decltype(&k_genz_umma<MODE, pol::Forward<float, GEN, false>>) {
+  switch (pa.kind) {
+    case kLoopForwardStore: return k_genz_umma<MODE, pol::Forward<float, GEN, true>>;
+    case kLoopAdjoint: return k_genz_umma<MODE, pol::Adjoint<float, GEN>>;
+    default: return k_genz_umma<MODE, pol::Forward<float, GEN, false>>;
+  }
+}
+template <int MODE>
+auto pick_kernel(const PassArgs &pa) -> decltype(pick_kind<MODE, 0>(pa)) {
+  return pa.qmc_type == DBGZ_QMC_SOBOL ? pick_kind<MODE, DBGZ_QMC_SOBOL>(pa) : pick_kind<MODE, DBGZ_QMC_RICHTMYER>(pa);
+}
+
 template <int MODE>
 int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
   using F = Fmt<MODE>;
@@ -537,22 +545,28 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   dbgz_ctx *ctx = p->ctx;
   const int64_t d = pa.d, nY = d - 1;
   const int64_t Dp = ((nY + 63) / 64) * 64;
-  // converted factor (built on first use for this precision)
-  DevBuf &u0 = MODE == DBGZ_PREC_FP32_TF32 ? p->Utf : p->Uhi;
-  if (!u0.p || p->ldU != Dp) {
-    p->ldU = Dp;
+  // converted coefficients (built on first use for this precision): the
+  // factor, or its anti-transpose for the adjoint
+  const bool adj = pa.kind == kLoopAdjoint;
+  if (adj && !p->Ub.p) DBGZ_TRY(dbgz_make_Ub(p));
+  DevBuf &src = adj ? p->Ub : p->U;
+  DevBuf &u0 = MODE == DBGZ_PREC_FP32_TF32 ? (adj ? p->Ubtf : p->Utf) : (adj ? p->Ubhi : p->Uhi);
+  DevBuf &u1 = adj ? p->Ublo : p->Ulo;
+  int64_t &ld = adj ? p->ldUb : p->ldU;
+  if (!u0.p || ld != Dp || (F::NPART > 1 && !u1.p)) {
+    ld = Dp;
     DBGZ_TRY(dbgz_ensure(ctx, u0, (size_t)d * Dp * F::ESZ));
-    if (F::NPART > 1) DBGZ_TRY(dbgz_ensure(ctx, p->Ulo, (size_t)d * Dp * F::ESZ));
+    if (F::NPART > 1) DBGZ_TRY(dbgz_ensure(ctx, u1, (size_t)d * Dp * F::ESZ));
     dim3 g((unsigned)((Dp + 255) / 256), (unsigned)d);
-    k_make_ut<MODE><<<g, 256, 0, ctx->stream>>>((const double *)p->U.p, d, Dp, u0.p,
-                                                F::NPART > 1 ? p->Ulo.p : nullptr);
+    k_make_ut<MODE><<<g, 256, 0, ctx->stream>>>((const double *)src.p, d, Dp, u0.p,
+                                                F::NPART > 1 ? u1.p : nullptr);
     dbgz_count_launch(ctx);
     DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   }
   if (!p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
   const int Pw = 256;
   const int smem = SM::total(Pw);
-  auto kern = pa.qmc_type == DBGZ_QMC_SOBOL ? k_genz_umma<MODE, DBGZ_QMC_SOBOL> : k_genz_umma<MODE, DBGZ_QMC_RICHTMYER>;
+  auto kern = pick_kernel<MODE>(pa);
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   // CTAs per SM from the kernel's own resources: TMEM columns (512 / P),
@@ -591,7 +605,17 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.shift32 = (const float *)p->shifts32.p;
   P.gen.V = (const uint32_t *)p->V.p;
   P.gen.ushift = (const uint64_t *)p->ushifts.p;
-  P.U32 = (const float *)p->U32.p;
+  P.U32 = (const float *)(adj ? p->Ub32.p : p->U32.p);
+  P.io.N = pa.grad.N;
+  P.io.y = (float *)pa.grad.y;
+  P.io.s = (float *)pa.grad.s;
+  P.io.dc = (float *)pa.grad.dc;
+  P.io.sbar = (float *)pa.grad.sbar;
+  P.io.p = pa.grad.p;
+  P.io.ga = pa.grad.ga;
+  P.io.gb = pa.grad.gb;
+  P.io.gu = pa.grad.gu;
+  P.io.dc1 = pa.grad.dc1;
   P.tgt = (const TargetParams32 *)p->tgt32.p;
   P.c1 = pa.c1;
   P.dc1 = pa.dc1;
@@ -599,7 +623,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.partials = partials;
   P.status = ctx->d_status;
   DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_u[0], u0.p, (uint64_t)Dp, (uint64_t)d, 64));
-  if (F::NPART > 1) DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_u[1], p->Ulo.p, (uint64_t)Dp, (uint64_t)d, 64));
+  if (F::NPART > 1) DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_u[1], u1.p, (uint64_t)Dp, (uint64_t)d, 64));
   // Y workspace: one 128-row slot per CTA, parts side by side
   const size_t part_bytes = (size_t)grid * TS * Dp * F::ESZ;
   (void)nphase;

@@ -51,6 +51,8 @@ struct StepFp64Scratch : dbgz::StepFp64 {
   }
 };
 
+using NoallocPolicy = pol::Forward<double, DBGZ_QMC_RICHTMYER, false, StepFp64Scratch>;
+
 // Per-target constants and the first dimension's CDF values
 // (src/qmc.jl:800-809, erf form).
 __global__ void k_noalloc_setup(const double *U, int64_t d, const double *a, const double *b,
@@ -78,7 +80,7 @@ int setup_device(int dev, DeviceSlot &slot) {
     return DBGZ_ERR_CUDA;
   }
   s.ptr = (unsigned char *)p;
-  auto kern = k_genz_simt<double, StepFp64Scratch>;
+  auto kern = k_genz_simt<double, NoallocPolicy>;
   const int smem = (int)sizeof(SimtSmem<double>);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s.per_sm, kern, NT, smem) != cudaSuccess ||
@@ -142,7 +144,7 @@ extern "C" int dbgz_pnorm_pass_noalloc(int64_t d, const double *U, const double 
   P.cdf_form = DBGZ_CDF_ERF;
   P.yws = yws;
   P.partials = partials;
-  k_genz_simt<double, StepFp64Scratch><<<(unsigned)grid, NT, sizeof(SimtSmem<double>), st>>>(P);
+  k_genz_simt<double, NoallocPolicy><<<(unsigned)grid, NT, sizeof(SimtSmem<double>), st>>>(P);
   // the output accumulates a running mean with weight 0 for a first pass:
   // clear it so that stale or uninitialised contents cannot leak in
   if (cudaMemsetAsync(qmc_reps, 0, sizeof(double) * n_reps, st) != cudaSuccess) {

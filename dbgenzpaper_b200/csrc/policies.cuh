@@ -1,0 +1,288 @@
+// policies.cuh -- what one sequential step of the integration loops does.
+//
+// Both loop kernels (SIMT and tensor-core) walk an "emitter" index l =
+// 0..d-2 in order; step l emits a value v_l, and the contraction delivers
+// to step l the receiver sum r_l = sum_{l' <= l} v_{l'} C[l', l] (the
+// emitter's own diagonal term included), where C is an upper-triangular
+// coefficient matrix given as a d x d column-major array with C[l', l] at
+// [(l + 1) * d + l'].  A policy supplies v_l (emit) and uses r_l
+// (consume):
+//
+//  * Forward (qmc_loop!, src/qmc.jl:315-444): C = U, v_l = y_l = Phi^-1(u_l),
+//    r_l = s_{l+1}, consume = the CDF update of variable l+1.  With STORE it
+//    also records y_l, s_{l+1}, dc_{l+1} and p per sample for the adjoint.
+//  * Adjoint (no counterpart in the reference): the reverse recurrence
+//      ybar_l = sum_{t > l} sbar_t U[l, t]
+//    has the same triangular shape once indices are reversed: emitter
+//    l' = d-1-t, C = the anti-transpose of U (C[i, j] = U[d-1-j, d-1-i]),
+//    v_{l'} = sbar_t, r_{l'} = ybar_{t-1}.  emit computes sbar_t of
+//    variable t = d-1-l' from the stored forward state and the saved
+//    ybar_t; consume saves ybar_{t-1} for the next step.
+//
+// Adjoint of one sample (L = p = prod_t dc_t; c_t = Phi(alpha_t),
+// e_t = Phi(beta_t), alpha_t = (a_t - s_t)/U_tt, u_t = (1-w_t) c_t + w_t e_t,
+// y_t = Phi^-1(u_t)):
+//   ubar_t = ybar_t / phi(y_t)                          (0 if u_t was clamped)
+//   ebar_t = p/dc_t + ubar_t w_t,   cbar_t = -p/dc_t + ubar_t (1 - w_t)
+//   dL/da_t = cbar_t phi(alpha_t)/U_tt,  dL/db_t = ebar_t phi(beta_t)/U_tt
+//   sbar_t = -(dL/da_t + dL/db_t),  dL/dU_tt = -(dL/da_t alpha_t + dL/db_t beta_t)
+//   dL/dU[l,t] = y_l sbar_t  (l < t; accumulated over samples by a GEMM)
+// The forward clamps (|x| < 9 in erf units, u in [eps64, 1-eps64]) pass no
+// derivative.  Everything is linear in p, so the recurrence runs with unit
+// seed (p replaced by 1) and per-sample results are scaled by p when they
+// are accumulated.
+#pragma once
+#include "internal.cuh"
+#include "genz_step.cuh"
+
+namespace pol {
+
+constexpr int PB = 32;  // staged dimensions per block
+
+template <typename T>
+struct TgtT;
+template <>
+struct TgtT<double> {
+  using type = TargetParams64;
+};
+template <>
+struct TgtT<float> {
+  using type = TargetParams32;
+};
+
+// Per-block staging shared by every policy: target constants, lattice
+// generator and shift of the block's steps (index mapping per policy).
+template <typename T>
+struct Staged {
+  typename TgtT<T>::type tg[PB];
+  double qv[PB];
+  T shv[PB];
+};
+
+// Arrays of the forward state kept for the adjoint, [index][sample] with
+// the sample index contiguous (coalesced per step).  N = samples of the pass.
+template <typename T>
+struct GradIO {
+  int64_t N = 0;
+  T *y = nullptr;     // y_l,  l = 0..d-2
+  T *s = nullptr;     // s_t,  t = 1..d-1 (row t)
+  T *dc = nullptr;    // dc_t, t = 1..d-1 (row t)
+  double *p = nullptr;
+  T *sbar = nullptr;  // p * sbar_t, t = 1..d-1 (row t)
+  double *ga = nullptr, *gb = nullptr, *gu = nullptr;  // [(tile * 4 + warp) * d + t]
+  double dc1 = 0.0;   // dc of variable 0
+};
+
+template <typename T>
+__device__ __forceinline__ T shift_at(const dbgz::GenParams &g, int64_t idx);
+template <>
+__device__ __forceinline__ double shift_at<double>(const dbgz::GenParams &g, int64_t idx) {
+  return g.shift64 ? g.shift64[idx] : 0.0;
+}
+template <>
+__device__ __forceinline__ float shift_at<float>(const dbgz::GenParams &g, int64_t idx) {
+  return g.shift32 ? g.shift32[idx] : 0.0f;
+}
+
+// Step numerics by working type.
+template <typename T>
+struct StepOf;
+template <>
+struct StepOf<double> {
+  using type = dbgz::StepFp64;
+};
+template <>
+struct StepOf<float> {
+  using type = dbgz::StepFp32;
+};
+
+// ---------------------------------------------------------------- forward ---
+template <typename T, int GEN, bool STORE, typename Step = typename StepOf<T>::type>
+struct Forward {
+  Step st;
+  dbgz::GenParams gen;
+  int64_t j, k, g;  // point index in the pass, shift, global sample index
+  int64_t d;
+  int cdf_form;
+  GradIO<T> io;
+
+  __device__ __forceinline__ void tile_begin(const dbgz::GenParams &gp, int64_t d_, int64_t tile,
+                                             int64_t tiles_per_shift, int r, double c1, double dc1,
+                                             double up1, int cdf_form_, const GradIO<T> &io_) {
+    gen = gp;
+    gen.qmc_type = GEN;
+    d = d_;
+    k = tile / tiles_per_shift;
+    j = (tile - k * tiles_per_shift) * 128 + r;
+    g = tile * 128 + r;
+    cdf_form = cdf_form_;
+    io = io_;
+    st.init(c1, dc1, up1);
+  }
+  // cooperative: r in [0, 128)
+  __device__ __forceinline__ void stage(Staged<T> &sg, const typename TgtT<T>::type *tgt, int r,
+                                        int64_t lbase, int nval) const {
+    if (r < nval) {
+      sg.tg[r] = tgt[lbase + r + 1];
+      sg.qv[r] = gen.q ? gen.q[lbase + r] : 0.0;
+      sg.shv[r] = shift_at<T>(gen, k * (d - 1) + lbase + r);
+    }
+  }
+  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
+    const T y = st.quantile(gen, d, j, k, l, sg.qv[li], sg.shv[li]);
+    if (STORE) io.y[l * io.N + g] = y;
+    return y;
+  }
+  __device__ __forceinline__ void consume(const Staged<T> &sg, T s, int li, int64_t l) {
+    const auto tg = sg.tg[li];
+    st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
+    if (STORE) {
+      io.s[(l + 1) * io.N + g] = s;
+      io.dc[(l + 1) * io.N + g] = (T)st.dc;
+    }
+  }
+  // value of this sample added to the tile's sum of p
+  __device__ __forceinline__ double tile_value(bool valid) {
+    if (STORE) io.p[g] = valid ? st.p : 0.0;
+    return valid ? st.p : 0.0;
+  }
+  __device__ __forceinline__ void tile_end(const typename TgtT<T>::type *, int, int, int64_t, bool) {}
+};
+
+// ---------------------------------------------------------------- adjoint ---
+__device__ __forceinline__ double inv_sqrt2pi() { return 0.3989422804014327; }
+
+template <typename T>
+__device__ __forceinline__ T phi_of_erfunits(T x) {  // standard normal pdf at sqrt(2) x
+  return (T)(0.3989422804014327 * exp(-(double)x * (double)x));
+}
+
+template <typename T, int GEN>
+struct Adjoint {
+  dbgz::GenParams gen;
+  int64_t j, k, g, d, tile;
+  GradIO<T> io;
+  double ybar;  // saved receiver value: ybar of the variable the next step handles
+  double p;     // this sample's weight (the seed scale)
+  int warp, lane;
+
+  __device__ __forceinline__ void tile_begin(const dbgz::GenParams &gp, int64_t d_, int64_t tile_,
+                                             int64_t tiles_per_shift, int r, double, double, double, int,
+                                             const GradIO<T> &io_) {
+    gen = gp;
+    gen.qmc_type = GEN;
+    d = d_;
+    tile = tile_;
+    k = tile / tiles_per_shift;
+    j = (tile - k * tiles_per_shift) * 128 + r;
+    g = tile * 128 + r;
+    io = io_;
+    ybar = 0.0;  // variable d-1 has no u: nothing downstream of it
+    p = io.p[g];
+    warp = r >> 5;
+    lane = r & 31;
+  }
+  // step li of the block handles variable t = d-1-(lbase+li); its point is
+  // QMC dimension t (y-index t), which exists for t <= d-2
+  __device__ __forceinline__ void stage(Staged<T> &sg, const typename TgtT<T>::type *tgt, int r,
+                                        int64_t lbase, int nval) const {
+    if (r < nval) {
+      const int64_t t = d - 1 - (lbase + r);
+      sg.tg[r] = tgt[t];
+      sg.qv[r] = (t <= d - 2 && gen.q) ? gen.q[t] : 0.0;
+      sg.shv[r] = t <= d - 2 ? shift_at<T>(gen, k * (d - 1) + t) : T(0);
+    }
+  }
+
+  // tent-transformed point w_t of y-index t (as StepFp*::quantile forms it)
+  __device__ __forceinline__ double point_w(const Staged<T> &sg, int li, int64_t t) const {
+    double u;
+    if (GEN == 0) {
+      double x = __dmul_rn((double)(gen.gen_base + j + 1), sg.qv[li]);
+      x = x - floor(x);
+      if (sizeof(T) == 4) {
+        float uf = (float)sg.shv[li] + (float)x;
+        uf = uf > 1.0f ? uf - 1.0f : uf;
+        return (double)fabsf(fmaf(uf, 2.0f, -1.0f));
+      }
+      u = (double)sg.shv[li] + x;
+      u = u > 1.0 ? u - 1.0 : u;
+    } else {
+      const int L = gen.n_bits;
+      const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
+      const uint64_t xi =
+          (uint64_t)dbgz::sobol_int(gen.V + t * 32, (uint64_t)(gen.sobol_first + gen.gen_base + j)) & mask;
+      const uint64_t sh = gen.ushift[k * (d - 1) + t] & mask;
+      u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
+    }
+    return fabs(fma(u, 2.0, -1.0));
+  }
+
+  // adjoint of variable t given ybar_t; returns sbar_t (unit seed), records
+  // the p-scaled per-variable gradient terms
+  __device__ __forceinline__ double variable(const typename TgtT<T>::type &tg, double w, bool has_u,
+                                             double y, double s, double dc, bool clamp9,
+                                             double &ga, double &gb, double &gu) const {
+    const double inv_u = (double)tg.inv_u;         // 1 / (U_tt sqrt 2)
+    const double rU = inv_u * 1.4142135623730951;  // 1 / U_tt
+    double xa = ((double)tg.a - s) * inv_u, xb = ((double)tg.b - s) * inv_u;
+    const bool pa = !clamp9 || fabs(xa) < 9.0, pb = !clamp9 || fabs(xb) < 9.0;
+    const double pex = dc != 0.0 ? 1.0 / dc : 0.0;
+    double ubar = 0.0;
+    if (has_u && fabs(y) < 8.12585) ubar = ybar / (inv_sqrt2pi() * exp(-0.5 * y * y));
+    const double eb = pex + ubar * w, cb = -pex + ubar * (1.0 - w);
+    const double fa = pa ? inv_sqrt2pi() * exp(-xa * xa) : 0.0;
+    const double fb = pb ? inv_sqrt2pi() * exp(-xb * xb) : 0.0;
+    ga = (fa != 0.0) ? cb * fa * rU : 0.0;
+    gb = (fb != 0.0) ? eb * fb * rU : 0.0;
+    const double al = xa * 1.4142135623730951, be = xb * 1.4142135623730951;
+    gu = -((ga != 0.0 ? ga * al : 0.0) + (gb != 0.0 ? gb * be : 0.0));
+    return -(ga + gb);
+  }
+
+  __device__ __forceinline__ void accumulate(int64_t t, double ga, double gb, double gu) const {
+    double v0 = p * ga, v1 = p * gb, v2 = p * gu;
+    for (int o = 16; o > 0; o >>= 1) {
+      v0 += __shfl_down_sync(0xffffffffu, v0, o);
+      v1 += __shfl_down_sync(0xffffffffu, v1, o);
+      v2 += __shfl_down_sync(0xffffffffu, v2, o);
+    }
+    if (lane == 0) {
+      const int64_t row = (tile * 4 + warp) * d + t;
+      io.ga[row] = v0;
+      io.gb[row] = v1;
+      io.gu[row] = v2;
+    }
+  }
+
+  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
+    const int64_t t = d - 1 - l;
+    const bool has_u = t <= d - 2;
+    const double y = has_u ? (double)io.y[t * io.N + g] : 0.0;
+    const double s = (double)io.s[t * io.N + g];
+    const double dc = (double)io.dc[t * io.N + g];
+    const double w = has_u ? point_w(sg, li, t) : 0.0;
+    double ga, gb, gu;
+    const double sb = variable(sg.tg[li], w, has_u, y, s, dc, true, ga, gb, gu);
+    accumulate(t, ga, gb, gu);
+    io.sbar[t * io.N + g] = (T)(p * sb);
+    return (T)sb;
+  }
+  __device__ __forceinline__ void consume(const Staged<T> &, T r_sum, int, int64_t) { ybar = (double)r_sum; }
+
+  __device__ __forceinline__ double tile_value(bool) { return 0.0; }
+  // variable 0 after the last step: its CDF has no conditioning sum and no
+  // clamp (src/qmc.jl:800-809); its point is QMC dimension 0
+  __device__ __forceinline__ void tile_end(const typename TgtT<T>::type *tgt, int r, int, int64_t, bool) {
+    Staged<T> sg0;
+    sg0.qv[0] = gen.q ? gen.q[0] : 0.0;
+    sg0.shv[0] = shift_at<T>(gen, k * (d - 1));
+    const double w = point_w(sg0, 0, 0);
+    const double y = (double)io.y[g];
+    double ga, gb, gu;
+    variable(tgt[0], w, true, y, 0.0, io.dc1, false, ga, gb, gu);
+    accumulate(0, ga, gb, gu);
+  }
+};
+
+}  // namespace pol

@@ -176,6 +176,22 @@ int dbgz_problem_factor(const dbgz_problem *p, double *U, int64_t *perm, double 
 int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err,
                int64_t *n_pts, double *qmc_reps);
 
+/* Gradient of the estimate (no counterpart in the reference).  Runs one
+ * pass of m points x n_reps shifts on the problem's current point set (the
+ * first pass of dbgz_pnorm; the generator is not advanced), keeps the
+ * forward state in device memory, and runs the adjoint of the sequential
+ * conditioning on the same points (common random numbers): the returned
+ * gradients are exact derivatives of the returned estimate.  The pivot
+ * order is held fixed.
+ *   dP_da, dP_db: length d, original variable order and scale (NULL skips);
+ *   dP_dU: d x d column-major, with respect to the factor U in the
+ *          permuted, correlation-scaled coordinates dbgz_problem_factor
+ *          returns (upper triangle with the diagonal; NULL skips).
+ * Dense structure and erf-form CDF only.  Device memory: four d x N state
+ * arrays of the working type (N = samples of the pass) plus partial sums. */
+int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, double *err,
+                    int64_t *n_pts, double *dP_da, double *dP_db, double *dP_dU);
+
 /* ---- allocation-free pass -------------------------------------------
  * No counterpart in the reference.  Some callers cannot let a library
  * allocate device memory: a host framework that owns every device buffer
