@@ -205,6 +205,7 @@ def main():
     ap.add_argument("--points", type=int, default=None, help="points per shift (default: 2^17)")
     ap.add_argument("--only", action="store_true",
                     help="time only --precision (no FP64/other modes/accuracy/e2e/CPU legs); for profiling")
+    ap.add_argument("--grad", action="store_true", help="with --only: time the gradient call instead")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -266,8 +267,25 @@ def main():
             dist.barrier()
         return res, tot / steps, loop / max(nl, 1), nl, nk
 
+    # gradient: estimate + adjoint on the same points (dbgz_pnorm_grad), timed
+    # on the device like the forward step (host-side D2H of dU included)
+    def grad_step(Qg, precision):
+        flush.zero_()
+        torch.cuda.synchronize()
+        r = D.qmc_pnorm_grad(Qg, precision=precision)
+        lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+        return r, prof.pnorm_ms, prof.kernel_launches
+
     Q = make(prec_mixed)
     peaks, peak_kind = _peaks()
+    if args.only and args.grad:
+        for _ in range(args.warmup):
+            grad_step(Q, prec_mixed)
+        g = [grad_step(Q, prec_mixed)[1] for _ in range(args.steps)]
+        if rank == 0:
+            print(json.dumps({"precision": args.precision, "grad_ms_per_step": statistics.mean(g),
+                              "workload": w.name, "samples": w.samples}), flush=True)
+        return 0
     with ClockSampler(local) as clk:
         (P_mix, err_mix, npts, reps_mix), ms_mix, loop_ms, n_loop, n_kern = timed(
             Q, prec_mixed, args.steps, args.warmup)
@@ -287,15 +305,6 @@ def main():
             continue
         (Po, _, _, _), mso, lo_ms, _, _ = timed(Q, D.PRECISIONS[name], max(2, args.steps // 2), 1)
         other[name] = {"ms_per_step": mso, "loop_ms": lo_ms, "P": Po}
-
-    # gradient: estimate + adjoint on the same points (dbgz_pnorm_grad), timed
-    # on the device like the forward step (host-side D2H of dU included)
-    def grad_step(Qg, precision):
-        flush.zero_()
-        torch.cuda.synchronize()
-        r = D.qmc_pnorm_grad(Qg, precision=precision)
-        lib.dbgz_get_profile(ctx.handle, C.byref(prof))
-        return r, prof.pnorm_ms, prof.kernel_launches
 
     grad_step(Q, prec_mixed)
     kg = max(2, args.steps // 2)
@@ -324,16 +333,21 @@ def main():
 
     # e2e: the public API from host buffers, upload and factorisation included
     def e2e_step():
-        t = time.perf_counter()
+        t0 = time.perf_counter()
         Qe = make(prec_mixed)
+        t1 = time.perf_counter()
         r = D.qmc_pnorm(Qe, precision=prec_mixed)
+        t2 = time.perf_counter()
         Qe.close()
         torch.cuda.synchronize()
-        return time.perf_counter() - t, r
+        t3 = time.perf_counter()
+        return t3 - t0, (t1 - t0, t2 - t1, t3 - t2)
     for _ in range(max(1, args.warmup)):
         e2e_step()
-    e2e_t = [e2e_step()[0] for _ in range(max(3, args.steps // 2))]
-    e2e_ms = 1e3 * statistics.mean(e2e_t)
+    e2e_runs = [e2e_step() for _ in range(max(3, args.steps // 2))]
+    e2e_ms = 1e3 * statistics.mean(t for t, _ in e2e_runs)
+    e2e_parts = {k: 1e3 * statistics.mean(p[i] for _, p in e2e_runs)
+                 for i, k in enumerate(("prepare_ms", "pnorm_ms", "free_ms"))}
     h2d = w.Sigma.nbytes + w.a.nbytes + w.b.nbytes + w.shifts.nbytes
     d2h = 8 * w.n_reps + 3 * 8
 
@@ -376,7 +390,7 @@ def main():
                          "flops_per_launch": flops, "launch_ms": loop_ms,
                          "peak_source": f"{peak_kind} bf16_tflops (burst)"},
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h), "host_timed_parts": e2e_parts},
             "gpu_launches": int(n_kern),
             "clocks": clocks,
         }

@@ -67,10 +67,16 @@ class Context:
         self.handle = h
         self.device = device
 
+    def release_cached(self) -> int:
+        """Return the context's cached device buffers to the driver; -> bytes freed."""
+        n = C.c_uint64()
+        L.check(self._lib.dbgz_release_cached(self.handle, C.byref(n)), self.handle)
+        return int(n.value)
+
     def close(self):
         if self.handle:
-            self._lib.dbgz_destroy(self.handle)
-            self.handle = None
+            if self._lib.dbgz_destroy(self.handle) == L.OK:
+                self.handle = None
 
     def __del__(self):
         try:
@@ -151,7 +157,8 @@ class QMCData:
 
     def __init__(self, C_mat, a, b, opts: Optional[QMCOpts] = None, rng=None, qmc_type=None, *,
                  shifts=None, ushifts=None, sobol_dirnums=None, sobol_first=None,
-                 precision: Optional[int] = None, cdf_form: int = L.CDF_ERF, device: int = 0):
+                 precision: Optional[int] = None, cdf_form: int = L.CDF_ERF, device: int = 0,
+                 context: Optional[Context] = None):
         qmc_type = self._default_type if qmc_type is None else str(qmc_type).lstrip(":")
         if qmc_type not in ("Richtmyer", "Sobol"):
             raise ValueError("qmc_type must be 'Richtmyer' or 'Sobol'")
@@ -164,7 +171,7 @@ class QMCData:
         if a.shape != (n,) or b.shape != (n,):
             raise ValueError("a and b must have length n")
         rng = np.random.default_rng() if rng is None else rng
-        self.ctx = get_context(device)
+        self.ctx = get_context(device) if context is None else context
         self.n = n
         self.opts = opts
         self.qmc_type = qmc_type

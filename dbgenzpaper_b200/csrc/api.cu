@@ -18,29 +18,64 @@ int dbgz_fail(dbgz_ctx *ctx, int status, const char *fmt, ...) {
   return status;
 }
 
+// Frees every cached block of the context's pool (cudaFree synchronises the
+// device, so the blocks are idle afterwards).
+static size_t pool_trim(dbgz_ctx *ctx) {
+  size_t freed = 0;
+  for (auto &kv : ctx->pool) {
+    cudaFree(kv.second);
+    freed += kv.first;
+  }
+  ctx->pool.clear();
+  ctx->pool_bytes = 0;
+  return freed;
+}
+
 int dbgz_ensure(dbgz_ctx *ctx, DevBuf &b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.p && b.bytes >= bytes) return DBGZ_OK;
-  if (b.p) {
-    cudaFree(b.p);
-    b.p = nullptr;
-    b.bytes = 0;
+  dbgz_release(b);
+  // capacity classes: 512 B steps below 1 MiB, 2 MiB steps above
+  const size_t want = bytes < (1u << 20) ? (bytes + 511) & ~size_t(511) : (bytes + (2u << 20) - 1) & ~size_t((2u << 20) - 1);
+  // smallest cached block that fits and wastes at most a quarter (+2 MiB)
+  auto it = ctx->pool.lower_bound(want);
+  if (it != ctx->pool.end() && it->first <= want + want / 4 + (2u << 20)) {
+    b.p = it->second;
+    b.bytes = it->first;
+    b.owner = ctx;
+    ctx->pool_bytes -= it->first;
+    ctx->pool.erase(it);
+    return DBGZ_OK;
   }
-  cudaError_t e = cudaMalloc(&b.p, bytes);
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e == cudaErrorMemoryAllocation && !ctx->pool.empty()) {
+    cudaGetLastError();
+    pool_trim(ctx);
+    e = cudaMalloc(&b.p, want);
+  }
   if (e != cudaSuccess) {
     b.p = nullptr;
     cudaGetLastError();
     return dbgz_fail(ctx, e == cudaErrorMemoryAllocation ? DBGZ_ERR_OUT_OF_MEMORY : DBGZ_ERR_CUDA,
-                     "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+                     "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
   }
-  b.bytes = bytes;
+  b.bytes = want;
+  b.owner = ctx;
   return DBGZ_OK;
 }
 
 void dbgz_release(DevBuf &b) {
-  if (b.p) cudaFree(b.p);
+  if (b.p) {
+    if (b.owner) {
+      b.owner->pool.emplace(b.bytes, b.p);
+      b.owner->pool_bytes += b.bytes;
+    } else {
+      cudaFree(b.p);
+    }
+  }
   b.p = nullptr;
   b.bytes = 0;
+  b.owner = nullptr;
 }
 
 static int upload(dbgz_ctx *ctx, DevBuf &b, const void *src, size_t bytes) {
@@ -111,13 +146,28 @@ int dbgz_create(int device, dbgz_ctx **out) {
 
 int dbgz_destroy(dbgz_ctx *ctx) {
   if (!ctx) return DBGZ_ERR_INVALID_ARGUMENT;
+  // problems run on the context's stream and return their buffers to its
+  // pool: they must be freed first
+  if (ctx->live_problems > 0)
+    return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "destroy: %lld problem(s) of this context are still alive",
+                     (long long)ctx->live_problems);
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  pool_trim(ctx);
   if (ctx->d_status) cudaFree(ctx->d_status);
   for (cudaEvent_t &e : ctx->ev)
     if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+  return DBGZ_OK;
+}
+
+int dbgz_release_cached(dbgz_ctx *ctx, uint64_t *freed_bytes) {
+  if (!ctx) return DBGZ_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  const size_t f = pool_trim(ctx);
+  if (freed_bytes) *freed_bytes = f;
   return DBGZ_OK;
 }
 
@@ -283,6 +333,7 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
   dbgz_problem *p = new (std::nothrow) dbgz_problem();
   if (!p) return dbgz_fail(ctx, DBGZ_ERR_OUT_OF_MEMORY, "prepare: host allocation");
   p->ctx = ctx;
+  ctx->live_problems += 1;
   p->d = d;
   p->opts = o;
   p->qmc_type = qmc_type;
@@ -367,11 +418,13 @@ int dbgz_problem_free(dbgz_problem *p) {
     cudaSetDevice(p->ctx->device);
     cudaStreamSynchronize(p->ctx->stream);
   }
-  DevBuf *bufs[] = {&p->U, &p->a, &p->b, &p->perm, &p->scale, &p->q, &p->shifts, &p->shifts32,
-                    &p->V, &p->ushifts, &p->tgt64, &p->tgt32, &p->U32, &p->Uhi, &p->Ulo,
-                    &p->Utf, &p->yws, &p->partials, &p->reps, &p->csc_colptr, &p->csc_row,
-                    &p->csc_val64, &p->csc_val32};
+  DevBuf *bufs[] = {&p->U,     &p->a,       &p->b,       &p->perm,       &p->scale,   &p->q,         &p->shifts,
+                    &p->shifts32, &p->V,   &p->ushifts, &p->tgt64,      &p->tgt32,   &p->U32,       &p->Uhi,
+                    &p->Ulo,   &p->Utf,     &p->Ub,      &p->Ub32,       &p->Ubhi,    &p->Ublo,      &p->Ubtf,
+                    &p->grad_buf, &p->yws, &p->partials, &p->reps,      &p->csc_colptr, &p->csc_row, &p->csc_val64,
+                    &p->csc_val32};
   for (DevBuf *b : bufs) dbgz_release(*b);
+  if (p->ctx) p->ctx->live_problems -= 1;
   delete p;
   return DBGZ_OK;
 }
@@ -391,8 +444,8 @@ int dbgz_problem_truncate_band(dbgz_problem *p, int64_t bandwidth) {
   cudaSetDevice(ctx->device);
   p->band = bandwidth;
   DBGZ_TRY(dbgz_band_dev(ctx, p->d, (double *)p->U.p, bandwidth));
-  DevBuf *derived[] = {&p->U32, &p->Uhi, &p->Ulo, &p->Utf, &p->csc_colptr, &p->csc_row, &p->csc_val64,
-                       &p->csc_val32};
+  DevBuf *derived[] = {&p->U32, &p->Uhi,  &p->Ulo,  &p->Utf,  &p->Ub,         &p->Ub32,    &p->Ubhi,
+                       &p->Ublo, &p->Ubtf, &p->csc_colptr, &p->csc_row, &p->csc_val64, &p->csc_val32};
   for (DevBuf *b : derived) dbgz_release(*b);
   p->ldU = 0;
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));

@@ -257,16 +257,87 @@ k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t
 }
 
 // ldiv!(UpperTriangular(M[p0:p1,p0:p1])', M[p0:p1, c0:c1]): forward
-// substitution, one column per thread, ascending fma chains.
-__global__ void k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1) {
-  int64_t c = c0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c > c1) return;
-  double *X = M + c * n;
-  for (int64_t r = p0; r <= p1; ++r) {
-    const double *Ur = M + r * n;
-    double acc = 0.0;
-    for (int64_t l = p0; l < r; ++l) acc = dm_fma(Ur[l], X[l], acc);
-    X[r] = dm_div(dm_sub(X[r], acc), Ur[r]);
+// substitution X[r] = (X[r] - sum_{l<r} U[l,r] X[l]) / U[r,r] per column.
+//
+// Right-looking wavefront with the same arithmetic as the left-looking
+// form: row r's accumulator receives fma(U[l,r], X[l], acc) for l = p0,
+// p0+1, ..., r-1 in that order, starting from 0, so every X[r] is the same
+// ascending fma chain.  One warp per column c; lane i owns rows
+// q0 + i + 32k (k < kTrsmSlots) of a pass of kTrsmPass rows; the owner of
+// row l finishes X[l] and broadcasts it, then every lane updates its rows
+// r > l.  U[l0:l0+31, pass rows] is staged in shared memory (coalesced
+// 256-byte row segments of the column-major M) and shared by the CTA's
+// kTrsmWarps columns.
+constexpr int kTrsmWarps = 8, kTrsmSlots = 8, kTrsmPass = 32 * kTrsmSlots, kTrsmLc = 32;
+constexpr int kTrsmLd = kTrsmPass + 1;  // padded row of the staged chunk
+__global__ void __launch_bounds__(32 * kTrsmWarps)
+k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1) {
+  extern __shared__ double Us[];  // [kTrsmLc][kTrsmLd]: Us[lc * kTrsmLd + rr] = U[l0 + lc, q0 + rr]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t c = c0 + (int64_t)blockIdx.x * kTrsmWarps + warp;
+  const bool active = c <= c1;
+  double *X = M + (active ? c : c0) * n;
+  for (int64_t q0 = p0; q0 <= p1; q0 += kTrsmPass) {
+    const int64_t q1 = q0 + kTrsmPass - 1 < p1 ? q0 + kTrsmPass - 1 : p1;
+    const int nrows = (int)(q1 - q0 + 1);
+    double acc[kTrsmSlots], xin[kTrsmSlots];
+#pragma unroll
+    for (int k = 0; k < kTrsmSlots; ++k) {
+      acc[k] = 0.0;
+      const int rr = lane + 32 * k;
+      xin[k] = (active && rr < nrows) ? X[q0 + rr] : 0.0;
+    }
+    for (int64_t l0 = p0; l0 <= q1; l0 += kTrsmLc) {
+      const int nl = (int)((q1 - l0 + 1) < kTrsmLc ? (q1 - l0 + 1) : kTrsmLc);
+      __syncthreads();
+      for (int idx = threadIdx.x; idx < kTrsmPass * kTrsmLc; idx += blockDim.x) {
+        const int rr = idx / kTrsmLc, lc = idx % kTrsmLc;
+        Us[lc * kTrsmLd + rr] = (rr < nrows && lc < nl) ? M[(q0 + rr) * n + l0 + lc] : 0.0;
+      }
+      __syncthreads();
+      if (!active) continue;
+      if (l0 < q0) {
+        // rows of earlier passes: X[l] is final (written by this lane)
+        const double xl = lane < nl ? X[l0 + lane] : 0.0;
+        for (int lc = 0; lc < nl; ++lc) {
+          const double xv = __shfl_sync(0xffffffffu, xl, lc);
+          const double *u = Us + lc * kTrsmLd;
+#pragma unroll
+          for (int k = 0; k < kTrsmSlots; ++k) {
+            const int rr = lane + 32 * k;
+            if (rr < nrows) acc[k] = dm_fma(u[rr], xv, acc[k]);
+          }
+        }
+      } else {
+        // rows of this pass: slot ks holds rows l0 .. l0+31, lane lc owns l0+lc
+        const int ks = (int)((l0 - q0) / 32);
+        for (int lc = 0; lc < nl; ++lc) {
+          double mine = 0.0;
+#pragma unroll
+          for (int k = 0; k < kTrsmSlots; ++k)
+            if (k == ks && lane == lc) {
+              xin[k] = dm_div(dm_sub(xin[k], acc[k]), Us[lc * kTrsmLd + (int)(l0 - q0) + lc]);
+              mine = xin[k];
+            }
+          const double xv = __shfl_sync(0xffffffffu, mine, lc);
+          const double *u = Us + lc * kTrsmLd;
+          const int rl = (int)(l0 - q0) + lc;  // pass-local row of l
+#pragma unroll
+          for (int k = 0; k < kTrsmSlots; ++k) {
+            const int rr = lane + 32 * k;
+            if (rr > rl && rr < nrows) acc[k] = dm_fma(u[rr], xv, acc[k]);
+          }
+        }
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < kTrsmSlots; ++k) {
+        const int rr = lane + 32 * k;
+        if (rr < nrows) X[q0 + rr] = xin[k];
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -351,8 +422,16 @@ int launch_schur(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, in
 int launch_trsm(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0,
                 int64_t c1) {
   if (c1 < c0) return DBGZ_OK;
-  int64_t nc = c1 - c0 + 1;
-  k_trsm_ut<<<(unsigned)((nc + 63) / 64), 64, 0, ctx->stream>>>(M, n, p0, p1, c0, c1);
+  const int64_t nc = c1 - c0 + 1;
+  const size_t smem = sizeof(double) * kTrsmLc * kTrsmLd;
+  // 66 KB of dynamic shared memory needs the opt-in, once per device
+  static bool attr_set[64] = {};
+  if (ctx->device < 0 || ctx->device >= 64 || !attr_set[ctx->device]) {
+    DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(k_trsm_ut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (ctx->device >= 0 && ctx->device < 64) attr_set[ctx->device] = true;
+  }
+  k_trsm_ut<<<(unsigned)((nc + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps, smem, ctx->stream>>>(M, n, p0, p1,
+                                                                                                    c0, c1);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   return DBGZ_OK;

@@ -18,20 +18,32 @@
 
 namespace {
 
-// sum over rows (tile * 4 + warp) of part[row * d + t], rows in order
-__global__ void k_reduce_partials(const double *ga, const double *gb, const double *gu, int64_t rows, int64_t d,
-                                  double *out) {
-  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// Fixed-order sums of the per-(tile, warp) partial rows part[row * d + t]:
+// stage 1 sums `chunk` consecutive rows per CTA column (coalesced over t),
+// stage 2 sums the chunk sums in chunk order.
+constexpr int kRedChunks = 256;
+__global__ void k_reduce_rows(const double *ga, const double *gb, const double *gu, int64_t rows, int64_t d,
+                              int64_t chunk, double *csum) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= d) return;
+  const int64_t r0 = blockIdx.y * chunk, r1 = r0 + chunk < rows ? r0 + chunk : rows;
   double a = 0.0, b = 0.0, u = 0.0;
-  for (int64_t r = 0; r < rows; ++r) {
+  for (int64_t r = r0; r < r1; ++r) {
     a += ga[r * d + t];
     b += gb[r * d + t];
     u += gu[r * d + t];
   }
-  out[t] = a;
-  out[d + t] = b;
-  out[2 * d + t] = u;
+  double *o = csum + (int64_t)blockIdx.y * 3 * d;
+  o[t] = a;
+  o[d + t] = b;
+  o[2 * d + t] = u;
+}
+__global__ void k_reduce_chunks(const double *csum, int64_t n_chunks, int64_t d, double *out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // i in [0, 3d)
+  if (i >= 3 * d) return;
+  double v = 0.0;
+  for (int64_t c = 0; c < n_chunks; ++c) v += csum[c * 3 * d + i];
+  out[i] = v;
 }
 
 struct CublasHandle {
@@ -82,7 +94,8 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   // one allocation for the pass: 4 state arrays, p, 3 partial arrays, sums, dU
   const size_t arr = esz * (size_t)d * N;
   const size_t part = sizeof(double) * (size_t)n_tiles * 4 * d;
-  const size_t total = 4 * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d + esz * (size_t)d * d + 4096;
+  const size_t total = 4 * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d * (kRedChunks + 1) +
+                       esz * (size_t)d * d + 8192;
   DBGZ_TRY(dbgz_ensure(ctx, p->grad_buf, total));
   char *base = (char *)p->grad_buf.p;
   auto take = [&](size_t bytes) {
@@ -102,6 +115,7 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   ga.gu = (double *)take(part);
   ga.dc1 = p->dc1;
   double *sums = (double *)take(3 * 8 * (size_t)d);
+  double *csum = (double *)take(3 * 8 * (size_t)d * kRedChunks);
   void *dU = take(esz * (size_t)d * d);
   // rows the passes leave unwritten enter the dU GEMM: clear them
   DBGZ_CUDA_TRY(ctx, cudaMemsetAsync((char *)ga.y + esz * (size_t)(d - 1) * N, 0, esz * N, ctx->stream));
@@ -136,8 +150,15 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   pa.kind = kLoopAdjoint;
   if (tensor) DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
   else DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
-  k_reduce_partials<<<(unsigned)((d + 127) / 128), 128, 0, ctx->stream>>>(ga.ga, ga.gb, ga.gu, n_tiles * 4, d, sums);
-  dbgz_count_launch(ctx);
+  {
+    const int64_t rows = n_tiles * 4, chunk = (rows + kRedChunks - 1) / kRedChunks;
+    const int64_t n_chunks = (rows + chunk - 1) / chunk;
+    k_reduce_rows<<<dim3((unsigned)((d + 127) / 128), (unsigned)n_chunks), 128, 0, ctx->stream>>>(
+        ga.ga, ga.gb, ga.gu, rows, d, chunk, csum);
+    dbgz_count_launch(ctx);
+    k_reduce_chunks<<<(unsigned)((3 * d + 255) / 256), 256, 0, ctx->stream>>>(csum, n_chunks, d, sums);
+    dbgz_count_launch(ctx);
+  }
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   // dU[l, t] = sum_n y[l][n] (p sbar)[t][n]: (d x N) x (N x d), sample-contiguous rows
   if (dP_dU) {

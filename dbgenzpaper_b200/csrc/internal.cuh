@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstdarg>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -25,9 +26,13 @@
     if (s_ != DBGZ_OK) return s_;     \
   } while (0)
 
+struct dbgz_ctx;
+// A device buffer of the library.  Buffers taken from a context's pool go
+// back to it on release (owner set); bytes is the block's capacity.
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
+  dbgz_ctx *owner = nullptr;
 };
 
 struct dbgz_ctx {
@@ -40,6 +45,15 @@ struct dbgz_ctx {
   cudaEvent_t ev[6] = {};   // 0/1: call bracket, 2/3: loop launch, 4/5: finalize
   dbgz_profile prof{};
   int64_t launch_count = 0; // kernels launched by the library on this context
+  // Stream-ordered block cache: released buffers wait here for the next
+  // request of similar size.  Every user of a block enqueues on `stream`, so
+  // a block handed out again is only touched after the work of its previous
+  // user; nothing is returned to the driver before dbgz_release_cached or
+  // dbgz_destroy (or an allocation failure, which empties the cache and
+  // retries once).
+  std::multimap<size_t, void *> pool;
+  size_t pool_bytes = 0;
+  int64_t live_problems = 0;  // problems created on this context and not yet freed
 };
 
 // Counts a kernel launch of the library (for dbgz_profile).

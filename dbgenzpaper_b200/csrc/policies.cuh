@@ -150,13 +150,6 @@ struct Forward {
 };
 
 // ---------------------------------------------------------------- adjoint ---
-__device__ __forceinline__ double inv_sqrt2pi() { return 0.3989422804014327; }
-
-template <typename T>
-__device__ __forceinline__ T phi_of_erfunits(T x) {  // standard normal pdf at sqrt(2) x
-  return (T)(0.3989422804014327 * exp(-(double)x * (double)x));
-}
-
 template <typename T, int GEN>
 struct Adjoint {
   dbgz::GenParams gen;
@@ -219,23 +212,28 @@ struct Adjoint {
   }
 
   // adjoint of variable t given ybar_t; returns sbar_t (unit seed), records
-  // the p-scaled per-variable gradient terms
-  __device__ __forceinline__ double variable(const typename TgtT<T>::type &tg, double w, bool has_u,
-                                             double y, double s, double dc, bool clamp9,
-                                             double &ga, double &gb, double &gu) const {
-    const double inv_u = (double)tg.inv_u;         // 1 / (U_tt sqrt 2)
-    const double rU = inv_u * 1.4142135623730951;  // 1 / U_tt
-    double xa = ((double)tg.a - s) * inv_u, xb = ((double)tg.b - s) * inv_u;
-    const bool pa = !clamp9 || fabs(xa) < 9.0, pb = !clamp9 || fabs(xb) < 9.0;
-    const double pex = dc != 0.0 ? 1.0 / dc : 0.0;
+  // the per-variable gradient terms (unit seed; accumulate scales by p).
+  // The bound arguments and the normal densities are formed in T (FP32
+  // paths: FP32 exp, as their y, s, dc are FP32 already); the reciprocals of
+  // dc and of the density of y, which reach 1e30 and beyond for narrow
+  // intervals, and everything multiplied by them stay FP64.
+  __device__ __forceinline__ double variable(const typename TgtT<T>::type &tg, double w, bool has_u, T y, T s,
+                                             T dc, bool clamp9, double &ga, double &gb, double &gu) const {
+    const T r2 = T(1.4142135623730951), rpi = T(0.3989422804014327);
+    const T inv_u = (T)tg.inv_u;  // 1 / (U_tt sqrt 2)
+    const T xa = ((T)tg.a - s) * inv_u, xb = ((T)tg.b - s) * inv_u;
+    const bool pa = !clamp9 || fabs(xa) < T(9), pb = !clamp9 || fabs(xb) < T(9);
+    const T fa = pa ? rpi * exp(-xa * xa) : T(0);
+    const T fb = pb ? rpi * exp(-xb * xb) : T(0);
+    // d log(dc) / d dc; a dc of zero (weight zero) contributes nothing
+    const double pex = dc > T(0) ? 1.0 / (double)dc : 0.0;
     double ubar = 0.0;
-    if (has_u && fabs(y) < 8.12585) ubar = ybar / (inv_sqrt2pi() * exp(-0.5 * y * y));
+    if (has_u && fabs(y) < T(8.12585)) ubar = ybar / (double)(rpi * exp(T(-0.5) * y * y));
     const double eb = pex + ubar * w, cb = -pex + ubar * (1.0 - w);
-    const double fa = pa ? inv_sqrt2pi() * exp(-xa * xa) : 0.0;
-    const double fb = pb ? inv_sqrt2pi() * exp(-xb * xb) : 0.0;
-    ga = (fa != 0.0) ? cb * fa * rU : 0.0;
-    gb = (fb != 0.0) ? eb * fb * rU : 0.0;
-    const double al = xa * 1.4142135623730951, be = xb * 1.4142135623730951;
+    const double rU = (double)inv_u * 1.4142135623730951;  // 1 / U_tt
+    ga = (fa != T(0)) ? cb * (double)fa * rU : 0.0;
+    gb = (fb != T(0)) ? eb * (double)fb * rU : 0.0;
+    const double al = (double)xa * 1.4142135623730951, be = (double)xb * 1.4142135623730951;
     gu = -((ga != 0.0 ? ga * al : 0.0) + (gb != 0.0 ? gb * be : 0.0));
     return -(ga + gb);
   }
@@ -258,9 +256,9 @@ struct Adjoint {
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const double y = has_u ? (double)io.y[t * io.N + g] : 0.0;
-    const double s = (double)io.s[t * io.N + g];
-    const double dc = (double)io.dc[t * io.N + g];
+    const T y = has_u ? io.y[t * io.N + g] : T(0);
+    const T s = io.s[t * io.N + g];
+    const T dc = io.dc[t * io.N + g];
     const double w = has_u ? point_w(sg, li, t) : 0.0;
     double ga, gb, gu;
     const double sb = variable(sg.tg[li], w, has_u, y, s, dc, true, ga, gb, gu);
@@ -278,9 +276,9 @@ struct Adjoint {
     sg0.qv[0] = gen.q ? gen.q[0] : 0.0;
     sg0.shv[0] = shift_at<T>(gen, k * (d - 1));
     const double w = point_w(sg0, 0, 0);
-    const double y = (double)io.y[g];
+    const T y = io.y[g];
     double ga, gb, gu;
-    variable(tgt[0], w, true, y, 0.0, io.dc1, false, ga, gb, gu);
+    variable(tgt[0], w, true, y, T(0), (T)io.dc1, false, ga, gb, gu);
     accumulate(0, ga, gb, gu);
   }
 };

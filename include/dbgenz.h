@@ -100,9 +100,19 @@ void dbgz_default_opts(dbgz_opts *opts);
 const char *dbgz_status_string(int status);
 int dbgz_abi_version(void);
 
-/* Context: one CUDA device, one stream, reusable workspaces. */
+/* Context: one CUDA device, one stream, reusable workspaces.  A context
+ * caches the device buffers of freed problems and hands them to later
+ * problems of similar size (stream-ordered on its stream), so repeated
+ * prepare/free cycles make no cudaMalloc/cudaFree calls.  Free every
+ * problem of a context before destroying it (DBGZ_ERR_INVALID_ARGUMENT
+ * otherwise, and nothing is destroyed).  A context is used by one host
+ * thread at a time. */
 int dbgz_create(int device, dbgz_ctx **out);
 int dbgz_destroy(dbgz_ctx *ctx);
+/* Returns the cached buffers of the context to the driver (after waiting
+ * for its stream); *freed_bytes (may be NULL) receives their total size.
+ * No reference counterpart (the reference runs on host memory). */
+int dbgz_release_cached(dbgz_ctx *ctx, uint64_t *freed_bytes);
 const char *dbgz_last_error(const dbgz_ctx *ctx);
 
 /* Device-side timing of the library's own work, measured with CUDA events
