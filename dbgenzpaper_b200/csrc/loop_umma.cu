@@ -101,8 +101,9 @@ struct Smem {
   static __host__ __device__ int total(int P) { return off_misc(P) + 12288 + 1024; }
 };
 
+constexpr int kUld = BK + 4;  // row stride of ublk: 16-byte aligned rows for LDS.128
 struct Misc {
-  float ublk[BK][2 * BK + 1];  // coefficients of the block's triangle, zero beyond column BK
+  float ublk[BK][kUld];  // coefficients of the block's triangle: ublk[li][ti] = U[lbase+li, lbase+ti+1]
   pol::Staged<float> sg;
   double red[4];
   uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
@@ -131,6 +132,23 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t t;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t) : "f"(x));
   return t;
+}
+
+// s[8 .. 8+N) += sum_k ys[k] * u[k * kUld + 0 .. N), k = 0..7 in order.
+template <int N>
+__device__ __forceinline__ void rank8_update(float (&s)[BK], const float (&ys)[8], const float *u) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float4 *row = reinterpret_cast<const float4 *>(u + k * kUld);
+#pragma unroll
+    for (int q = 0; q < N / 4; ++q) {
+      const float4 v = row[q];
+      s[8 + 4 * q] = fmaf(ys[k], v.x, s[8 + 4 * q]);
+      s[9 + 4 * q] = fmaf(ys[k], v.y, s[9 + 4 * q]);
+      s[10 + 4 * q] = fmaf(ys[k], v.z, s[10 + 4 * q]);
+      s[11 + 4 * q] = fmaf(ys[k], v.w, s[11 + 4 * q]);
+    }
+  }
 }
 
 // Policy: pol::Forward<float, GEN, STORE> or pol::Adjoint<float, GEN>.
@@ -356,7 +374,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           const int nval = (int)((P.nY - lbase) < BK ? (P.nY - lbase) : BK);
           // stage the block's U triangle and per-dimension parameters
           named_sync(kBarScalar, TS);
-          for (int e = r; e < BK * 2 * BK; e += TS) {
+          for (int e = r; e < BK * BK; e += TS) {
             const int li = e % BK, ti = e / BK;
             ms->ublk[li][ti] =
                 (li <= ti && ti < nval) ? P.U32[(lbase + ti + 1) * P.d + lbase + li] : 0.f;
@@ -388,24 +406,37 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
             // 4 chunks of 8 sequential steps.  s[] is kept in a frame that
             // rotates by 8 per chunk, so that every register index is static:
             // in chunk ch, s[t] is the partial sum of target lbase + 8 ch + t + 1.
+            // Step k adds y_k to the chunk's own targets s[k..7] (its
+            // triangle); the later chunks' targets s[8 .. 31-8ch] take the
+            // chunk's 8 y's in one rank-8 update after the chunk, in the same
+            // k order, so every sum is the same fma sequence as step by step.
             unsigned char *A = abuf + ia * SM::ABYTES;
 #pragma unroll 1
             for (int ch = 0; ch < BK / 8; ++ch) {
               uint32_t hi[4], lo[4];
               float ys[8];
+              pl.chunk_begin(lbase + 8 * ch, nval - 8 * ch);
 #pragma unroll
               for (int k = 0; k < 8; ++k) {
                 const int li = 8 * ch + k;
                 float y = 0.f;
                 if (li < nval) {
                   const int64_t l = lbase + li;
-                  y = pl.emit(ms->sg, li, l);
-                  const float *urow = &ms->ublk[li][8 * ch];
+                  y = pl.emit_k(ms->sg, li, l, k);
+                  const float4 *urow = reinterpret_cast<const float4 *>(&ms->ublk[li][8 * ch]);
+                  const float4 u0 = urow[0], u1 = urow[1];
+                  const float uu[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
-                  for (int t = k; t < BK; ++t) s[t] = fmaf(y, urow[t], s[t]);
+                  for (int t = k; t < 8; ++t) s[t] = fmaf(y, uu[t], s[t]);
                   pl.consume(ms->sg, s[k], li, l);
                 }
                 ys[k] = y;
+              }
+              switch (ch) {
+                case 0: rank8_update<24>(s, ys, &ms->ublk[0][8]); break;
+                case 1: rank8_update<16>(s, ys, &ms->ublk[8][16]); break;
+                case 2: rank8_update<8>(s, ys, &ms->ublk[16][24]); break;
+                default: break;
               }
               if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
 #pragma unroll

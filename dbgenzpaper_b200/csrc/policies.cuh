@@ -133,6 +133,9 @@ struct Forward {
     if (STORE) io.y[l * io.N + g] = y;
     return y;
   }
+  // chunked form (8 steps whose per-sample inputs may be loaded up front)
+  __device__ __forceinline__ void chunk_begin(int64_t, int) {}
+  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int) { return emit(sg, li, l); }
   __device__ __forceinline__ void consume(const Staged<T> &sg, T s, int li, int64_t l) {
     const auto tg = sg.tg[li];
     st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
@@ -253,18 +256,36 @@ struct Adjoint {
     }
   }
 
-  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
+  __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc) {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const T y = has_u ? io.y[t * io.N + g] : T(0);
-    const T s = io.s[t * io.N + g];
-    const T dc = io.dc[t * io.N + g];
     const double w = has_u ? point_w(sg, li, t) : 0.0;
     double ga, gb, gu;
     const double sb = variable(sg.tg[li], w, has_u, y, s, dc, true, ga, gb, gu);
     accumulate(t, ga, gb, gu);
     io.sbar[t * io.N + g] = (T)(p * sb);
     return (T)sb;
+  }
+  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
+    const int64_t t = d - 1 - l;
+    const T y = t <= d - 2 ? io.y[t * io.N + g] : T(0);
+    return emit_from(sg, li, l, y, io.s[t * io.N + g], io.dc[t * io.N + g]);
+  }
+  // chunked form: the stored state of the chunk's 8 steps (steps l0 .. l0+7,
+  // n of them valid) is loaded before the first, so the loads overlap
+  T pre_y[8], pre_s[8], pre_dc[8];
+  __device__ __forceinline__ void chunk_begin(int64_t l0, int n) {
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const int64_t t = d - 1 - (l0 + kk);
+      const bool v = kk < n;
+      pre_y[kk] = (v && t <= d - 2) ? io.y[t * io.N + g] : T(0);
+      pre_s[kk] = v ? io.s[t * io.N + g] : T(0);
+      pre_dc[kk] = v ? io.dc[t * io.N + g] : T(0);
+    }
+  }
+  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk) {
+    return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk]);
   }
   __device__ __forceinline__ void consume(const Staged<T> &, T r_sum, int, int64_t) { ybar = (double)r_sum; }
 
