@@ -267,21 +267,44 @@ def main():
             dist.barrier()
         return res, tot / steps, loop / max(nl, 1), nl, nk
 
-    # gradient: estimate + adjoint on the same points (dbgz_pnorm_grad), timed
-    # on the device like the forward step (host-side D2H of dU included)
+    # gradient: P and dP/dB of the factor model behind the workload,
+    # Sigma(B) = B B' + diag(psi) with the thresholds fixed in correlation
+    # units, through dbgz_pnorm_grad_sigma (estimate, adjoint loop, factor
+    # gradient GEMM, Cholesky adjoint on the device); timed on the device like
+    # the forward step.  The host finishes dP/dB = 2 G B (d x d x k).
+    Bm, psi = w.extra["B"], w.extra["psi"]
+
+    def make_fm(wk, Bx=None, precision=None):
+        Bx = Bm if Bx is None else Bx
+        S = Bx @ Bx.T + np.diag(psi)
+        sx = np.sqrt(np.diag(S))
+        opts = D.QMC_opts(m=wk.m, n_reps=wk.n_reps, max_pts=wk.m, max_abs_err=0.0)
+        return D.QMCData(S, wk.a * sx, wk.b * sx, opts, qmc_type="Richtmyer", shifts=wk.shifts,
+                         precision=precision, device=local), sx
+
+    def dP_dB(res, wk, sx):
+        _, _, _, da, db, G = res
+        G = G.copy()
+        # thresholds b_S = b s move with S_ii: d b_S / d S_ii = b / (2 s)
+        for gv, bv in ((da, wk.a), (db, wk.b)):
+            f = np.isfinite(bv)
+            G[np.flatnonzero(f), np.flatnonzero(f)] += gv[f] * bv[f] / (2 * sx[f])
+        return 2 * G @ Bm
+
     def grad_step(Qg, precision):
         flush.zero_()
         torch.cuda.synchronize()
-        r = D.qmc_pnorm_grad(Qg, precision=precision)
+        r = D.qmc_pnorm_grad_sigma(Qg, precision=precision)
         lib.dbgz_get_profile(ctx.handle, C.byref(prof))
         return r, prof.pnorm_ms, prof.kernel_launches
 
     Q = make(prec_mixed)
     peaks, peak_kind = _peaks()
     if args.only and args.grad:
+        Qg, _ = make_fm(w, precision=prec_mixed)
         for _ in range(args.warmup):
-            grad_step(Q, prec_mixed)
-        g = [grad_step(Q, prec_mixed)[1] for _ in range(args.steps)]
+            grad_step(Qg, prec_mixed)
+        g = [grad_step(Qg, prec_mixed)[1] for _ in range(args.steps)]
         if rank == 0:
             print(json.dumps({"precision": args.precision, "grad_ms_per_step": statistics.mean(g),
                               "workload": w.name, "samples": w.samples}), flush=True)
@@ -306,12 +329,22 @@ def main():
         (Po, _, _, _), mso, lo_ms, _, _ = timed(Q, D.PRECISIONS[name], max(2, args.steps // 2), 1)
         other[name] = {"ms_per_step": mso, "loop_ms": lo_ms, "P": Po}
 
-    grad_step(Q, prec_mixed)
+    Qg, sg = make_fm(w, precision=prec_mixed)
+    grad_step(Qg, prec_mixed)
     kg = max(2, args.steps // 2)
-    g_ms = [grad_step(Q, prec_mixed)[1] for _ in range(kg)]
+    g_ms, host_ms = [], []
+    for _ in range(kg):
+        res_g, gms, _ = grad_step(Qg, prec_mixed)
+        t = time.perf_counter()
+        dP_dB(res_g, w, sg)
+        host_ms.append(1e3 * (time.perf_counter() - t))
+        g_ms.append(gms)
     grad = {"precision": args.precision, "ms_per_step": statistics.mean(g_ms),
             "over_fwd": statistics.mean(g_ms) / ms_mix, "steps": kg,
-            "outputs": "P, dP/da, dP/db (original order), dP/dU (factor coordinates)"}
+            "host_dP_dB_ms": statistics.mean(host_ms),
+            "outputs": "P, dP/da, dP/db, dP/dSigma on the device; dP/dB = 2 G B on the host",
+            "model": "Sigma = B B' + diag(psi), B 1000x20, thresholds fixed in correlation units"}
+    Qg.close()
     # accuracy where P is O(0.1): the same covariance with the reference's own
     # bound design (+-k sqrt(S_ii), P(independent) = 0.25), same points
     from dbgenzpaper_b200 import workloads as W
@@ -323,13 +356,33 @@ def main():
     for name in ("fp32_split_bf16", "fp32_tf32", "fp32_simt"):
         Pm = D.qmc_pnorm(Qq, precision=D.PRECISIONS[name])[0]
         acc[name] = {"P": Pm, "abs_err": abs(Pm - acc["P_fp64"]), "rel_err": abs(Pm - acc["P_fp64"]) / acc["P_fp64"]}
-    g64 = D.qmc_pnorm_grad(Qq, precision=L.PREC_FP64)
-    gm = D.qmc_pnorm_grad(Qq, precision=prec_mixed)
-    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
-    acc["grad_" + args.precision] = {"rel_err_dP_da": rel(gm[3], g64[3]), "rel_err_dP_db": rel(gm[4], g64[4]),
-                                     "rel_err_dP_dU": rel(gm[5], g64[5]), "norm": "Frobenius, vs FP64 adjoint"}
-    del g64, gm
     Qq.close()
+    # gradient accuracy on the same model: mixed vs FP64 adjoint, and dP/dB
+    # against central differences (h = 1e-4) of FP64 estimates on common points
+    Qf, sq = make_fm(wq)
+    r64 = D.qmc_pnorm_grad_sigma(Qf, precision=L.PREC_FP64)
+    rm = D.qmc_pnorm_grad_sigma(Qf, precision=prec_mixed)
+    perm0 = Qf.C.perm.copy()
+    Qf.close()
+    dB64, dBm = dP_dB(r64, wq, sq), dP_dB(rm, wq, sq)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    fd = []
+    hB = 1e-4
+    for (i, j) in ((0, 0), (123, 5), (777, 19)):
+        vals, same = [], True
+        for sgn in (1, -1):
+            Bx = Bm.copy()
+            Bx[i, j] += sgn * hB
+            Qx, _ = make_fm(wq, Bx)
+            vals.append(D.qmc_pnorm(Qx, precision=L.PREC_FP64)[0])
+            same = same and np.array_equal(Qx.C.perm, perm0)
+            Qx.close()
+        f = (vals[0] - vals[1]) / (2 * hB)
+        fd.append({"entry": [i, j], "fd": f, "fp64_adjoint": float(dB64[i, j]),
+                   args.precision + "_adjoint": float(dBm[i, j]), "pivots_unchanged": bool(same)})
+    acc["grad_" + args.precision] = {"rel_err_dP_da": rel(rm[3], r64[3]), "rel_err_dP_db": rel(rm[4], r64[4]),
+                                     "rel_err_dP_dSigma": rel(rm[5], r64[5]), "rel_err_dP_dB": rel(dBm, dB64),
+                                     "norm": "Frobenius, vs FP64 adjoint", "fd_dP_dB": fd}
 
     # e2e: the public API from host buffers, upload and factorisation included
     def e2e_step():

@@ -315,6 +315,38 @@ def qmc_pnorm_grad(D, *, precision: Optional[int] = None, want_U: bool = True):
     return res.value, err.value, int(npts.value), da, db, dU
 
 
+def sigma_adjoint(D, dP_dU, dP_da=None, dP_db=None) -> np.ndarray:
+    """dP/dSigma (original order, symmetric; dP = sum_ij G_ij E_ij for a
+    symmetric perturbation E) from the outputs of qmc_pnorm_grad, through
+    the pivoted Cholesky (permutation held fixed) and the correlation scaling
+    (no counterpart in the reference).  For Sigma = B B' + diag(psi):
+    dP/dB = 2 G B."""
+    base = D.D if isinstance(D, QMCData_Distributions) else D
+    n = base.n
+    G = np.zeros((n, n), order="F")
+    dU = np.asfortranarray(np.asarray(dP_dU, dtype=np.float64))
+    da = None if dP_da is None else _f64(dP_da)
+    db = None if dP_db is None else _f64(dP_db)
+    L.check(L.lib().dbgz_problem_sigma_adjoint(base.handle, L.ptr(dU), L.ptr(da), L.ptr(db), L.ptr(G)),
+            base.ctx.handle)
+    return G
+
+
+def qmc_pnorm_grad_sigma(D, *, precision: Optional[int] = None):
+    """Estimate and gradients with respect to the inputs of QMCData, the
+    factor gradient kept on the device (dbgz_pnorm_grad_sigma):
+    -> (P, err, n_pts, dP_da, dP_db, dP_dSigma), all in the original order."""
+    base = D.D if isinstance(D, QMCData_Distributions) else D
+    prec = base.resolved_precision() if precision is None else int(precision)
+    n = base.n
+    res, err, npts = C.c_double(), C.c_double(), C.c_int64()
+    da, db = np.zeros(n), np.zeros(n)
+    G = np.zeros((n, n), order="F")
+    L.check(L.lib().dbgz_pnorm_grad_sigma(base.handle, prec, C.byref(res), C.byref(err), C.byref(npts),
+                                          L.ptr(da), L.ptr(db), L.ptr(G)), base.ctx.handle)
+    return res.value, err.value, int(npts.value), da, db, G
+
+
 # ---- primitives -------------------------------------------------------------
 def cholesky_genz(M, a, b, block_size=2**7, block_size2=2**9, block_size3=2**10,
                   block_size4=2**11, *, device=0) -> CholeskyGenz:

@@ -55,6 +55,7 @@ class DbgzProfile(C.Structure):
         ("kernel_launches", C.c_int64),
         ("prepare_ms", C.c_double),
         ("prepare_launches", C.c_int64),
+        ("sigma_adjoint_ms", C.c_double),
     ]
 
 
@@ -91,6 +92,8 @@ SIGNATURES = {
     "dbgz_problem_factor": (C.c_int, [_vp, _pd, _pi64, _pd, _pd, _pd, _pi64]),
     "dbgz_pnorm": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
     "dbgz_pnorm_grad": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
+    "dbgz_problem_sigma_adjoint": (C.c_int, [_vp, _pd, _pd, _pd, _pd]),
+    "dbgz_pnorm_grad_sigma": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
     "dbgz_pnorm_pass_noalloc": (C.c_int, [C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int64,
                                           C.c_int64, C.c_int64, _vp, _vp]),
     "dbgz_cholesky_genz": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,

@@ -46,6 +46,28 @@ __global__ void k_reduce_chunks(const double *csum, int64_t n_chunks, int64_t d,
   out[i] = v;
 }
 
+// Device-side assembly of the outputs: dU64 (d x d FP64, factor coordinates),
+// da/db in the original order and scale.  gemm[t*d + l] = sum_n y_l (p sbar_t).
+__global__ void k_grad_assemble(const void *gemm, int esz, const double *sums, const int64_t *perm,
+                                const double *scale, double inv, int64_t d, double *dU64, double *da, double *db) {
+  const int64_t t = blockIdx.y;
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < d; l += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    if (l < t) {
+      const size_t ix = (size_t)t * d + l;
+      v = (esz == 8 ? static_cast<const double *>(gemm)[ix] : (double)static_cast<const float *>(gemm)[ix]) * inv;
+    } else if (l == t) {
+      v = sums[2 * d + t] * inv;
+    }
+    dU64[t * d + l] = v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int64_t o = perm[t];
+    da[o] = sums[t] * inv / scale[o];
+    db[o] = sums[d + t] * inv / scale[o];
+  }
+}
+
 struct CublasHandle {
   cublasHandle_t h = nullptr;
   int device = -1;
@@ -55,7 +77,11 @@ struct CublasHandle {
 };
 thread_local CublasHandle g_cublas;
 
-int get_cublas(dbgz_ctx *ctx, cublasHandle_t *out) {
+}  // namespace
+
+// The calling thread's cuBLAS handle for the context's device, bound to the
+// context's stream.
+int dbgz_get_cublas(dbgz_ctx *ctx, cublasHandle_t *out) {
   if (!g_cublas.h || g_cublas.device != ctx->device) {
     if (g_cublas.h) cublasDestroy(g_cublas.h);
     g_cublas.h = nullptr;
@@ -69,12 +95,13 @@ int get_cublas(dbgz_ctx *ctx, cublasHandle_t *out) {
   return DBGZ_OK;
 }
 
-}  // namespace
-
 extern "C" int dbgz_first_dim_cdf(dbgz_problem *p);  // api.cu
 
-extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, double *err, int64_t *n_pts,
-                               double *dP_da, double *dP_db, double *dP_dU) {
+int dbgz_sigma_adjoint_dev(dbgz_problem *p, const double *dU, const double *da, const double *db,
+                           double *host_out);  // chol_adjoint.cu
+
+static int grad_impl(dbgz_problem *p, int precision, double *result, double *err, int64_t *n_pts, double *dP_da,
+                     double *dP_db, double *dP_dU, double *dP_dSigma) {
   if (!p || !result || !err || !n_pts) return DBGZ_ERR_INVALID_ARGUMENT;
   dbgz_ctx *ctx = p->ctx;
   if (precision < DBGZ_PREC_FP64 || precision > DBGZ_PREC_FP32_SIMT)
@@ -95,7 +122,7 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   const size_t arr = esz * (size_t)d * N;
   const size_t part = sizeof(double) * (size_t)n_tiles * 4 * d;
   const size_t total = 4 * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d * (kRedChunks + 1) +
-                       esz * (size_t)d * d + 8192;
+                       esz * (size_t)d * d + 8 * (size_t)d * d + 2 * 8 * (size_t)d + 16384;
   DBGZ_TRY(dbgz_ensure(ctx, p->grad_buf, total));
   char *base = (char *)p->grad_buf.p;
   auto take = [&](size_t bytes) {
@@ -117,6 +144,8 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   double *sums = (double *)take(3 * 8 * (size_t)d);
   double *csum = (double *)take(3 * 8 * (size_t)d * kRedChunks);
   void *dU = take(esz * (size_t)d * d);
+  double *dU64 = (double *)take(8 * (size_t)d * d);
+  double *da_o = (double *)take(8 * (size_t)d), *db_o = (double *)take(8 * (size_t)d);
   // rows the passes leave unwritten enter the dU GEMM: clear them
   DBGZ_CUDA_TRY(ctx, cudaMemsetAsync((char *)ga.y + esz * (size_t)(d - 1) * N, 0, esz * N, ctx->stream));
   DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ga.sbar, 0, esz * N, ctx->stream));
@@ -161,9 +190,10 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   }
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   // dU[l, t] = sum_n y[l][n] (p sbar)[t][n]: (d x N) x (N x d), sample-contiguous rows
-  if (dP_dU) {
+  const bool want_U = dP_dU || dP_dSigma;
+  if (want_U) {
     cublasHandle_t h;
-    DBGZ_TRY(get_cublas(ctx, &h));
+    DBGZ_TRY(dbgz_get_cublas(ctx, &h));
     cublasStatus_t cs;
     if (precision == DBGZ_PREC_FP64) {
       const double one = 1.0, zero = 0.0;
@@ -177,18 +207,19 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
     }
     if (cs != CUBLAS_STATUS_SUCCESS) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
   }
-  std::vector<double> reps(n_reps), hs(3 * d), scale(d), hU;
-  std::vector<int64_t> perm(d);
+  const double inv = 1.0 / ((double)m * (double)n_reps);
+  k_grad_assemble<<<dim3((unsigned)((d + 255) / 256), (unsigned)d), 256, 0, ctx->stream>>>(
+      dU, (int)esz, sums, (const int64_t *)p->perm.p, (const double *)p->scale.p, inv, d, dU64, da_o, db_o);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  if (dP_dSigma) DBGZ_TRY(dbgz_sigma_adjoint_dev(p, dU64, da_o, db_o, dP_dSigma));
+  std::vector<double> reps(n_reps);
   int dev_status = 0;
   cudaMemcpyAsync(reps.data(), p->reps.p, 8 * n_reps, cudaMemcpyDeviceToHost, ctx->stream);
-  cudaMemcpyAsync(hs.data(), sums, 8 * 3 * d, cudaMemcpyDeviceToHost, ctx->stream);
-  cudaMemcpyAsync(perm.data(), p->perm.p, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
-  cudaMemcpyAsync(scale.data(), p->scale.p, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
+  if (dP_da) cudaMemcpyAsync(dP_da, da_o, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
+  if (dP_db) cudaMemcpyAsync(dP_db, db_o, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
+  if (dP_dU) cudaMemcpyAsync(dP_dU, dU64, 8 * (size_t)d * d, cudaMemcpyDeviceToHost, ctx->stream);
   if (tensor) cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  if (dP_dU) {
-    hU.resize((size_t)d * d * (esz / 4));
-    cudaMemcpyAsync(hU.data(), dU, esz * (size_t)d * d, cudaMemcpyDeviceToHost, ctx->stream);
-  }
   if (prof) cudaEventRecord(ctx->ev[1], ctx->stream);
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (dev_status != 0)
@@ -208,25 +239,16 @@ extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, d
   *result = res;
   *err = 3.0 * std::sqrt(acc / (double)(n_reps - 1));
   *n_pts = m;
-  const double inv = 1.0 / ((double)m * (double)n_reps);
-  for (int64_t t = 0; t < d; ++t) {
-    const int64_t orig = perm[t];
-    if (dP_da) dP_da[orig] = hs[t] * inv / scale[orig];
-    if (dP_db) dP_db[orig] = hs[d + t] * inv / scale[orig];
-  }
-  if (dP_dU) {
-    for (int64_t t = 0; t < d; ++t)
-      for (int64_t l = 0; l < d; ++l) {
-        double v = 0.0;
-        if (l < t) {
-          const size_t ix = (size_t)t * d + l;  // column t, row l of the GEMM result
-          v = (esz == 8 ? reinterpret_cast<const double *>(hU.data())[ix]
-                        : (double)reinterpret_cast<const float *>(hU.data())[ix]) * inv;
-        } else if (l == t) {
-          v = hs[2 * d + t] * inv;
-        }
-        dP_dU[(size_t)t * d + l] = v;
-      }
-  }
   return DBGZ_OK;
+}
+
+extern "C" int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, double *err, int64_t *n_pts,
+                               double *dP_da, double *dP_db, double *dP_dU) {
+  return grad_impl(p, precision, result, err, n_pts, dP_da, dP_db, dP_dU, nullptr);
+}
+
+extern "C" int dbgz_pnorm_grad_sigma(dbgz_problem *p, int precision, double *result, double *err, int64_t *n_pts,
+                                     double *dP_da, double *dP_db, double *dP_dSigma) {
+  if (!dP_dSigma) return DBGZ_ERR_INVALID_ARGUMENT;
+  return grad_impl(p, precision, result, err, n_pts, dP_da, dP_db, nullptr, dP_dSigma);
 }

@@ -126,6 +126,7 @@ typedef struct dbgz_profile {
   int64_t kernel_launches;  /* every kernel it launched                     */
   double prepare_ms;        /* last dbgz_prepare: upload + factorisation    */
   int64_t prepare_launches; /* kernels the last dbgz_prepare launched       */
+  double sigma_adjoint_ms;  /* last dbgz_problem_sigma_adjoint              */
 } dbgz_profile;
 int dbgz_set_profiling(dbgz_ctx *ctx, int enable);
 int dbgz_get_profile(const dbgz_ctx *ctx, dbgz_profile *out);
@@ -201,6 +202,24 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err,
  * arrays of the working type (N = samples of the pass) plus partial sums. */
 int dbgz_pnorm_grad(dbgz_problem *p, int precision, double *result, double *err,
                     int64_t *n_pts, double *dP_da, double *dP_db, double *dP_dU);
+
+/* dP/dSigma from the outputs of dbgz_pnorm_grad, through the pivoted
+ * Cholesky (permutation held fixed) and the correlation scaling of
+ * dbgz_prepare; no counterpart in the reference.  dP_dU is the factor
+ * gradient (d x d column-major, upper triangle read), dP_da / dP_db the
+ * bound gradients in the original order (NULL = zero).  dP_dSigma (d x d
+ * column-major, symmetric) is the gradient for symmetric perturbations:
+ * dP = sum_ij dP_dSigma[i,j] E[i,j] for symmetric E, so that for
+ * Sigma = B B' + diag(psi), dP/dB = 2 dP_dSigma B.  FP64 throughout
+ * (cuBLAS TRMM/TRSM/GEMM on the context's stream). */
+int dbgz_problem_sigma_adjoint(dbgz_problem *p, const double *dP_dU, const double *dP_da,
+                               const double *dP_db, double *dP_dSigma);
+/* dbgz_pnorm_grad followed by dbgz_problem_sigma_adjoint with the factor
+ * gradient kept on the device: P, its 3 SEM error, dP/da, dP/db (original
+ * order, may be NULL) and dP_dSigma (required, as above).  No counterpart in
+ * the reference. */
+int dbgz_pnorm_grad_sigma(dbgz_problem *p, int precision, double *result, double *err,
+                          int64_t *n_pts, double *dP_da, double *dP_db, double *dP_dSigma);
 
 /* ---- allocation-free pass -------------------------------------------
  * No counterpart in the reference.  Some callers cannot let a library

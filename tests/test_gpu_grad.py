@@ -106,3 +106,99 @@ def test_fp32_gradients_close_to_fp64(dbgz, prec, tol, n):
     assert abs(P - P64) <= 1e-4 * abs(P64) + 1e-6
     for g, g64 in ((da, da64), (db, db64), (dU, dU64)):
         assert np.linalg.norm(g - g64) <= tol * np.linalg.norm(g64), (np.linalg.norm(g - g64) / np.linalg.norm(g64))
+
+
+def _sigma_problem(n, seed, finite_a=True):
+    rng = np.random.default_rng(seed)
+    R = W.correlation(W.rand_spd(n, 1.0, rng))
+    s = rng.uniform(0.5, 2.0, n)
+    S = R * np.outer(s, s)  # a covariance, not a correlation: exercises the scaling
+    # bounds without ties in the first pivot scores (a symmetric design such
+    # as +-k sqrt(S_ii) makes every first score equal, and a perturbation of
+    # Sigma_ii then moves the pivot order)
+    lo, up = -rng.uniform(0.3, 2.0, n) * s, rng.uniform(0.3, 2.0, n) * s
+    if not finite_a:
+        lo = np.full(n, -np.inf)
+    return S, lo, up, rng.random((n - 1, 4))
+
+
+def _P(D, S, lo, up, sh):
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=384, n_reps=4, max_pts=384, max_abs_err=0.0), shifts=sh)
+    P = D.qmc_pnorm(Q, precision=L.PREC_FP64)[0]
+    perm = Q.C.perm.copy()
+    Q.close()
+    return P, perm
+
+
+@pytest.mark.parametrize("n,finite_a", [(12, True), (48, False)])
+def test_sigma_gradient_matches_finite_differences(dbgz, n, finite_a):
+    D = dbgz
+    S, lo, up, sh = _sigma_problem(n, 3000 + n, finite_a)
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=384, n_reps=4, max_pts=384, max_abs_err=0.0), shifts=sh)
+    P, _, _, da, db, G = D.qmc_pnorm_grad_sigma(Q, precision=L.PREC_FP64)
+    perm0 = Q.C.perm.copy()
+    Q.close()
+    assert np.allclose(G, G.T, rtol=1e-12, atol=1e-14 * np.abs(G).max())
+    rng = np.random.default_rng(n)
+    h = 1e-6
+    pairs = [(i, i) for i in rng.choice(n, 3, replace=False)]
+    pairs += [tuple(sorted(rng.choice(n, 2, replace=False))) for _ in range(6)]
+    checked = 0
+    for i, j in pairs:
+        E = np.zeros((n, n))
+        E[i, j] = E[j, i] = h
+        Pp, pp = _P(D, S + E, lo, up, sh)
+        Pm, pm = _P(D, S - E, lo, up, sh)
+        if not (np.array_equal(pp, perm0) and np.array_equal(pm, perm0)):
+            continue  # the pivot order moved: not a derivative of the same estimate
+        fd = (Pp - Pm) / (2 * h)
+        an = G[i, i] if i == j else 2 * G[i, j]
+        assert abs(an - fd) <= 2e-6 * max(abs(fd), abs(P)) + 1e-11, (i, j, an, fd)
+        checked += 1
+    assert checked >= len(pairs) - 1
+    # bounds at fixed Sigma through the public gradient
+    for i in rng.choice(n, 3, replace=False):
+        e = np.zeros(n)
+        e[i] = h
+        fd = (_P(D, S, lo, up + e, sh)[0] - _P(D, S, lo, up - e, sh)[0]) / (2 * h)
+        assert abs(db[i] - fd) <= 2e-6 * max(abs(fd), abs(P)) + 1e-11
+
+
+def test_factor_model_dB(dbgz):
+    # Sigma = B B' + diag(psi): dP/dB = 2 G B, checked by central differences on B
+    D = dbgz
+    rng = np.random.default_rng(77)
+    n, k = 40, 3
+    B = rng.normal(0, 0.5, (n, k))
+    psi = rng.uniform(0.2, 1.0, n)
+    S = B @ B.T + np.diag(psi)
+    lo = np.full(n, -np.inf)
+    up = rng.uniform(0.0, 2.0, n) * np.sqrt(np.diag(S))
+    sh = rng.random((n - 1, 4))
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=384, n_reps=4, max_pts=384, max_abs_err=0.0), shifts=sh)
+    P, _, _, _, _, G = D.qmc_pnorm_grad_sigma(Q, precision=L.PREC_FP64)
+    # the host-side entry point on the outputs of qmc_pnorm_grad gives the same matrix
+    _, _, _, da, db, dU = D.qmc_pnorm_grad(Q, precision=L.PREC_FP64)
+    assert np.array_equal(D.sigma_adjoint(Q, dU, da, db), G)
+    perm0 = Q.C.perm.copy()
+    Q.close()
+    dB = 2 * G @ B
+    h = 1e-6
+    for i, j in [(0, 0), (5, 1), (n - 1, 2), (17, 0)]:
+        Bp, Bm = B.copy(), B.copy()
+        Bp[i, j] += h
+        Bm[i, j] -= h
+        Pp, pp = _P(D, Bp @ Bp.T + np.diag(psi), lo, up, sh)
+        Pm, pm = _P(D, Bm @ Bm.T + np.diag(psi), lo, up, sh)
+        assert np.array_equal(pp, perm0) and np.array_equal(pm, perm0)
+        fd = (Pp - Pm) / (2 * h)
+        assert abs(dB[i, j] - fd) <= 2e-6 * max(abs(fd), abs(P)) + 1e-11, (i, j, dB[i, j], fd)
+
+
+def test_fp32_sigma_gradient_close_to_fp64(dbgz):
+    D = dbgz
+    S, lo, up, sh = _sigma_problem(200, 4200)
+    Q = D.QMCData(S, lo, up, D.QMC_opts(m=2048, n_reps=4, max_pts=2048, max_abs_err=0.0), shifts=sh)
+    G64 = D.qmc_pnorm_grad_sigma(Q, precision=L.PREC_FP64)[5]
+    G = D.qmc_pnorm_grad_sigma(Q, precision=L.PREC_FP32_SPLIT_BF16)[5]
+    assert np.linalg.norm(G - G64) <= 3e-3 * np.linalg.norm(G64)
