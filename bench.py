@@ -150,6 +150,57 @@ def cpu_baseline(w, threads: int, target_s: float = 12.0):
     }
 
 
+def run_c4(args):
+    """The batch configuration: 4096 problems, d ~ U{16..256}, Sobol 2^14 x 8
+    each, one dbgz_pnorm_batch call (upload, batched FP64 Cholesky, batched
+    loop, read-back).  Rank 0 only; one JSON line."""
+    import torch
+    import dbgenzpaper_b200 as D
+    from dbgenzpaper_b200 import _lib as L
+    from dbgenzpaper_b200 import workloads as W
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    n_prob = 256 if args.quick else 4096
+    ws = W.c4(n_problems=n_prob)
+    probs = [(w.Sigma, w.a, w.b) for w in ws]
+    ush = [w.ushifts for w in ws]
+    opts = D.QMC_opts(m=ws[0].m, n_reps=ws[0].n_reps, max_pts=ws[0].m, max_abs_err=0.0)
+    ctx = D.get_context(0)
+    lib = L.lib()
+    lib.dbgz_set_profiling(ctx.handle, 1)
+    prof = L.DbgzProfile()
+    out = {}
+    for name, prec in (("fp32_simt", L.PREC_FP32_SIMT), ("fp64", L.PREC_FP64)):
+        for _ in range(args.warmup):
+            D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=prec)
+        wall, dev, loop, prep = [], [], [], []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            P, err = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=prec)
+            wall.append(1e3 * (time.perf_counter() - t))
+            lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+            dev.append(prof.pnorm_ms)
+            loop.append(prof.loop_ms)
+            prep.append(prof.prepare_ms)
+        out[name] = {"e2e_ms": statistics.mean(wall), "device_ms": statistics.mean(dev),
+                     "loop_ms": statistics.mean(loop), "prepare_ms": statistics.mean(prep), "P": P}
+    dims = np.array([w.d for w in ws])
+    samples = float(opts.m * opts.n_reps * len(ws))
+    P32, P64 = out["fp32_simt"].pop("P"), out["fp64"].pop("P")
+    line = {
+        "metric": "C4 batch: 4096 MVN probabilities (d ~ U{16..256}) per call", "value": out["fp32_simt"]["e2e_ms"],
+        "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"c4_{len(ws)}_problems_sobol", "points": opts.m, "shifts": opts.n_reps,
+                   "sum_d": int(dims.sum()), "sample_dims": samples * float(dims.mean())},
+        "modes": out, "max_abs_err_fp32_vs_fp64": float(np.max(np.abs(P32 - P64))),
+        "sample_dims_per_s_fp32": samples * float(dims.mean() - 1) / (out["fp32_simt"]["loop_ms"] * 1e-3),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -206,9 +257,13 @@ def main():
     ap.add_argument("--only", action="store_true",
                     help="time only --precision (no FP64/other modes/accuracy/e2e/CPU legs); for profiling")
     ap.add_argument("--grad", action="store_true", help="with --only: time the gradient call instead")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c4"],
+                    help="c3: the headline line (default); c4: the 4096-problem batch, a separate line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "c4":
+        return run_c4(args)
 
     import torch
     import dbgenzpaper_b200 as D

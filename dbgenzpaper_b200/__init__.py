@@ -347,6 +347,57 @@ def qmc_pnorm_grad_sigma(D, *, precision: Optional[int] = None):
     return res.value, err.value, int(npts.value), da, db, G
 
 
+def qmc_pnorm_batch(problems, opts: Optional[QMCOpts] = None, rng=None, qmc_type="Richtmyer", *,
+                    shifts=None, ushifts=None, sobol_dirnums=None, sobol_first=None,
+                    precision: Optional[int] = None, device: int = 0, context: Optional[Context] = None,
+                    return_ranks: bool = False):
+    """P and 3 SEM of many independent problems in one call (dbgz_pnorm_batch;
+    no counterpart in the reference, which loops over QMCData/qmc_pnorm!).
+
+    problems: sequence of (Sigma, a, b).  One pass of opts.m points x
+    opts.n_reps shifts per problem.  shifts / ushifts: sequences of the
+    per-problem (d-1, n_reps) arrays (drawn from rng when None).  Returns
+    (P, err) arrays (and the ranks with return_ranks); a problem that is not
+    full rank raises, unless return_ranks is set (its P is then NaN)."""
+    qmc_type = str(qmc_type).lstrip(":")
+    if qmc_type not in ("Richtmyer", "Sobol"):
+        raise ValueError("qmc_type must be 'Richtmyer' or 'Sobol'")
+    opts = QMC_opts() if opts is None else opts
+    rng = np.random.default_rng() if rng is None else rng
+    ctx = get_context(device) if context is None else context
+    dims = np.array([np.asarray(p[0]).shape[0] for p in problems], dtype=np.int64)
+    Sig = np.concatenate([np.ravel(np.asarray(p[0], dtype=np.float64), order="F") for p in problems])
+    a = np.concatenate([_f64(p[1]) for p in problems])
+    b = np.concatenate([_f64(p[2]) for p in problems])
+    R = opts.n_reps
+    sh = ush = V = None
+    first = 0
+    if qmc_type == "Richtmyer":
+        if shifts is None:
+            shifts = [rng.random((d - 1, R)) for d in dims]
+        sh = np.concatenate([np.ravel(np.asarray(x, dtype=np.float64), order="F") for x in shifts])
+    else:
+        if ushifts is None:
+            ushifts = [rng.integers(0, 2**64, size=(d - 1, R), dtype=np.uint64, endpoint=False) for d in dims]
+        ush = np.concatenate([np.ravel(np.asarray(x, dtype=np.uint64), order="F") for x in ushifts])
+        if sobol_dirnums is not None:
+            V = np.ascontiguousarray(sobol_dirnums, dtype=np.uint32)
+        first = (2 * opts.m - 1) + 1 if sobol_first is None else int(sobol_first)
+    prec = (L.PREC_FP64 if opts.T == np.float64 else DEFAULT_FP32_PRECISION) if precision is None else int(precision)
+    n = len(problems)
+    P, err = np.zeros(n), np.zeros(n)
+    ranks = np.zeros(n, dtype=np.int64)
+    co = opts.to_c()
+    st = L.lib().dbgz_pnorm_batch(ctx.handle, n, L.ptr(dims, C.c_int64), L.ptr(Sig), L.ptr(a), L.ptr(b),
+                                  C.byref(co), L.QMC_RICHTMYER if qmc_type == "Richtmyer" else L.QMC_SOBOL,
+                                  prec, L.ptr(sh), L.ptr(ush, C.c_uint64), L.ptr(V, C.c_uint32), first,
+                                  L.ptr(P), L.ptr(err), L.ptr(ranks, C.c_int64))
+    if return_ranks and st == L.ERR_RANK_DEFICIENT:
+        return P, err, ranks
+    L.check(st, ctx.handle)
+    return (P, err, ranks) if return_ranks else (P, err)
+
+
 # ---- primitives -------------------------------------------------------------
 def cholesky_genz(M, a, b, block_size=2**7, block_size2=2**9, block_size3=2**10,
                   block_size4=2**11, *, device=0) -> CholeskyGenz:

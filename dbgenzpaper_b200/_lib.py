@@ -94,6 +94,9 @@ SIGNATURES = {
     "dbgz_pnorm_grad": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
     "dbgz_problem_sigma_adjoint": (C.c_int, [_vp, _pd, _pd, _pd, _pd]),
     "dbgz_pnorm_grad_sigma": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
+    "dbgz_pnorm_batch": (C.c_int, [_vp, C.c_int64, _pi64, _pd, _pd, _pd, C.POINTER(DbgzOpts), C.c_int, C.c_int,
+                                   _pd, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_int64, _pd, _pd,
+                                   _pi64]),
     "dbgz_pnorm_pass_noalloc": (C.c_int, [C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int64,
                                           C.c_int64, C.c_int64, _vp, _vp]),
     "dbgz_cholesky_genz": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,

@@ -20,27 +20,12 @@
 // on the whole GPU.
 #include "internal.cuh"
 #include "detmath.h"
+#include "chol_dev.cuh"
 #include <cfloat>
 
 namespace {
 
 constexpr int kStepThreads = 1024;
-
-__device__ __forceinline__ bool julia_min_less(double x, double y) {
-  // Base.isgreater order used by findmin/argmin: NaN lowest, -0.0 < +0.0.
-  if (x != x) return y == y;
-  if (y != y) return false;
-  if (x < y) return true;
-  if (x == y && x == 0.0) return signbit(x) && !signbit(y);
-  return false;
-}
-
-__device__ __forceinline__ void argmin_combine(double &v, int64_t &i, double v2, int64_t i2) {
-  if (julia_min_less(v2, v) || (!julia_min_less(v, v2) && i2 < i)) {
-    v = v2;
-    i = i2;
-  }
-}
 
 __global__ void k_diag_absmax(const double *M, int64_t n, double *out) {
   __shared__ double sh[32];
@@ -89,171 +74,19 @@ __global__ void k_scale_apply(double *M, int64_t n, double *a, double *b, const 
   }
 }
 
-// One bs1 block [i0, i1] of cholesky_genz! inside the bs2 panel ending at
-// ii1 (0-based, inclusive), src/cholesky.jl:494-572.  One CTA.
+// One bs1 block of cholesky_genz! (src/cholesky.jl:494-572), one CTA.
 __global__ void __launch_bounds__(kStepThreads)
-k_genz_block(double *M, int64_t n, double *a, double *b, double *dvec, double *svec,
-             double *ovec, int64_t *perm, int64_t i0, int64_t i1, int64_t ii1,
-             const double *eps0_ptr, int64_t *rank) {
-  __shared__ double red_v[kStepThreads / 32];
-  __shared__ int64_t red_i[kStepThreads / 32];
-  __shared__ int64_t sh_im;
-  __shared__ double sh_mii, sh_yi;
-  __shared__ int sh_stop;
-  const double c2 = dm_div(1.0, dm_sqrt(2.0));
-  const double is2pi = dm_div(2.0, dm_sqrt(dm_mul(2.0, M_PI)));
-  const double eps0 = eps0_ptr[0];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (rank[0] < n) return;  // an earlier block already stopped
-  for (int64_t k = i0 + tid; k <= ii1; k += blockDim.x) dvec[k] = 0.0;
-  __syncthreads();
-  for (int64_t i = i0; i <= i1; ++i) {
-    // pivot scores :500-512, then argmin :514
-    double bv = 0.0;
-    int64_t bi = INT64_MAX;
-    for (int64_t k = i + tid; k <= ii1; k += blockDim.x) {
-      double m_kk = dm_sub(M[k * n + k], dvec[k]);
-      m_kk = m_kk < 0 ? 0.0 : dm_sqrt(m_kk);
-      double a_k = dm_mul(dm_div(dm_sub(a[k], svec[k]), m_kk), c2);
-      double b_k = dm_mul(dm_div(dm_sub(b[k], svec[k]), m_kk), c2);
-      double o = dm_sub(det_erf(b_k), det_erf(a_k));
-      ovec[k] = o;
-      if (bi == INT64_MAX) { bv = o; bi = k; }
-      else argmin_combine(bv, bi, o, k);
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
-      if (lane + off < 32 && i2 != INT64_MAX) {
-        if (bi == INT64_MAX) { bv = v2; bi = i2; }
-        else argmin_combine(bv, bi, v2, i2);
-      }
-    }
-    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
-    __syncthreads();
-    if (tid == 0) {
-      double v = red_v[0];
-      int64_t im = red_i[0];
-      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-        if (red_i[w] == INT64_MAX) continue;
-        if (im == INT64_MAX) { v = red_v[w]; im = red_i[w]; }
-        else argmin_combine(v, im, red_v[w], red_i[w]);
-      }
-      double d_ii = ovec[im];
-      double m_ii = dm_sub(M[im * n + im], dvec[im]);
-      if (im != i) {  // :518-523
-        int64_t tp = perm[i]; perm[i] = perm[im]; perm[im] = tp;
-        double t;
-        t = dvec[im]; dvec[im] = dvec[i]; dvec[i] = t;
-        t = svec[im]; svec[im] = svec[i]; svec[i] = t;
-        t = a[im]; a[im] = a[i]; a[i] = t;
-        t = b[im]; b[im] = b[i]; b[i] = t;
-      }
-      sh_im = im;
-      sh_mii = m_ii;
-      sh_yi = d_ii;  // carried to the y_i step
-    }
-    __syncthreads();
-    const int64_t im = sh_im;
-    if (im != i) {  // :525-530: rows over columns i0..n, then full columns
-      for (int64_t k = i0 + tid; k < n; k += blockDim.x) {
-        double t = M[k * n + i];
-        M[k * n + i] = M[k * n + im];
-        M[k * n + im] = t;
-      }
-      __syncthreads();
-      for (int64_t k = tid; k < n; k += blockDim.x) {
-        double t = M[i * n + k];
-        M[i * n + k] = M[im * n + k];
-        M[im * n + k] = t;
-      }
-      __syncthreads();
-    }
-    if (tid == 0) {
-      double m_ii = sh_mii;
-      double d_ii = sh_yi;
-      int stop = 0;
-      if (m_ii > eps0) {
-        m_ii = dm_sqrt(m_ii);
-      } else {
-        rank[0] = i;  // 0-based i == reference's i - 1
-        stop = 1;
-      }
-      if (!stop) {
-        M[i * n + i] = m_ii;
-        double a_norm = dm_div(dm_sub(a[i], svec[i]), m_ii);
-        double b_norm = dm_div(dm_sub(b[i], svec[i]), m_ii);
-        double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
-        double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
-        sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), d_ii);
-        sh_mii = m_ii;
-      }
-      sh_stop = stop;
-    }
-    __syncthreads();
-    if (sh_stop) return;
-    const double m_ii = sh_mii, y_i = sh_yi;
-    if (i == i0) {  // :547-554
-      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
-        double m_ij = dm_div(M[j * n + i], m_ii);
-        M[j * n + i] = m_ij;
-        M[i * n + j] = m_ij;
-        dvec[j] = dm_add(dvec[j], dm_mul(m_ij, m_ij));
-        svec[j] = dm_add(svec[j], dm_mul(y_i, m_ij));
-      }
-    } else if (i < ii1) {  // :555-570
-      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
-        double acc = 0.0;
-        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[l * n + j], M[i * n + l], acc);
-        double m_ij = dm_div(dm_sub(M[i * n + j], acc), m_ii);
-        M[j * n + i] = m_ij;
-        M[i * n + j] = m_ij;
-        dvec[j] = dm_add(dvec[j], dm_mul(m_ij, m_ij));
-        svec[j] = dm_add(svec[j], dm_mul(y_i, m_ij));
-      }
-    }
-    __syncthreads();
-  }
+k_genz_block(double *M, int64_t n, double *a, double *b, double *dvec, double *svec, double *ovec, int64_t *perm,
+             int64_t i0, int64_t i1, int64_t ii1, const double *eps0_ptr, int64_t *rank) {
+  cholk::genz_block_dev(M, n, a, b, dvec, svec, ovec, perm, i0, i1, ii1, eps0_ptr, rank);
 }
 
-// C[j,k] -= sum_{l=p0..p1} A(l,j) * B(l,k) for j,k in [c0, c1], one
-// ascending fma chain per element.  A(l,j) = M[j,l] (row form, the
-// reference's lower-triangle copy) when a_row, else M[l,j]; B(l,k) = M[l,k].
-constexpr int kTile = 32;
+// C[j,k] -= sum_{l=p0..p1} A(l,j) B(l,k) over [c0, c1]^2, one tile per CTA.
+constexpr int kTile = cholk::kTile;
 __global__ void __launch_bounds__(256)
 k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, int a_row) {
-  __shared__ double As[kTile][kTile + 1];
-  __shared__ double Bs[kTile][kTile + 1];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-  const int64_t j0 = c0 + blockIdx.x * (int64_t)kTile, k0 = c0 + blockIdx.y * (int64_t)kTile;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t l0 = p0; l0 <= p1; l0 += kTile) {
-    for (int r = ty; r < kTile; r += 8) {
-      // As[l][c] = A(l0 + l, j0 + c); Bs[l][c] = B(l0 + l, k0 + c)
-      int64_t l = l0 + tx, jj = j0 + r, kk = k0 + r;
-      if (a_row) {
-        int64_t lr = l0 + r, jc = j0 + tx;  // coalesced over j
-        As[r][tx] = (lr <= p1 && jc <= c1) ? M[lr * n + jc] : 0.0;
-      } else {
-        As[tx][r] = (l <= p1 && jj <= c1) ? M[jj * n + l] : 0.0;
-      }
-      Bs[tx][r] = (l <= p1 && kk <= c1) ? M[kk * n + l] : 0.0;
-    }
-    __syncthreads();
-    const int lmax = (int)((p1 - l0 + 1) < kTile ? (p1 - l0 + 1) : kTile);
-    for (int l = 0; l < lmax; ++l) {
-      double av = As[l][tx];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) acc[r] = dm_fma(av, Bs[l][ty + 8 * r], acc[r]);
-    }
-    __syncthreads();
-  }
-  const int64_t j = j0 + tx;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    int64_t k = k0 + ty + 8 * r;
-    if (j <= c1 && k <= c1) M[k * n + j] = dm_sub(M[k * n + j], acc[r]);
-  }
+  cholk::schur_tile_dev(M, n, p0, p1, c0, c1, a_row, c0 + blockIdx.x * (int64_t)kTile,
+                        c0 + blockIdx.y * (int64_t)kTile);
 }
 
 // ldiv!(UpperTriangular(M[p0:p1,p0:p1])', M[p0:p1, c0:c1]): forward

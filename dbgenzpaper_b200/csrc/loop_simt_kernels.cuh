@@ -53,17 +53,15 @@ struct SimtSmem {
   double red[NT / 32];
 };
 
+// One tile of 128 samples of the problem P (all NT threads of the CTA; Yw
+// is the CTA's slot of the Y workspace).
 // Policy: pol::Forward<...> or pol::Adjoint<...> (policies.cuh).
 template <typename T, typename Policy>
-__global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SimtSmem<T> &sm = *reinterpret_cast<SimtSmem<T> *>(smem_raw);
+__device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &sm, T *Yw, int64_t tile) {
   const int tid = threadIdx.x;
   const int64_t d = P.d, nY = d - 1;
-  T *Yw = P.yws + (int64_t)blockIdx.x * P.Dp * TS;
   const int64_t last_g0 = ((nY - 1) / G) * G;  // start of the last group
-
-  for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
+  {
     const int r = tid;  // sample row for the scalar threads (tid < TS)
     const int64_t k = tile / P.tiles_per_shift;
     const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
@@ -174,6 +172,46 @@ __global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
       for (int w = 0; w < NT / 32; ++w) sum += sm.red[w];
       P.partials[tile] = sum;
     }
+    __syncthreads();
+  }
+}
+
+template <typename T, typename Policy>
+__global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SimtSmem<T> &sm = *reinterpret_cast<SimtSmem<T> *>(smem_raw);
+  T *Yw = P.yws + (int64_t)blockIdx.x * P.Dp * TS;
+  for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) simt_tile<T, Policy>(P, sm, Yw, tile);
+}
+
+// Many problems in one launch: a work item is a run of tiles of one problem
+// (items ordered largest problem first); persistent CTAs take items from a
+// global counter.  Each problem's parameters (pointers into packed arrays,
+// its own first-dimension constants) are copied to shared memory per item;
+// the Y workspace slots are sized for the largest problem (Dp).
+struct BatchItem {
+  int32_t prob, tile0, ntiles, pad;
+};
+
+template <typename T, typename Policy>
+__global__ void __launch_bounds__(NT, 2) k_genz_simt_batch(const SimtParams<T> *params, const BatchItem *items,
+                                                           int64_t n_items, unsigned long long *counter, T *yws,
+                                                           int64_t Dp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SimtSmem<T> &sm = *reinterpret_cast<SimtSmem<T> *>(smem_raw);
+  __shared__ SimtParams<T> Ps;
+  __shared__ long long cur;
+  T *Yw = yws + (int64_t)blockIdx.x * Dp * TS;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      cur = (long long)atomicAdd(counter, 1ull);
+      if (cur < n_items) Ps = params[items[cur].prob];
+    }
+    __syncthreads();
+    const long long it = cur;
+    if (it >= n_items) break;
+    const BatchItem bi = items[it];
+    for (int64_t tile = bi.tile0; tile < (int64_t)bi.tile0 + bi.ntiles; ++tile) simt_tile<T, Policy>(Ps, sm, Yw, tile);
     __syncthreads();
   }
 }

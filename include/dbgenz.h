@@ -255,6 +255,25 @@ int dbgz_pnorm_pass_noalloc(int64_t d, const double *U, const double *a, const d
                             const double *q, const double *shifts, int64_t m, int64_t n_reps,
                             int64_t n_base, double *qmc_reps, void *stream);
 
+/* Many independent problems in one call (QMCData + qmc_pnorm! for each,
+ * one pass of opts->m points x opts->n_reps shifts; no reference
+ * counterpart, the reference loops over problems on the host).  Problem k
+ * has dimension dims[k] (2 <= d <= min(512, chol_block_size2)); Sigma holds
+ * the column-major d_k x d_k matrices one after another, a and b the d_k
+ * bounds one after another, shifts (Richtmyer) or ushifts (Sobol) the
+ * (d_k - 1) x n_reps blocks one after another; sobol_dirnums is one table
+ * for the largest d - 1 (NULL: the library's own) and sobol_first the
+ * first Sobol index (as in dbgz_prepare).  precision: DBGZ_PREC_FP64, or any
+ * FP32 mode (the batch runs the FP32 SIMT loop for all of them).  results
+ * and errs (may be NULL) receive P and 3 SEM per problem, ranks (may be
+ * NULL) the Cholesky rank; a problem that is not full rank gets NaN and the
+ * call returns DBGZ_ERR_RANK_DEFICIENT after finishing the others. */
+int dbgz_pnorm_batch(dbgz_ctx *ctx, int64_t n_problems, const int64_t *dims, const double *Sigma,
+                     const double *a, const double *b, const dbgz_opts *opts, int qmc_type,
+                     int precision, const double *shifts, const uint64_t *ushifts,
+                     const uint32_t *sobol_dirnums, int64_t sobol_first, double *results,
+                     double *errs, int64_t *ranks);
+
 /* ---- primitives of the path (device compute, host buffers) ---------- */
 
 /* cholesky_genz!(M, a, b, bs1, bs2, bs3, bs4) (src/cholesky.jl:445-628):
