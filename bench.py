@@ -201,6 +201,62 @@ def run_c4(args):
     return 0
 
 
+def run_c5(args):
+    """The banded configuration: d = 10^4 AR(1) (rho = 0.9), factor truncated to
+    64 super-diagonals, a = -inf, Sobol 2^18 x 10; P (FP32 and FP64 banded
+    loops) and P with dP/da, dP/db (FP32 adjoint, chunked over samples).
+    Rank 0 only; one JSON line."""
+    import torch
+    import dbgenzpaper_b200 as D
+    from dbgenzpaper_b200 import _lib as L
+    from dbgenzpaper_b200 import workloads as W
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    w = W.c5(m=2**14 if args.quick else 2**18)
+    band = w.extra["bandwidth"]
+    ctx = D.get_context(0)
+    lib = L.lib()
+    lib.dbgz_set_profiling(ctx.handle, 1)
+    prof = L.DbgzProfile()
+    opts = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0)
+    t = time.perf_counter()
+    Q = D.QMCDataSparse(w.Sigma, w.a, w.b, opts, qmc_type="Sobol", ushifts=w.ushifts)
+    Q.truncate_band(band)
+    prep_ms = 1e3 * (time.perf_counter() - t)
+    lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+    out = {"prepare_host_ms": prep_ms, "prepare_device_ms": prof.prepare_ms}
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        ms = []
+        for _ in range(k):
+            r = fn()
+            lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+            ms.append(prof.pnorm_ms)
+        return r, statistics.mean(ms)
+
+    (P32, e32, _), out["fp32_ms"] = timed(lambda: D.qmc_pnorm(Q, precision=L.PREC_FP32_SIMT), args.steps)
+    (P64, e64, _), out["fp64_ms"] = timed(lambda: D.qmc_pnorm(Q, precision=L.PREC_FP64), max(1, args.steps // 2))
+    g, out["fp32_grad_ms"] = timed(lambda: D.qmc_pnorm_grad(Q, precision=L.PREC_FP32_SIMT), max(1, args.steps // 2))
+    Q.close()
+    samples = float(w.m * w.n_reps)
+    line = {
+        "metric": "C5 banded d=1e4 MVN P time (FP32) and P + dP/db", "value": out["fp32_ms"], "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "dtype": "fp32",
+        "data": "synthetic",
+        "config": {"workload": w.name, "d": w.d, "bandwidth": band, "points": w.m, "shifts": w.n_reps,
+                   "samples": samples},
+        "modes": out, "P_fp32": P32, "P_fp64": P64, "abs_err_fp32_vs_fp64": abs(P32 - P64),
+        "qmc_3sem_fp64": e64, "grad_over_fwd": out["fp32_grad_ms"] / out["fp32_ms"],
+        "dP_db_norm": float(np.linalg.norm(g[4])), "P_grad_call": g[0],
+        "sample_dims_per_s_fp32": samples * (w.d - 1) / (out["fp32_ms"] * 1e-3),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -257,13 +313,16 @@ def main():
     ap.add_argument("--only", action="store_true",
                     help="time only --precision (no FP64/other modes/accuracy/e2e/CPU legs); for profiling")
     ap.add_argument("--grad", action="store_true", help="with --only: time the gradient call instead")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c4"],
-                    help="c3: the headline line (default); c4: the 4096-problem batch, a separate line")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c5"],
+                    help="c3: the headline line (default); c4: the 4096-problem batch; c5: the banded "
+                         "d = 10^4 problem (separate lines)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "c4":
         return run_c4(args)
+    if args.workload == "c5":
+        return run_c5(args)
 
     import torch
     import dbgenzpaper_b200 as D

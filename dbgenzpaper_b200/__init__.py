@@ -73,6 +73,11 @@ class Context:
         L.check(self._lib.dbgz_release_cached(self.handle, C.byref(n)), self.handle)
         return int(n.value)
 
+    def set_state_budget(self, nbytes: int) -> None:
+        """Cap the device memory of stored forward state in gradient calls
+        (larger sample counts run in chunks of tiles)."""
+        L.check(self._lib.dbgz_set_state_budget(self.handle, int(nbytes)), self.handle)
+
     def close(self):
         if self.handle:
             if self._lib.dbgz_destroy(self.handle) == L.OK:
@@ -309,6 +314,7 @@ def qmc_pnorm_grad(D, *, precision: Optional[int] = None, want_U: bool = True):
     n = base.n
     res, err, npts = C.c_double(), C.c_double(), C.c_int64()
     da, db = np.zeros(n), np.zeros(n)
+    want_U = want_U and base._structure == L.STRUCTURE_DENSE  # the banded path gives da, db only
     dU = np.zeros((n, n), order="F") if want_U else None
     L.check(L.lib().dbgz_pnorm_grad(base.handle, prec, C.byref(res), C.byref(err), C.byref(npts), L.ptr(da),
                                     L.ptr(db), L.ptr(dU)), base.ctx.handle)

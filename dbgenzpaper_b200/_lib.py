@@ -81,6 +81,7 @@ SIGNATURES = {
     "dbgz_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "dbgz_destroy": (C.c_int, [_vp]),
     "dbgz_release_cached": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "dbgz_set_state_budget": (C.c_int, [_vp, C.c_uint64]),
     "dbgz_last_error": (C.c_char_p, [_vp]),
     "dbgz_set_profiling": (C.c_int, [_vp, C.c_int]),
     "dbgz_get_profile": (C.c_int, [_vp, C.POINTER(DbgzProfile)]),

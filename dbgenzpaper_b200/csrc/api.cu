@@ -162,6 +162,12 @@ int dbgz_destroy(dbgz_ctx *ctx) {
   return DBGZ_OK;
 }
 
+int dbgz_set_state_budget(dbgz_ctx *ctx, uint64_t bytes) {
+  if (!ctx || bytes == 0) return DBGZ_ERR_INVALID_ARGUMENT;
+  ctx->state_budget = (size_t)bytes;
+  return DBGZ_OK;
+}
+
 int dbgz_release_cached(dbgz_ctx *ctx, uint64_t *freed_bytes) {
   if (!ctx) return DBGZ_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
@@ -422,7 +428,7 @@ int dbgz_problem_free(dbgz_problem *p) {
                     &p->shifts32, &p->V,   &p->ushifts, &p->tgt64,      &p->tgt32,   &p->U32,       &p->Uhi,
                     &p->Ulo,   &p->Utf,     &p->Ub,      &p->Ub32,       &p->Ubhi,    &p->Ublo,      &p->Ubtf,
                     &p->grad_buf, &p->yws, &p->partials, &p->reps,      &p->csc_colptr, &p->csc_row, &p->csc_val64,
-                    &p->csc_val32};
+                    &p->csc_val32, &p->cscb_colptr, &p->cscb_row, &p->cscb_val64, &p->cscb_val32};
   for (DevBuf *b : bufs) dbgz_release(*b);
   if (p->ctx) p->ctx->live_problems -= 1;
   delete p;
@@ -445,7 +451,8 @@ int dbgz_problem_truncate_band(dbgz_problem *p, int64_t bandwidth) {
   p->band = bandwidth;
   DBGZ_TRY(dbgz_band_dev(ctx, p->d, (double *)p->U.p, bandwidth));
   DevBuf *derived[] = {&p->U32, &p->Uhi,  &p->Ulo,  &p->Utf,  &p->Ub,         &p->Ub32,    &p->Ubhi,
-                       &p->Ublo, &p->Ubtf, &p->csc_colptr, &p->csc_row, &p->csc_val64, &p->csc_val32};
+                       &p->Ublo, &p->Ubtf, &p->csc_colptr, &p->csc_row, &p->csc_val64, &p->csc_val32,
+                       &p->cscb_colptr, &p->cscb_row, &p->cscb_val64, &p->cscb_val32};
   for (DevBuf *b : derived) dbgz_release(*b);
   p->ldU = 0;
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));

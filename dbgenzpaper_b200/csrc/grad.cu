@@ -38,20 +38,21 @@ __global__ void k_reduce_rows(const double *ga, const double *gb, const double *
   o[d + t] = b;
   o[2 * d + t] = u;
 }
-__global__ void k_reduce_chunks(const double *csum, int64_t n_chunks, int64_t d, double *out) {
+__global__ void k_reduce_chunks(const double *csum, int64_t n_chunks, int64_t d, double *out, int accumulate) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // i in [0, 3d)
   if (i >= 3 * d) return;
   double v = 0.0;
   for (int64_t c = 0; c < n_chunks; ++c) v += csum[c * 3 * d + i];
-  out[i] = v;
+  out[i] = accumulate ? out[i] + v : v;
 }
 
-// Device-side assembly of the outputs: dU64 (d x d FP64, factor coordinates),
-// da/db in the original order and scale.  gemm[t*d + l] = sum_n y_l (p sbar_t).
+// Device-side assembly of the outputs: dU64 (d x d FP64, factor coordinates;
+// skipped when null), da/db in the original order and scale.  gemm[t*d + l] = sum_n y_l (p sbar_t).
 __global__ void k_grad_assemble(const void *gemm, int esz, const double *sums, const int64_t *perm,
                                 const double *scale, double inv, int64_t d, double *dU64, double *da, double *db) {
   const int64_t t = blockIdx.y;
-  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < d; l += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; dU64 && l < d;
+       l += (int64_t)gridDim.x * blockDim.x) {
     double v = 0.0;
     if (l < t) {
       const size_t ix = (size_t)t * d + l;
@@ -106,23 +107,32 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   dbgz_ctx *ctx = p->ctx;
   if (precision < DBGZ_PREC_FP64 || precision > DBGZ_PREC_FP32_SIMT)
     return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "pnorm_grad: bad precision %d", precision);
-  if (p->structure != DBGZ_STRUCTURE_DENSE)
-    return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm_grad: the adjoint is built for the dense structure");
-  if (p->cdf_form != DBGZ_CDF_ERF)
+  const bool sparse = p->structure == DBGZ_STRUCTURE_SPARSE;
+  if (sparse && (dP_dU || dP_dSigma))
+    return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm_grad: the banded path gives dP/da and dP/db only");
+  if (p->cdf_form != DBGZ_CDF_ERF && !sparse)
     return dbgz_fail(ctx, DBGZ_ERR_UNSUPPORTED, "pnorm_grad: the adjoint is built for the erf-form CDF");
   cudaSetDevice(ctx->device);
   const dbgz_opts &o = p->opts;
   const int64_t d = p->d, m = o.m, n_reps = o.n_reps;
-  const int64_t tps = (m + 127) / 128, n_tiles = tps * n_reps, N = n_tiles * 128;
+  const int64_t tps = (m + 127) / 128, n_tiles = tps * n_reps;
   const size_t esz = precision == DBGZ_PREC_FP64 ? 8 : 4;
   DBGZ_TRY(dbgz_first_dim_cdf(p));
-  if (precision != DBGZ_PREC_FP64 && !p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
+  if (precision != DBGZ_PREC_FP64 && !p->U32.p && !sparse) DBGZ_TRY(dbgz_make_U32(p));
   if (!p->Ub.p) DBGZ_TRY(dbgz_make_Ub(p));
-  // one allocation for the pass: 4 state arrays, p, 3 partial arrays, sums, dU
+  // samples per chunk: as many whole tiles as the context's state budget
+  // allows (forward-store, adjoint, reduction and the dU GEMM run per chunk;
+  // the GEMM accumulates across chunks)
+  const size_t tile_bytes = 128 * ((sparse ? 3 : 4) * esz * (size_t)d + 8) + 3 * 4 * 8 * (size_t)d;
+  const int64_t chunk =
+      std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)(ctx->state_budget / tile_bytes)));
+  const int64_t N = chunk * 128;
+  // one allocation: y, s, dc (+ p sbar on the dense path), p, 3 partial arrays, sums, dU
   const size_t arr = esz * (size_t)d * N;
-  const size_t part = sizeof(double) * (size_t)n_tiles * 4 * d;
-  const size_t total = 4 * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d * (kRedChunks + 1) +
-                       esz * (size_t)d * d + 8 * (size_t)d * d + 2 * 8 * (size_t)d + 16384;
+  const size_t part = sizeof(double) * (size_t)chunk * 4 * d;
+  const size_t total = (sparse ? 3 : 4) * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d * (kRedChunks + 1) +
+                       (sparse ? 0 : esz * (size_t)d * d + 8 * (size_t)d * d) + 2 * 8 * (size_t)d +
+                       8 * (size_t)n_tiles + 16384;
   DBGZ_TRY(dbgz_ensure(ctx, p->grad_buf, total));
   char *base = (char *)p->grad_buf.p;
   auto take = [&](size_t bytes) {
@@ -135,7 +145,7 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   ga.y = take(arr);
   ga.s = take(arr);
   ga.dc = take(arr);
-  ga.sbar = take(arr);
+  ga.sbar = sparse ? nullptr : take(arr);
   ga.p = (double *)take(8 * (size_t)N);
   ga.ga = (double *)take(part);
   ga.gb = (double *)take(part);
@@ -143,12 +153,17 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   ga.dc1 = p->dc1;
   double *sums = (double *)take(3 * 8 * (size_t)d);
   double *csum = (double *)take(3 * 8 * (size_t)d * kRedChunks);
-  void *dU = take(esz * (size_t)d * d);
-  double *dU64 = (double *)take(8 * (size_t)d * d);
+  void *dU = sparse ? nullptr : take(esz * (size_t)d * d);
+  double *dU64 = sparse ? nullptr : (double *)take(8 * (size_t)d * d);
   double *da_o = (double *)take(8 * (size_t)d), *db_o = (double *)take(8 * (size_t)d);
-  // rows the passes leave unwritten enter the dU GEMM: clear them
-  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync((char *)ga.y + esz * (size_t)(d - 1) * N, 0, esz * N, ctx->stream));
-  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ga.sbar, 0, esz * N, ctx->stream));
+  // the adjoint pass writes per-tile values too (zeros); keep them away from
+  // the forward pass's tile sums, which are reduced after the last chunk
+  double *adj_tiles = (double *)take(8 * (size_t)n_tiles);
+  if (!sparse) {
+    // rows the passes leave unwritten enter the dU GEMM: clear them
+    DBGZ_CUDA_TRY(ctx, cudaMemsetAsync((char *)ga.y + esz * (size_t)(d - 1) * N, 0, esz * N, ctx->stream));
+    DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ga.sbar, 0, esz * N, ctx->stream));
+  }
 
   DBGZ_TRY(dbgz_ensure(ctx, p->partials, sizeof(double) * n_tiles));
   DBGZ_TRY(dbgz_ensure(ctx, p->reps, sizeof(double) * n_reps));
@@ -169,46 +184,53 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   pa.dc1 = p->dc1;
   pa.gen_base = p->gen_base;
   pa.grad = ga;
-  const bool tensor = precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16;
-  // forward, keeping the state
-  pa.kind = kLoopForwardStore;
-  if (tensor) DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
-  else DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
-  DBGZ_TRY(dbgz_finalize_pass(p, (const double *)p->partials.p, tps, 0, m, (double *)p->reps.p));
-  // adjoint on the anti-transposed factor
-  pa.kind = kLoopAdjoint;
-  if (tensor) DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
-  else DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
-  {
-    const int64_t rows = n_tiles * 4, chunk = (rows + kRedChunks - 1) / kRedChunks;
-    const int64_t n_chunks = (rows + chunk - 1) / chunk;
-    k_reduce_rows<<<dim3((unsigned)((d + 127) / 128), (unsigned)n_chunks), 128, 0, ctx->stream>>>(
-        ga.ga, ga.gb, ga.gu, rows, d, chunk, csum);
-    dbgz_count_launch(ctx);
-    k_reduce_chunks<<<(unsigned)((3 * d + 255) / 256), 256, 0, ctx->stream>>>(csum, n_chunks, d, sums);
-    dbgz_count_launch(ctx);
-  }
-  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
-  // dU[l, t] = sum_n y[l][n] (p sbar)[t][n]: (d x N) x (N x d), sample-contiguous rows
+  const bool tensor = !sparse && (precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16);
+  auto run = [&](int kind, int64_t t0, int64_t t1) -> int {
+    pa.kind = kind;
+    pa.tile0 = t0;
+    double *tiles = kind == kLoopAdjoint ? adj_tiles : (double *)p->partials.p;
+    if (sparse) return dbgz_loop_sparse(p, pa, precision, tiles, t1);
+    if (tensor) return dbgz_loop_umma(p, pa, precision, tiles, t1);
+    return dbgz_loop_simt(p, pa, precision, tiles, t1);
+  };
   const bool want_U = dP_dU || dP_dSigma;
-  if (want_U) {
-    cublasHandle_t h;
-    DBGZ_TRY(dbgz_get_cublas(ctx, &h));
-    cublasStatus_t cs;
-    if (precision == DBGZ_PREC_FP64) {
-      const double one = 1.0, zero = 0.0;
-      cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, (int)N, &one, (const double *)ga.y, (int)N,
-                       (const double *)ga.sbar, (int)N, &zero, (double *)dU, (int)d);
-    } else {
-      const float one = 1.0f, zero = 0.0f;
-      cs = cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, (int)N, &one, ga.y, CUDA_R_32F, (int)N,
-                        ga.sbar, CUDA_R_32F, (int)N, &zero, dU, CUDA_R_32F, (int)d, CUBLAS_COMPUTE_32F_FAST_TF32,
-                        CUBLAS_GEMM_DEFAULT);
+  for (int64_t t0 = 0; t0 < n_tiles; t0 += chunk) {
+    const int64_t t1 = std::min(n_tiles, t0 + chunk);
+    // forward keeping the state, then the adjoint on the anti-transposed factor
+    DBGZ_TRY(run(kLoopForwardStore, t0, t1));
+    DBGZ_TRY(run(kLoopAdjoint, t0, t1));
+    const int64_t rows = (t1 - t0) * 4, per = (rows + kRedChunks - 1) / kRedChunks;
+    const int64_t n_chunks = (rows + per - 1) / per;
+    k_reduce_rows<<<dim3((unsigned)((d + 127) / 128), (unsigned)n_chunks), 128, 0, ctx->stream>>>(
+        ga.ga, ga.gb, ga.gu, rows, d, per, csum);
+    dbgz_count_launch(ctx);
+    k_reduce_chunks<<<(unsigned)((3 * d + 255) / 256), 256, 0, ctx->stream>>>(csum, n_chunks, d, sums, t0 > 0);
+    dbgz_count_launch(ctx);
+    // dU[l, t] += sum_n y[l][n] (p sbar)[t][n] over the chunk's samples:
+    // (d x Nc) x (Nc x d), sample-contiguous rows of leading dimension N
+    if (want_U) {
+      cublasHandle_t h;
+      DBGZ_TRY(dbgz_get_cublas(ctx, &h));
+      cublasStatus_t cs;
+      const int nc = (int)((t1 - t0) * 128);
+      if (precision == DBGZ_PREC_FP64) {
+        const double one = 1.0, beta = t0 > 0 ? 1.0 : 0.0;
+        cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, nc, &one, (const double *)ga.y, (int)N,
+                         (const double *)ga.sbar, (int)N, &beta, (double *)dU, (int)d);
+      } else {
+        const float one = 1.0f, beta = t0 > 0 ? 1.0f : 0.0f;
+        cs = cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, nc, &one, ga.y, CUDA_R_32F, (int)N, ga.sbar,
+                          CUDA_R_32F, (int)N, &beta, dU, CUDA_R_32F, (int)d, CUBLAS_COMPUTE_32F_FAST_TF32,
+                          CUBLAS_GEMM_DEFAULT);
+      }
+      if (cs != CUBLAS_STATUS_SUCCESS)
+        return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
     }
-    if (cs != CUBLAS_STATUS_SUCCESS) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
   }
+  DBGZ_TRY(dbgz_finalize_pass(p, (const double *)p->partials.p, tps, 0, m, (double *)p->reps.p));
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   const double inv = 1.0 / ((double)m * (double)n_reps);
-  k_grad_assemble<<<dim3((unsigned)((d + 255) / 256), (unsigned)d), 256, 0, ctx->stream>>>(
+  k_grad_assemble<<<dim3(sparse ? 1u : (unsigned)((d + 255) / 256), (unsigned)d), 256, 0, ctx->stream>>>(
       dU, (int)esz, sums, (const int64_t *)p->perm.p, (const double *)p->scale.p, inv, d, dU64, da_o, db_o);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());

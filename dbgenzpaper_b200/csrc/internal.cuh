@@ -54,6 +54,7 @@ struct dbgz_ctx {
   std::multimap<size_t, void *> pool;
   size_t pool_bytes = 0;
   int64_t live_problems = 0;  // problems created on this context and not yet freed
+  size_t state_budget = size_t(48) << 30;  // bytes of stored forward state a gradient call may hold
 };
 
 // Counts a kernel launch of the library (for dbgz_profile).
@@ -95,6 +96,8 @@ struct dbgz_problem {
   DevBuf grad_buf;       // forward state and partial gradients of dbgz_pnorm_grad
   // sparse (banded) structure: CSC of the strict upper factor
   DevBuf csc_colptr, csc_row, csc_val64, csc_val32;
+  DevBuf cscb_colptr, cscb_row, cscb_val64, cscb_val32;  // CSC of the anti-transposed factor (adjoint)
+  int64_t bandwidth_b = 1;
   int64_t nnz = 0, bandwidth = 0, band = 0;  // band > 0: entries beyond it dropped
   // workspaces
   DevBuf yws, partials, reps;
@@ -145,6 +148,7 @@ struct PassArgs {
   int qmc_type;
   int cdf_form;
   double c1, dc1;
+  int64_t tile0 = 0;  // run tiles [tile0, n_tiles) only (sample chunks of the adjoint)
 };
 int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);

@@ -38,6 +38,7 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.n_reps = pa.n_reps;
   P.tiles_per_shift = (pa.m + TS - 1) / TS;
   P.n_tiles = n_tiles;
+  P.tile0 = pa.tile0;
   P.Dp = ((d - 1 + G - 1) / G) * G;
   P.gen.qmc_type = pa.qmc_type;
   P.gen.n_bits = pa.n_bits;
@@ -71,13 +72,14 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.io.gb = pa.grad.gb;
   P.io.gu = pa.grad.gu;
   P.io.dc1 = pa.grad.dc1;
+  P.io.tile0 = pa.tile0;
   const size_t smem = sizeof(SimtSmem<T>);
   auto kern = k_genz_simt<T, Policy>;
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   DBGZ_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
   if (per_sm < 1) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "simt loop: kernel does not fit on an SM");
-  int64_t grid = std::min<int64_t>(n_tiles, (int64_t)per_sm * ctx->num_sms);
+  int64_t grid = std::min<int64_t>(n_tiles - pa.tile0, (int64_t)per_sm * ctx->num_sms);
   DBGZ_TRY(dbgz_ensure(ctx, p->yws, sizeof(T) * (size_t)P.Dp * TS * grid));
   P.yws = (T *)p->yws.p;
   kern<<<(unsigned)grid, NT, smem, ctx->stream>>>(P);

@@ -28,6 +28,7 @@ struct TgtOf<float> {
 template <typename T>
 struct SimtParams {
   int64_t d, m, n_reps, tiles_per_shift, n_tiles, Dp;
+  int64_t tile0;  // tiles [tile0, n_tiles) of the pass
   dbgz::GenParams gen;
   const T *U;  // d x d col-major coefficient array (policies.cuh)
   const typename TgtOf<T>::type *tgt;
@@ -181,7 +182,8 @@ __global__ void __launch_bounds__(NT, 2) k_genz_simt(SimtParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SimtSmem<T> &sm = *reinterpret_cast<SimtSmem<T> *>(smem_raw);
   T *Yw = P.yws + (int64_t)blockIdx.x * P.Dp * TS;
-  for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) simt_tile<T, Policy>(P, sm, Yw, tile);
+  for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles; tile += gridDim.x)
+    simt_tile<T, Policy>(P, sm, Yw, tile);
 }
 
 // Many problems in one launch: a work item is a run of tiles of one problem

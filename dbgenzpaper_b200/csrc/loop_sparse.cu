@@ -16,6 +16,7 @@
 // staged in shared memory per block of 32 dimensions.
 #include "internal.cuh"
 #include "genz_step.cuh"
+#include "policies.cuh"
 #include <algorithm>
 #include <vector>
 
@@ -49,20 +50,13 @@ struct SparseParams {
   int W;                   // ring size (power of two)
   int ring_in_smem;
   int max_block_nnz;       // staging capacity (entries)
+  int64_t tile0;           // tiles [tile0, n_tiles) of the pass
+  pol::GradIO<T> io;
 };
 
-template <typename T>
-__device__ __forceinline__ T shift_of(const dbgz::GenParams &g, int64_t idx);
-template <>
-__device__ __forceinline__ double shift_of<double>(const dbgz::GenParams &g, int64_t idx) {
-  return g.shift64 ? g.shift64[idx] : 0.0;
-}
-template <>
-__device__ __forceinline__ float shift_of<float>(const dbgz::GenParams &g, int64_t idx) {
-  return g.shift32 ? g.shift32[idx] : 0.0f;
-}
-
-template <typename T, typename Step, int GEN>
+// Policy: pol::Forward<T, GEN, STORE> or pol::Adjoint<T, GEN> (policies.cuh);
+// the adjoint runs on the CSC of the anti-transposed factor.
+template <typename T, typename Policy>
 __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // layout: [staged rowval int32 x cap][staged nzval T x cap][colptr of block (CB+1)][ring]
@@ -70,23 +64,18 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   T *sval = reinterpret_cast<T *>(smem_raw + ((sizeof(int32_t) * P.max_block_nnz + 15) & ~size_t(15)));
   int *scol = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sval) +
                                       ((sizeof(T) * P.max_block_nnz + 15) & ~size_t(15)));
-  double *sq = reinterpret_cast<double *>(scol + CB + 2 + 2);
-  T *ssh = reinterpret_cast<T *>(sq + CB);
-  typename TgtT<T>::type *stg =
-      reinterpret_cast<typename TgtT<T>::type *>(reinterpret_cast<unsigned char *>(ssh) + 16 * ((sizeof(T) * CB + 15) / 16));
-  T *ring = reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(stg) + sizeof(*stg) * CB);
+  T *ring = reinterpret_cast<T *>(scol + CB + 4);
+  __shared__ pol::Staged<T> sg;
   __shared__ double red[TS / 32];
   const int r = threadIdx.x;
   const int Wm = P.W - 1;
   T *yr = P.ring_in_smem ? ring : P.yglob + (int64_t)blockIdx.x * P.W * TS;
-  dbgz::GenParams gen = P.gen;
-  gen.qmc_type = GEN;
 
-  for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
+  for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
     const int64_t k = tile / P.tiles_per_shift;
     const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
-    Step st;
-    st.init(P.c1, P.dc1, P.up1);
+    Policy pl;
+    pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
     for (int64_t i0 = 0; i0 < P.nY; i0 += CB) {
       const int nb = (int)(P.nY - i0 < CB ? P.nY - i0 : CB);
       // stage the CSC columns i0+1 .. i0+nb (targets of y-indices i0..i0+nb-1)
@@ -100,16 +89,12 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
           sval[e] = P.nzval[p0 + e];
         }
       if (r <= nb) scol[r] = (int)(P.colptr[i0 + 1 + r] - p0);
-      if (r < nb) {
-        sq[r] = gen.q ? gen.q[i0 + r] : 0.0;
-        ssh[r] = shift_of<T>(gen, k * P.nY + i0 + r);
-        stg[r] = P.tgt[i0 + r + 1];
-      }
+      pl.stage(sg, P.tgt, r, i0, nb);
       __syncthreads();
 #pragma unroll 1
       for (int li = 0; li < nb; ++li) {
         const int64_t i = i0 + li;
-        T y = st.quantile(gen, P.d, j, k, i, sq[li], ssh[li]);
+        const T y = pl.emit(sg, li, i);
         yr[(i & Wm) * TS + r] = y;
         T s = T(0);
         const int q0 = scol[li], q1 = scol[li + 1];
@@ -119,11 +104,11 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
           for (int q = q0; q < q1; ++q)
             s = fma(yr[(P.rowval[p0 + q] & Wm) * TS + r], P.nzval[p0 + q], s);
         }
-        const auto tg = stg[li];
-        st.cdf(s, tg.a, tg.b, tg.inv_u, 0);
+        pl.consume(sg, s, li, i);
       }
     }
-    double pv = (j < P.m) ? st.p : 0.0;
+    pl.tile_end(P.tgt, r, r >> 5, tile, j < P.m);
+    double pv = pl.tile_value(j < P.m);
     for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
     if ((r & 31) == 0) red[r >> 5] = pv;
     __syncthreads();
@@ -162,31 +147,33 @@ __global__ void k_col_fill(const double *U, int64_t d, int64_t band, const int64
 
 }  // namespace
 
-int dbgz_build_csc(dbgz_problem *p) {
+// CSC of the strict upper triangle of U (d x d, column-major), limited to
+// p->band super-diagonals when set; returns nnz and the bandwidth.
+static int build_csc_from(dbgz_problem *p, const double *U, DevBuf &colptr_b, DevBuf &row_b, DevBuf &v64_b,
+                          DevBuf &v32_b, int64_t *nnz_out, int64_t *bw_out) {
   dbgz_ctx *ctx = p->ctx;
   const int64_t d = p->d;
   std::vector<int64_t> cnt(d), colptr(d + 1);
-  DBGZ_TRY(dbgz_ensure(ctx, p->csc_colptr, sizeof(int64_t) * (d + 1)));
-  k_col_count<<<(unsigned)((d + 127) / 128), 128, 0, ctx->stream>>>((const double *)p->U.p, d, p->band,
-                                                                     (int64_t *)p->csc_colptr.p);
+  DBGZ_TRY(dbgz_ensure(ctx, colptr_b, sizeof(int64_t) * (d + 1)));
+  k_col_count<<<(unsigned)((d + 127) / 128), 128, 0, ctx->stream>>>(U, d, p->band, (int64_t *)colptr_b.p);
   dbgz_count_launch(ctx);
-  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(cnt.data(), p->csc_colptr.p, sizeof(int64_t) * d, cudaMemcpyDeviceToHost,
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(cnt.data(), colptr_b.p, sizeof(int64_t) * d, cudaMemcpyDeviceToHost,
                                      ctx->stream));
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   colptr[0] = 0;
   for (int64_t t = 0; t < d; ++t) colptr[t + 1] = colptr[t] + cnt[t];
   const int64_t nnz = colptr[d];
-  p->nnz = nnz;
-  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(p->csc_colptr.p, colptr.data(), sizeof(int64_t) * (d + 1),
-                                     cudaMemcpyHostToDevice, ctx->stream));
-  DBGZ_TRY(dbgz_ensure(ctx, p->csc_row, sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
-  DBGZ_TRY(dbgz_ensure(ctx, p->csc_val64, sizeof(double) * std::max<int64_t>(nnz, 1)));
-  DBGZ_TRY(dbgz_ensure(ctx, p->csc_val32, sizeof(float) * std::max<int64_t>(nnz, 1)));
+  *nnz_out = nnz;
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(colptr_b.p, colptr.data(), sizeof(int64_t) * (d + 1), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+  DBGZ_TRY(dbgz_ensure(ctx, row_b, sizeof(int32_t) * std::max<int64_t>(nnz, 1)));
+  DBGZ_TRY(dbgz_ensure(ctx, v64_b, sizeof(double) * std::max<int64_t>(nnz, 1)));
+  DBGZ_TRY(dbgz_ensure(ctx, v32_b, sizeof(float) * std::max<int64_t>(nnz, 1)));
   DevBuf minrow;
   DBGZ_TRY(dbgz_ensure(ctx, minrow, sizeof(int32_t) * d));
-  k_col_fill<<<(unsigned)((d + 127) / 128), 128, 0, ctx->stream>>>(
-      (const double *)p->U.p, d, p->band, (const int64_t *)p->csc_colptr.p, (int32_t *)p->csc_row.p,
-      (double *)p->csc_val64.p, (float *)p->csc_val32.p, (int32_t *)minrow.p);
+  k_col_fill<<<(unsigned)((d + 127) / 128), 128, 0, ctx->stream>>>(U, d, p->band, (const int64_t *)colptr_b.p,
+                                                                    (int32_t *)row_b.p, (double *)v64_b.p,
+                                                                    (float *)v32_b.p, (int32_t *)minrow.p);
   dbgz_count_launch(ctx);
   std::vector<int32_t> mr(d);
   cudaMemcpyAsync(mr.data(), minrow.p, sizeof(int32_t) * d, cudaMemcpyDeviceToHost, ctx->stream);
@@ -195,13 +182,23 @@ int dbgz_build_csc(dbgz_problem *p) {
   if (e != cudaSuccess) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "build_csc: %s", cudaGetErrorString(e));
   int64_t bw = 1;
   for (int64_t t = 1; t < d; ++t) bw = std::max<int64_t>(bw, t - mr[t]);
+  *bw_out = bw;
+  return DBGZ_OK;
+}
+
+int dbgz_build_csc(dbgz_problem *p) {
+  int64_t nnz = 0, bw = 1;
+  DBGZ_TRY(build_csc_from(p, (const double *)p->U.p, p->csc_colptr, p->csc_row, p->csc_val64, p->csc_val32, &nnz,
+                          &bw));
+  p->nnz = nnz;
   p->bandwidth = bw;
   return DBGZ_OK;
 }
 
-template <typename T, typename Step>
+template <typename T, typename Policy>
 static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
   dbgz_ctx *ctx = p->ctx;
+  const bool adj = pa.kind == kLoopAdjoint;
   SparseParams<T> P{};
   P.d = pa.d;
   P.nY = pa.d - 1;
@@ -209,6 +206,7 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.n_reps = pa.n_reps;
   P.tiles_per_shift = (pa.m + TS - 1) / TS;
   P.n_tiles = n_tiles;
+  P.tile0 = pa.tile0;
   P.gen.qmc_type = pa.qmc_type;
   P.gen.n_bits = pa.n_bits;
   P.gen.gen_base = pa.gen_base;
@@ -218,32 +216,43 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.gen.shift32 = (const float *)p->shifts32.p;
   P.gen.V = (const uint32_t *)p->V.p;
   P.gen.ushift = (const uint64_t *)p->ushifts.p;
-  P.colptr = (const int64_t *)p->csc_colptr.p;
-  P.rowval = (const int32_t *)p->csc_row.p;
-  P.nzval = sizeof(T) == 8 ? (const T *)p->csc_val64.p : (const T *)p->csc_val32.p;
+  P.colptr = (const int64_t *)(adj ? p->cscb_colptr.p : p->csc_colptr.p);
+  P.rowval = (const int32_t *)(adj ? p->cscb_row.p : p->csc_row.p);
+  if (sizeof(T) == 8) P.nzval = (const T *)(adj ? p->cscb_val64.p : p->csc_val64.p);
+  else P.nzval = (const T *)(adj ? p->cscb_val32.p : p->csc_val32.p);
   P.tgt = sizeof(T) == 8 ? (const typename TgtT<T>::type *)p->tgt64.p : (const typename TgtT<T>::type *)p->tgt32.p;
   P.c1 = pa.c1;
   P.dc1 = pa.dc1;
   P.up1 = 1.0 - pa.c1 - pa.dc1;
   P.partials = partials;
+  P.io.N = pa.grad.N;
+  P.io.y = (T *)pa.grad.y;
+  P.io.s = (T *)pa.grad.s;
+  P.io.dc = (T *)pa.grad.dc;
+  P.io.sbar = (T *)pa.grad.sbar;
+  P.io.p = pa.grad.p;
+  P.io.ga = pa.grad.ga;
+  P.io.gb = pa.grad.gb;
+  P.io.gu = pa.grad.gu;
+  P.io.dc1 = pa.grad.dc1;
+  P.io.tile0 = pa.tile0;
+  const int64_t bwid = adj ? p->bandwidth_b : p->bandwidth;
   int W = 1;
-  while (W < p->bandwidth + 1) W <<= 1;
+  while (W < bwid + 1) W <<= 1;
   P.W = W;
   const int ring_cap = sizeof(T) == 8 ? 128 : 256;
   P.ring_in_smem = W <= ring_cap;
-  P.max_block_nnz = (int)std::min<int64_t>(CB * std::min<int64_t>(p->bandwidth, 256), 8192);
+  P.max_block_nnz = (int)std::min<int64_t>(CB * std::min<int64_t>(bwid, 256), 8192);
   const size_t stage = ((sizeof(int32_t) * P.max_block_nnz + 15) & ~size_t(15)) +
-                       ((sizeof(T) * P.max_block_nnz + 15) & ~size_t(15)) + sizeof(int) * (CB + 4) +
-                       sizeof(double) * CB + 16 * ((sizeof(T) * CB + 15) / 16) +
-                       sizeof(typename TgtT<T>::type) * CB;
+                       ((sizeof(T) * P.max_block_nnz + 15) & ~size_t(15)) + sizeof(int) * (CB + 4);
   const size_t smem = stage + (P.ring_in_smem ? sizeof(T) * (size_t)W * TS : 0) + 64;
-  auto kern = pa.qmc_type == DBGZ_QMC_SOBOL ? k_genz_sparse<T, Step, DBGZ_QMC_SOBOL>
-                                             : k_genz_sparse<T, Step, DBGZ_QMC_RICHTMYER>;
+  auto kern = k_genz_sparse<T, Policy>;
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   DBGZ_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TS, smem));
   per_sm = std::max(per_sm, 1);
-  const int64_t grid = std::min<int64_t>(n_tiles, (int64_t)per_sm * ctx->num_sms);
+  const int64_t grid = std::min<int64_t>(n_tiles - pa.tile0, (int64_t)per_sm * ctx->num_sms);
+  if (grid < 1) return DBGZ_OK;
   if (!P.ring_in_smem) {
     DBGZ_TRY(dbgz_ensure(ctx, p->yws, sizeof(T) * (size_t)grid * W * TS));
     P.yglob = (T *)p->yws.p;
@@ -254,8 +263,30 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   return DBGZ_OK;
 }
 
+template <typename T, int GEN>
+static int launch_sparse_kind(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
+  switch (pa.kind) {
+    case kLoopForwardStore: return launch_sparse<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
+    case kLoopAdjoint: return launch_sparse<T, pol::Adjoint<T, GEN>>(p, pa, partials, n_tiles);
+    default: return launch_sparse<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
+  }
+}
+
+template <typename T>
+static int launch_sparse_gen(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
+  if (pa.qmc_type == DBGZ_QMC_SOBOL) return launch_sparse_kind<T, DBGZ_QMC_SOBOL>(p, pa, partials, n_tiles);
+  return launch_sparse_kind<T, DBGZ_QMC_RICHTMYER>(p, pa, partials, n_tiles);
+}
+
 int dbgz_loop_sparse(dbgz_problem *p, const PassArgs &pa, int precision, double *partials, int64_t n_tiles) {
   if (!p->csc_colptr.p) DBGZ_TRY(dbgz_build_csc(p));
-  if (precision == DBGZ_PREC_FP64) return launch_sparse<double, dbgz::StepFp64>(p, pa, partials, n_tiles);
-  return launch_sparse<float, dbgz::StepFp32>(p, pa, partials, n_tiles);
+  if (pa.kind == kLoopAdjoint && !p->cscb_colptr.p) {
+    if (!p->Ub.p) DBGZ_TRY(dbgz_make_Ub(p));
+    int64_t nnz = 0, bw = 1;
+    DBGZ_TRY(build_csc_from(p, (const double *)p->Ub.p, p->cscb_colptr, p->cscb_row, p->cscb_val64, p->cscb_val32,
+                            &nnz, &bw));
+    p->bandwidth_b = bw;
+  }
+  if (precision == DBGZ_PREC_FP64) return launch_sparse_gen<double>(p, pa, partials, n_tiles);
+  return launch_sparse_gen<float>(p, pa, partials, n_tiles);
 }

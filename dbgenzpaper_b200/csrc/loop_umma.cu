@@ -60,7 +60,7 @@ struct Fmt<DBGZ_PREC_FP32_TF32> {
 struct __align__(64) UmmaParams {
   CUtensorMap tm_u[2];  // U^T panel parts: rows = targets, K = y-index
   CUtensorMap tm_y[2];  // Y workspace parts: rows = slot*128 + sample, K = y-index
-  int64_t d, nY, m, n_reps, tiles_per_shift, n_tiles;
+  int64_t d, nY, m, n_reps, tiles_per_shift, n_tiles, tile0;  // tiles [tile0, n_tiles) of the pass
   int P;
   dbgz::GenParams gen;
   const float *U32;  // d x d column-major (in-block triangle)
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0}, ws_cnt = 0;
       uint32_t ja = 0, jb = 0;
       bool ok = true;
-      for (int64_t tile = blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
+      for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
         for (int64_t ph = 0; ph < nphase && ok; ++ph) {
           const Phase f = phase_of(P, ph);
           if (ph > 0) {
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           }
         }
       };
-      for (int64_t tile = blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
+      for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
         for (int64_t ph = 0; ph < nphase && ok; ++ph) {
           const Phase f = phase_of(P, ph);
           const int64_t nkc = ph > 0 ? f.L / BK : 0;
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
     uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
     const bool need_ws = nphase > 1;
-    for (int64_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
+    for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
       const int64_t k_shift = tile / P.tiles_per_shift;
       const int64_t jt = tile - k_shift * P.tiles_per_shift;
       const int64_t j = jt * TS + r;
@@ -617,7 +617,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
     fprintf(stderr, "dbgz: tensor-core loop %d CTA/SM (smem %d of %d B, regs %d x %d of %d)\n", per_sm, smem,
             smem_per_sm, fa.numRegs, NT, regs_per_sm);
   if (per_sm < 1) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor-core loop does not fit on an SM");
-  const int64_t grid = std::min<int64_t>(n_tiles, (int64_t)per_sm * ctx->num_sms);
+  const int64_t grid = std::min<int64_t>(n_tiles - pa.tile0, (int64_t)per_sm * ctx->num_sms);
   const int64_t nphase = (nY + Pw - 1) / Pw;
   UmmaParams P{};
   P.d = d;
@@ -626,6 +626,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.n_reps = pa.n_reps;
   P.tiles_per_shift = (pa.m + TS - 1) / TS;
   P.n_tiles = n_tiles;
+  P.tile0 = pa.tile0;
   P.P = Pw;
   P.gen.qmc_type = pa.qmc_type;
   P.gen.n_bits = pa.n_bits;
@@ -647,6 +648,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.io.gb = pa.grad.gb;
   P.io.gu = pa.grad.gu;
   P.io.dc1 = pa.grad.dc1;
+  P.io.tile0 = pa.tile0;
   P.tgt = (const TargetParams32 *)p->tgt32.p;
   P.c1 = pa.c1;
   P.dc1 = pa.dc1;

@@ -69,8 +69,9 @@ struct GradIO {
   T *dc = nullptr;    // dc_t, t = 1..d-1 (row t)
   double *p = nullptr;
   T *sbar = nullptr;  // p * sbar_t, t = 1..d-1 (row t)
-  double *ga = nullptr, *gb = nullptr, *gu = nullptr;  // [(tile * 4 + warp) * d + t]
+  double *ga = nullptr, *gb = nullptr, *gu = nullptr;  // [((tile - tile0) * 4 + warp) * d + t]
   double dc1 = 0.0;   // dc of variable 0
+  int64_t tile0 = 0;  // first tile of the sample chunk these arrays hold (sample g = (tile - tile0) * 128 + r)
 };
 
 template <typename T>
@@ -114,7 +115,7 @@ struct Forward {
     d = d_;
     k = tile / tiles_per_shift;
     j = (tile - k * tiles_per_shift) * 128 + r;
-    g = tile * 128 + r;
+    g = (tile - io_.tile0) * 128 + r;
     cdf_form = cdf_form_;
     io = io_;
     st.init(c1, dc1, up1);
@@ -171,7 +172,7 @@ struct Adjoint {
     tile = tile_;
     k = tile / tiles_per_shift;
     j = (tile - k * tiles_per_shift) * 128 + r;
-    g = tile * 128 + r;
+    g = (tile - io_.tile0) * 128 + r;
     io = io_;
     ybar = 0.0;  // variable d-1 has no u: nothing downstream of it
     p = io.p[g];
@@ -249,7 +250,7 @@ struct Adjoint {
       v2 += __shfl_down_sync(0xffffffffu, v2, o);
     }
     if (lane == 0) {
-      const int64_t row = (tile * 4 + warp) * d + t;
+      const int64_t row = ((tile - io.tile0) * 4 + warp) * d + t;
       io.ga[row] = v0;
       io.gb[row] = v1;
       io.gu[row] = v2;
@@ -263,7 +264,7 @@ struct Adjoint {
     double ga, gb, gu;
     const double sb = variable(sg.tg[li], w, has_u, y, s, dc, true, ga, gb, gu);
     accumulate(t, ga, gb, gu);
-    io.sbar[t * io.N + g] = (T)(p * sb);
+    if (io.sbar) io.sbar[t * io.N + g] = (T)(p * sb);
     return (T)sb;
   }
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {

@@ -113,6 +113,11 @@ int dbgz_destroy(dbgz_ctx *ctx);
  * for its stream); *freed_bytes (may be NULL) receives their total size.
  * No reference counterpart (the reference runs on host memory). */
 int dbgz_release_cached(dbgz_ctx *ctx, uint64_t *freed_bytes);
+/* Upper bound on the device bytes of stored forward state (y, s, dc, p s-bar
+ * of every sample-variable) that one gradient call may hold; larger sample
+ * counts run the forward and adjoint passes in chunks of whole 128-sample
+ * tiles (default 48 GiB).  No reference counterpart. */
+int dbgz_set_state_budget(dbgz_ctx *ctx, uint64_t bytes);
 const char *dbgz_last_error(const dbgz_ctx *ctx);
 
 /* Device-side timing of the library's own work, measured with CUDA events

@@ -202,3 +202,98 @@ def test_fp32_sigma_gradient_close_to_fp64(dbgz):
     G64 = D.qmc_pnorm_grad_sigma(Q, precision=L.PREC_FP64)[5]
     G = D.qmc_pnorm_grad_sigma(Q, precision=L.PREC_FP32_SPLIT_BF16)[5]
     assert np.linalg.norm(G - G64) <= 3e-3 * np.linalg.norm(G64)
+
+
+@pytest.mark.parametrize("prec,rtol", [(L.PREC_FP64, 1e-11), (L.PREC_FP32_SPLIT_BF16, 1e-4)])
+def test_chunked_gradient_matches_one_chunk(dbgz, prec, rtol):
+    # a small state budget splits the samples into chunks of tiles: the same
+    # estimate, and the same gradient up to the summation grouping
+    D = dbgz
+    ctx = D.Context(0)
+    try:
+        rng = np.random.default_rng(90)
+        n = 120
+        S = W.rand_spd(n, 1.0, rng)
+        lo, up = W.bounds_quarter(S)
+        opts = D.QMC_opts(m=3000, n_reps=5, max_pts=3000, max_abs_err=0.0)
+        Q = D.QMCData(S, lo, up, opts, shifts=rng.random((n - 1, 5)), context=ctx)
+        r1 = D.qmc_pnorm_grad(Q, precision=prec)
+        ctx.set_state_budget(3 << 20)  # a few tiles per chunk
+        r2 = D.qmc_pnorm_grad(Q, precision=prec)
+        P1 = D.qmc_pnorm(Q, precision=prec)[0]
+        Q.close()
+        assert r1[0] == r2[0] and r1[1] == r2[1] and abs(r1[0] - P1) <= 1e-12 * P1
+        for x, y in zip(r1[3:], r2[3:]):
+            assert np.linalg.norm(y) > 0
+            assert np.linalg.norm(x - y) <= rtol * np.linalg.norm(y)
+    finally:
+        ctx.close()
+
+
+def _banded(n, seed):
+    rng = np.random.default_rng(seed)
+    idx = np.arange(n)
+    dist = np.abs(idx[:, None] - idx[None, :])
+    S = 0.8 ** dist + 0.3 * (dist == 1) + 0.5 * np.eye(n)
+    up = rng.uniform(-0.5, 2.5, n)
+    lo = np.minimum(-rng.uniform(0.5, 2.5, n), up - 0.3)
+    return S, lo, up, rng.random((n - 1, 4))
+
+
+def _banded_problem(D, S, lo, up, sh, band, m=512, context=None):
+    Q = D.QMCDataSparse(S, lo, up, D.QMC_opts(m=m, n_reps=4, max_pts=m, max_abs_err=0.0),
+                        qmc_type="Richtmyer", shifts=sh, context=context)
+    Q.truncate_band(band)
+    return Q
+
+
+def _Pband(D, S, lo, up, sh, band):
+    Q = _banded_problem(D, S, lo, up, sh, band)
+    P = D.qmc_pnorm(Q, precision=L.PREC_FP64)[0]
+    Q.close()
+    return P
+
+
+def test_banded_gradient_matches_finite_differences(dbgz):
+    # the banded path (classic factor, no pivoting) against central
+    # differences of the banded estimate in the original bounds
+    D = dbgz
+    n, band = 90, 6
+    S, lo, up, sh = _banded(n, 91)
+    Q = _banded_problem(D, S, lo, up, sh, band)
+    P, _, _, da, db, dU = D.qmc_pnorm_grad(Q, precision=L.PREC_FP64)
+    assert dU is None
+    assert abs(P - D.qmc_pnorm(Q, precision=L.PREC_FP64)[0]) <= 1e-14 * P
+    Q.close()
+    h = 1e-6
+    rng = np.random.default_rng(3)
+    for i in rng.choice(n, 6, replace=False):
+        e = np.zeros(n)
+        e[i] = h
+        fdb = (_Pband(D, S, lo, up + e, sh, band) - _Pband(D, S, lo, up - e, sh, band)) / (2 * h)
+        fda = (_Pband(D, S, lo + e, up, sh, band) - _Pband(D, S, lo - e, up, sh, band)) / (2 * h)
+        assert abs(db[i] - fdb) <= 2e-6 * max(abs(fdb), abs(P)) + 1e-12, (i, db[i], fdb)
+        assert abs(da[i] - fda) <= 2e-6 * max(abs(fda), abs(P)) + 1e-12, (i, da[i], fda)
+
+
+def test_banded_gradient_chunked_and_fp32(dbgz):
+    D = dbgz
+    ctx = D.Context(0)
+    try:
+        n, band = 700, 40  # the anti-transposed CSC in a 64-slot shared-memory ring
+        S, lo, up, sh = _banded(n, 92)
+        Q = _banded_problem(D, S, lo, up, sh, band, m=1024, context=ctx)
+        r64 = D.qmc_pnorm_grad(Q, precision=L.PREC_FP64)
+        r32 = D.qmc_pnorm_grad(Q, precision=L.PREC_FP32_SIMT)
+        ctx.set_state_budget(8 << 20)
+        r64c = D.qmc_pnorm_grad(Q, precision=L.PREC_FP64)
+        P64 = D.qmc_pnorm(Q, precision=L.PREC_FP64)[0]
+        Q.close()
+        assert r64[0] == r64c[0] and abs(r64[0] - P64) <= 1e-14 * P64
+        for x, y in zip(r64c[3:5], r64[3:5]):
+            assert np.linalg.norm(x - y) <= 1e-11 * np.linalg.norm(y)
+        assert abs(r32[0] - r64[0]) <= 1e-5 * r64[0] + 1e-7
+        for x, y in zip(r32[3:5], r64[3:5]):
+            assert np.linalg.norm(x - y) <= 2e-3 * np.linalg.norm(y)
+    finally:
+        ctx.close()
