@@ -103,8 +103,10 @@ struct Smem {
 
 constexpr int kUld = BK + 4;  // row stride of ublk: 16-byte aligned rows for LDS.128
 struct Misc {
-  float ublk[BK][kUld];  // coefficients of the block's triangle: ublk[li][ti] = U[lbase+li, lbase+ti+1]
-  pol::Staged<float> sg;
+  // coefficients of the block's triangle, ublk[buf][li][ti] = U[lbase+li, lbase+ti+1], and the
+  // block's per-dimension constants; two buffers: the next block stages while this one runs
+  float ublk[2][BK][kUld];
+  pol::Staged<float> sg[2];
   double red[4];
   uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
   uint32_t tmem_base;
@@ -354,12 +356,23 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
     uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
     const bool need_ws = nphase > 1;
+    uint32_t blk = 0;  // blocks run by this CTA (selects the staging buffer)
     for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
       const int64_t k_shift = tile / P.tiles_per_shift;
       const int64_t jt = tile - k_shift * P.tiles_per_shift;
       const int64_t j = jt * TS + r;
       Policy pl;
       pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
+      // asynchronous staging of one block into buffer `buf` (one commit group)
+      auto stage_block = [&](int buf, int64_t lb, int nv) {
+        for (int e = r; e < BK * BK; e += TS) {
+          const int li = e % BK, ti = e / BK;
+          const bool v = li <= ti && ti < nv;
+          pol::cp_async_or_zero<4>(&ms->ublk[buf][li][ti], v ? P.U32 + (lb + ti + 1) * P.d + lb + li : P.U32, v);
+        }
+        pl.stage_async(ms->sg[buf], P.tgt, r, lb, nv);
+        pol::cp_async_commit();
+      };
       for (int64_t ph = 0; ph < nphase; ++ph) {
         const Phase f = phase_of(P, ph);
         if (ph > 0) {
@@ -372,14 +385,18 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           const int ia = ja & 1;
           const int64_t lbase = f.L + BK * b;
           const int nval = (int)((P.nY - lbase) < BK ? (P.nY - lbase) : BK);
-          // stage the block's U triangle and per-dimension parameters
+          const int cur = (int)(blk & 1);
+          // the block's U triangle and per-dimension constants: staged during
+          // the previous block of the tile, or now for the tile's first block
+          if (ph == 0 && b == 0) stage_block(cur, lbase, nval);
+          pol::cp_async_wait_all();
           named_sync(kBarScalar, TS);
-          for (int e = r; e < BK * BK; e += TS) {
-            const int li = e % BK, ti = e / BK;
-            ms->ublk[li][ti] =
-                (li <= ti && ti < nval) ? P.U32[(lbase + ti + 1) * P.d + lbase + li] : 0.f;
+          if (lbase + BK < P.nY) {
+            const int64_t nb2 = P.nY - lbase - BK;
+            stage_block(cur ^ 1, lbase + BK, (int)(nb2 < BK ? nb2 : BK));
           }
-          pl.stage(ms->sg, P.tgt, r, lbase, nval);
+          float(*ublk)[kUld] = ms->ublk[cur];
+          const pol::Staged<float> &sgc = ms->sg[cur];
           // partial sums of the block's targets, accumulated by the tensor cores
           float s[BK];
           bool ok = true;
@@ -422,20 +439,20 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 float y = 0.f;
                 if (li < nval) {
                   const int64_t l = lbase + li;
-                  y = pl.emit_k(ms->sg, li, l, k);
-                  const float4 *urow = reinterpret_cast<const float4 *>(&ms->ublk[li][8 * ch]);
+                  y = pl.emit_k(sgc, li, l, k);
+                  const float4 *urow = reinterpret_cast<const float4 *>(&ublk[li][8 * ch]);
                   const float4 u0 = urow[0], u1 = urow[1];
                   const float uu[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
                   for (int t = k; t < 8; ++t) s[t] = fmaf(y, uu[t], s[t]);
-                  pl.consume(ms->sg, s[k], li, l);
+                  pl.consume(sgc, s[k], li, l);
                 }
                 ys[k] = y;
               }
               switch (ch) {
-                case 0: rank8_update<24>(s, ys, &ms->ublk[0][8]); break;
-                case 1: rank8_update<16>(s, ys, &ms->ublk[8][16]); break;
-                case 2: rank8_update<8>(s, ys, &ms->ublk[16][24]); break;
+                case 0: rank8_update<24>(s, ys, &ublk[0][8]); break;
+                case 1: rank8_update<16>(s, ys, &ublk[8][16]); break;
+                case 2: rank8_update<8>(s, ys, &ublk[16][24]); break;
                 default: break;
               }
               if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
@@ -482,6 +499,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           }
           ++a_use[ia];
           ++ja;
+          ++blk;
         }
       }
       // per-tile end and sum of p in a fixed order
@@ -495,6 +513,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       }
     }
   done:
+    pol::cp_async_wait_all();
     if (r == 0) bulk_wait_all();
     (void)ws_cnt;
   }

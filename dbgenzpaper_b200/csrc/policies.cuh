@@ -74,6 +74,17 @@ struct GradIO {
   int64_t tile0 = 0;  // first tile of the sample chunk these arrays hold (sample g = (tile - tile0) * 128 + r)
 };
 
+// Asynchronous global -> shared copy of `BYTES` (4, 8 or 16) bytes, or zeros
+// when !valid (no bytes are read then; `src` must still be a mapped address).
+template <int BYTES>
+__device__ __forceinline__ void cp_async_or_zero(void *dst_smem, const void *src, bool valid) {
+  const uint32_t dst = (uint32_t)__cvta_generic_to_shared(dst_smem);
+  const int n = valid ? BYTES : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(BYTES), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename T>
 __device__ __forceinline__ T shift_at(const dbgz::GenParams &g, int64_t idx);
 template <>
@@ -127,6 +138,19 @@ struct Forward {
       sg.tg[r] = tgt[lbase + r + 1];
       sg.qv[r] = gen.q ? gen.q[lbase + r] : 0.0;
       sg.shv[r] = shift_at<T>(gen, k * (d - 1) + lbase + r);
+    }
+  }
+  // stage() by asynchronous copies (FP32 staging only): the caller commits
+  // and waits
+  __device__ __forceinline__ void stage_async(Staged<T> &sg, const typename TgtT<T>::type *tgt, int r,
+                                              int64_t lbase, int nval) const {
+    static_assert(sizeof(typename TgtT<T>::type) == 16 && sizeof(T) == 4, "FP32 staging");
+    if (r < nval) {
+      const int64_t si = k * (d - 1) + lbase + r;
+      cp_async_or_zero<16>(&sg.tg[r], &tgt[lbase + r + 1], true);
+      cp_async_or_zero<8>(&sg.qv[r], gen.q ? (const void *)(gen.q + lbase + r) : (const void *)tgt, gen.q != nullptr);
+      cp_async_or_zero<4>(&sg.shv[r], gen.shift32 ? (const void *)(gen.shift32 + si) : (const void *)tgt,
+                          gen.shift32 != nullptr);
     }
   }
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
@@ -188,6 +212,20 @@ struct Adjoint {
       sg.tg[r] = tgt[t];
       sg.qv[r] = (t <= d - 2 && gen.q) ? gen.q[t] : 0.0;
       sg.shv[r] = t <= d - 2 ? shift_at<T>(gen, k * (d - 1) + t) : T(0);
+    }
+  }
+
+  __device__ __forceinline__ void stage_async(Staged<T> &sg, const typename TgtT<T>::type *tgt, int r,
+                                              int64_t lbase, int nval) const {
+    static_assert(sizeof(typename TgtT<T>::type) == 16 && sizeof(T) == 4, "FP32 staging");
+    if (r < nval) {
+      const int64_t t = d - 1 - (lbase + r);
+      const bool has_u = t <= d - 2;
+      const int64_t si = k * (d - 1) + t;
+      cp_async_or_zero<16>(&sg.tg[r], &tgt[t], true);
+      const bool vq = has_u && gen.q, vs = has_u && gen.shift32;
+      cp_async_or_zero<8>(&sg.qv[r], vq ? (const void *)(gen.q + t) : (const void *)tgt, vq);
+      cp_async_or_zero<4>(&sg.shv[r], vs ? (const void *)(gen.shift32 + si) : (const void *)tgt, vs);
     }
   }
 
