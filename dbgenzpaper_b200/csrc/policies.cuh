@@ -185,6 +185,11 @@ struct Adjoint {
   GradIO<T> io;
   double ybar;  // saved receiver value: ybar of the variable the next step handles
   double p;     // this sample's weight (the seed scale)
+  // FP32 paths: the warp's largest weight, and this sample's weight relative
+  // to it (in [0, 1]); the per-variable sums over the warp's samples are then
+  // taken in FP32 and scaled back by wmax in FP64
+  double wmax;
+  float wrel;
   int warp, lane;
 
   __device__ __forceinline__ void tile_begin(const dbgz::GenParams &gp, int64_t d_, int64_t tile_,
@@ -202,6 +207,12 @@ struct Adjoint {
     p = io.p[g];
     warp = r >> 5;
     lane = r & 31;
+    if (sizeof(T) == 4) {
+      double m = p;
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      wmax = m;
+      wrel = m > 0.0 ? (float)(p / m) : 0.f;
+    }
   }
   // step li of the block handles variable t = d-1-(lbase+li); its point is
   // QMC dimension t (y-index t), which exists for t <= d-2
@@ -267,10 +278,18 @@ struct Adjoint {
     const bool pa = !clamp9 || fabs(xa) < T(9), pb = !clamp9 || fabs(xb) < T(9);
     const T fa = pa ? rpi * exp(-xa * xa) : T(0);
     const T fb = pb ? rpi * exp(-xb * xb) : T(0);
-    // d log(dc) / d dc; a dc of zero (weight zero) contributes nothing
-    const double pex = dc > T(0) ? 1.0 / (double)dc : 0.0;
-    double ubar = 0.0;
-    if (has_u && fabs(y) < T(8.12585)) ubar = ybar / (double)(rpi * exp(T(-0.5) * y * y));
+    // d log(dc) / d dc; a dc of zero (weight zero) contributes nothing.  In
+    // the FP32 paths the reciprocals are FP32 (2 ulp) while their results
+    // stay in FP32 range, and FP64 divisions otherwise.
+    double pex = 0.0, ubar = 0.0;
+    if (sizeof(T) == 4) {
+      if (dc > T(1e-30)) pex = (double)__fdividef(1.0f, (float)dc);
+      else if (dc > T(0)) pex = 1.0 / (double)dc;
+      if (has_u && fabs(y) < T(8.12585)) ubar = ybar * (double)__fdividef(1.0f, (float)(rpi * exp(T(-0.5) * y * y)));
+    } else {
+      pex = dc > T(0) ? 1.0 / (double)dc : 0.0;
+      if (has_u && fabs(y) < T(8.12585)) ubar = ybar / (double)(rpi * exp(T(-0.5) * y * y));
+    }
     const double eb = pex + ubar * w, cb = -pex + ubar * (1.0 - w);
     const double rU = (double)inv_u * 1.4142135623730951;  // 1 / U_tt
     ga = (fa != T(0)) ? cb * (double)fa * rU : 0.0;
@@ -281,6 +300,25 @@ struct Adjoint {
   }
 
   __device__ __forceinline__ void accumulate(int64_t t, double ga, double gb, double gu) const {
+    if (sizeof(T) == 4) {
+      float f0 = (float)(wrel * ga), f1 = (float)(wrel * gb), f2 = (float)(wrel * gu);
+      const bool finite = isfinite(f0) && isfinite(f1) && isfinite(f2);
+      if (__all_sync(0xffffffffu, finite)) {
+        for (int o = 16; o > 0; o >>= 1) {
+          f0 += __shfl_down_sync(0xffffffffu, f0, o);
+          f1 += __shfl_down_sync(0xffffffffu, f1, o);
+          f2 += __shfl_down_sync(0xffffffffu, f2, o);
+        }
+        if (lane == 0) {
+          const int64_t row = ((tile - io.tile0) * 4 + warp) * d + t;
+          io.ga[row] = (double)f0 * wmax;
+          io.gb[row] = (double)f1 * wmax;
+          io.gu[row] = (double)f2 * wmax;
+        }
+        return;
+      }
+      // a term beyond FP32 range somewhere in the warp: FP64 sums
+    }
     double v0 = p * ga, v1 = p * gb, v2 = p * gu;
     for (int o = 16; o > 0; o >>= 1) {
       v0 += __shfl_down_sync(0xffffffffu, v0, o);
