@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(256) k_prepare_batch(const BatchProb *probs, d
   int64_t *perm = perm_all + P.off1, *rank = rank_all + blockIdx.x;
   double *dvec = work_all + 3 * P.off1, *svec = dvec + n, *ovec = svec + n;
   const int tid = threadIdx.x, nt = blockDim.x;
+  extern __shared__ double genz_sh[];  // the panel's vectors, cholk::genz_block_smem_bytes(n)
   __shared__ double red[32];
   __shared__ double eps0;
   __shared__ int any_nan;
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(256) k_prepare_batch(const BatchProb *probs, d
   // one bs2 panel [0, n-1]: Genz blocks of bs1 and the panel's Schur updates
   for (int64_t i0 = 0; i0 < n; i0 += bs1) {
     const int64_t i1 = i0 + bs1 - 1 < n - 1 ? i0 + bs1 - 1 : n - 1;
-    cholk::genz_block_dev(M, n, a, b, dvec, svec, ovec, perm, i0, i1, n - 1, &eps0, rank);
+    cholk::genz_block_smem(M, n, a, b, dvec, svec, perm, i0, i1, n - 1, &eps0, rank, genz_sh);
     __syncthreads();
     if (i1 < n - 1) {
       const int64_t c0 = i1 + 1, ntl = (n - 1 - c0 + cholk::kTile) / cholk::kTile;
@@ -334,8 +335,12 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
       break;
     }
     if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
-    k_prepare_batch<T><<<(unsigned)np, 256, 0, st>>>(dprobs, dM, da, db, dperm, dscale, dwork, drank, dU32, dt64,
-                                                    dt32, dparams, o.chol_block_size);
+    {
+      const int smb = (int)cholk::genz_block_smem_bytes(dmax);
+      cudaFuncSetAttribute(k_prepare_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smb);
+      k_prepare_batch<T><<<(unsigned)np, 256, smb, st>>>(dprobs, dM, da, db, dperm, dscale, dwork, drank, dU32,
+                                                         dt64, dt32, dparams, o.chol_block_size);
+    }
     dbgz_count_launch(ctx);
     if (ctx->profiling) cudaEventRecord(ctx->ev[3], st);
     if (qmc_type == DBGZ_QMC_SOBOL)

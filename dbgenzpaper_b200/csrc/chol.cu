@@ -80,6 +80,15 @@ k_genz_block(double *M, int64_t n, double *a, double *b, double *dvec, double *s
              int64_t i0, int64_t i1, int64_t ii1, const double *eps0_ptr, int64_t *rank) {
   cholk::genz_block_dev(M, n, a, b, dvec, svec, ovec, perm, i0, i1, ii1, eps0_ptr, rank);
 }
+// The same with the panel's vectors in shared memory (panels of up to
+// kGenzSmemPanel candidates).
+constexpr int64_t kGenzSmemPanel = 1024;
+__global__ void __launch_bounds__(kStepThreads)
+k_genz_block_smem(double *M, int64_t n, double *a, double *b, double *dvec, double *svec, int64_t *perm, int64_t i0,
+                  int64_t i1, int64_t ii1, const double *eps0_ptr, int64_t *rank) {
+  extern __shared__ double genz_sh[];
+  cholk::genz_block_smem(M, n, a, b, dvec, svec, perm, i0, i1, ii1, eps0_ptr, rank, genz_sh);
+}
 
 // C[j,k] -= sum_{l=p0..p1} A(l,j) B(l,k) over [c0, c1]^2, one tile per CTA.
 constexpr int kTile = cholk::kTile;
@@ -315,8 +324,19 @@ int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b
         int64_t ii1 = std::min(iii1, ii0 + bs2 - 1);
         for (int64_t i0 = ii0; i0 <= ii1 && rc == DBGZ_OK; i0 += bs1) {
           int64_t i1 = std::min(ii1, i0 + bs1 - 1);
-          k_genz_block<<<1, kStepThreads, 0, st>>>(M, n, a, b, dvec, svec, ovec, perm, i0, i1,
-                                                    ii1, eps0, rank);
+          const int64_t panel = ii1 - i0 + 1;
+          if (panel <= kGenzSmemPanel) {
+            const size_t sm = cholk::genz_block_smem_bytes(panel);
+            static bool attr[64] = {};
+            if (ctx->device < 0 || ctx->device >= 64 || !attr[ctx->device]) {
+              cudaFuncSetAttribute(k_genz_block_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)cholk::genz_block_smem_bytes(kGenzSmemPanel));
+              if (ctx->device >= 0 && ctx->device < 64) attr[ctx->device] = true;
+            }
+            k_genz_block_smem<<<1, kStepThreads, sm, st>>>(M, n, a, b, dvec, svec, perm, i0, i1, ii1, eps0, rank);
+          } else {
+            k_genz_block<<<1, kStepThreads, 0, st>>>(M, n, a, b, dvec, svec, ovec, perm, i0, i1, ii1, eps0, rank);
+          }
           dbgz_count_launch(ctx);
           if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1);
         }

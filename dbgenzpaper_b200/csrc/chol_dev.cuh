@@ -155,6 +155,171 @@ __device__ __forceinline__ void genz_block_dev(double *M, int64_t n, double *a, 
   }
 }
 
+// genz_block_dev with the panel's per-candidate vectors held in shared
+// memory for the whole block: dvec, svec, a, b, perm and the diagonal of M
+// over [i0, ii1] (sh: 7 (ii1 - i0 + 1) words, see genz_block_smem_bytes).
+// The pivot step's serial part (argmin, swaps, the pivot's own terms) then
+// makes no global round trips; M's rows and columns stay in global memory.
+// Same operations in the same order as genz_block_dev: the same bits.
+__host__ __device__ inline size_t genz_block_smem_bytes(int64_t panel_len) { return (size_t)56 * panel_len; }
+
+__device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a, double *b, double *dvec,
+                                                double *svec, int64_t *perm, int64_t i0, int64_t i1, int64_t ii1,
+                                                const double *eps0_ptr, int64_t *rank, double *sh) {
+  __shared__ double red_v[32];
+  __shared__ int64_t red_i[32];
+  __shared__ int64_t sh_im;
+  __shared__ double sh_mii, sh_yi;
+  __shared__ int sh_stop;
+  const double c2 = dm_div(1.0, dm_sqrt(2.0));
+  const double is2pi = dm_div(2.0, dm_sqrt(dm_mul(2.0, M_PI)));
+  const double eps0 = eps0_ptr[0];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (rank[0] < n) return;  // an earlier block already stopped
+  const int64_t len = ii1 - i0 + 1;
+  double *s_d = sh, *s_s = sh + len, *s_a = sh + 2 * len, *s_b = sh + 3 * len, *s_g = sh + 4 * len,
+         *s_o = sh + 5 * len;
+  int64_t *s_p = reinterpret_cast<int64_t *>(sh + 6 * len);
+  for (int64_t k = tid; k < len; k += blockDim.x) {
+    const int64_t g = i0 + k;
+    s_d[k] = 0.0;
+    s_s[k] = svec[g];
+    s_a[k] = a[g];
+    s_b[k] = b[g];
+    s_g[k] = M[g * n + g];
+    s_p[k] = perm[g];
+  }
+  __syncthreads();
+  auto write_back = [&]() {
+    __syncthreads();
+    for (int64_t k = tid; k < len; k += blockDim.x) {
+      const int64_t g = i0 + k;
+      dvec[g] = s_d[k];
+      svec[g] = s_s[k];
+      a[g] = s_a[k];
+      b[g] = s_b[k];
+      perm[g] = s_p[k];
+    }
+  };
+  for (int64_t i = i0; i <= i1; ++i) {
+    // pivot scores :500-512, then argmin :514
+    double bv = 0.0;
+    int64_t bi = INT64_MAX;
+    for (int64_t k = i + tid; k <= ii1; k += blockDim.x) {
+      const int64_t q = k - i0;
+      double m_kk = dm_sub(s_g[q], s_d[q]);
+      m_kk = m_kk < 0 ? 0.0 : dm_sqrt(m_kk);
+      double a_k = dm_mul(dm_div(dm_sub(s_a[q], s_s[q]), m_kk), c2);
+      double b_k = dm_mul(dm_div(dm_sub(s_b[q], s_s[q]), m_kk), c2);
+      double o = dm_sub(det_erf(b_k), det_erf(a_k));
+      s_o[q] = o;
+      if (bi == INT64_MAX) { bv = o; bi = k; }
+      else argmin_combine(bv, bi, o, k);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
+      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
+      if (lane + off < 32 && i2 != INT64_MAX) {
+        if (bi == INT64_MAX) { bv = v2; bi = i2; }
+        else argmin_combine(bv, bi, v2, i2);
+      }
+    }
+    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double v = red_v[0];
+      int64_t im = red_i[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        if (red_i[w] == INT64_MAX) continue;
+        if (im == INT64_MAX) { v = red_v[w]; im = red_i[w]; }
+        else argmin_combine(v, im, red_v[w], red_i[w]);
+      }
+      const int64_t qi = i - i0, qm = im - i0;
+      double d_ii = s_o[qm];
+      double m_ii = dm_sub(s_g[qm], s_d[qm]);
+      if (im != i) {  // :518-523 (and the diagonal, which the row/column swap moves)
+        int64_t tp = s_p[qi]; s_p[qi] = s_p[qm]; s_p[qm] = tp;
+        double t;
+        t = s_d[qm]; s_d[qm] = s_d[qi]; s_d[qi] = t;
+        t = s_s[qm]; s_s[qm] = s_s[qi]; s_s[qi] = t;
+        t = s_a[qm]; s_a[qm] = s_a[qi]; s_a[qi] = t;
+        t = s_b[qm]; s_b[qm] = s_b[qi]; s_b[qi] = t;
+        t = s_g[qm]; s_g[qm] = s_g[qi]; s_g[qi] = t;
+      }
+      sh_im = im;
+      sh_mii = m_ii;
+      sh_yi = d_ii;  // carried to the y_i step
+    }
+    __syncthreads();
+    const int64_t im = sh_im;
+    if (im != i) {  // :525-530: rows over columns i0..n, then full columns
+      for (int64_t k = i0 + tid; k < n; k += blockDim.x) {
+        double t = M[k * n + i];
+        M[k * n + i] = M[k * n + im];
+        M[k * n + im] = t;
+      }
+      __syncthreads();
+      for (int64_t k = tid; k < n; k += blockDim.x) {
+        double t = M[i * n + k];
+        M[i * n + k] = M[im * n + k];
+        M[im * n + k] = t;
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      double m_ii = sh_mii;
+      double d_ii = sh_yi;
+      int stop = 0;
+      if (m_ii > eps0) {
+        m_ii = dm_sqrt(m_ii);
+      } else {
+        rank[0] = i;  // 0-based i == reference's i - 1
+        stop = 1;
+      }
+      if (!stop) {
+        const int64_t qi = i - i0;
+        M[i * n + i] = m_ii;
+        double a_norm = dm_div(dm_sub(s_a[qi], s_s[qi]), m_ii);
+        double b_norm = dm_div(dm_sub(s_b[qi], s_s[qi]), m_ii);
+        double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
+        double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
+        sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), d_ii);
+        sh_mii = m_ii;
+      }
+      sh_stop = stop;
+    }
+    __syncthreads();
+    if (sh_stop) {
+      write_back();
+      return;
+    }
+    const double m_ii = sh_mii, y_i = sh_yi;
+    if (i == i0) {  // :547-554
+      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
+        const int64_t q = j - i0;
+        double m_ij = dm_div(M[j * n + i], m_ii);
+        M[j * n + i] = m_ij;
+        M[i * n + j] = m_ij;
+        s_d[q] = dm_add(s_d[q], dm_mul(m_ij, m_ij));
+        s_s[q] = dm_add(s_s[q], dm_mul(y_i, m_ij));
+      }
+    } else if (i < ii1) {  // :555-570
+      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
+        const int64_t q = j - i0;
+        double acc = 0.0;
+        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[l * n + j], M[i * n + l], acc);
+        double m_ij = dm_div(dm_sub(M[i * n + j], acc), m_ii);
+        M[j * n + i] = m_ij;
+        M[i * n + j] = m_ij;
+        s_d[q] = dm_add(s_d[q], dm_mul(m_ij, m_ij));
+        s_s[q] = dm_add(s_s[q], dm_mul(y_i, m_ij));
+      }
+    }
+    __syncthreads();
+  }
+  write_back();
+}
+
 // C[j,k] -= sum_{l=p0..p1} A(l,j) * B(l,k) for j,k in [c0, c1], one
 // ascending fma chain per element.  A(l,j) = M[j,l] (row form, the
 // reference's lower-triangle copy) when a_row, else M[l,j]; B(l,k) = M[l,k].

@@ -16,9 +16,10 @@
 // Two numerics are provided:
 //  * StepFp64: the reference's Float64 arithmetic (erf form or erfc form of
 //    the CDF, the clamp to [-9, 9] in erf units, the same fma pattern).
-//  * StepFp32: FP32 special functions written to stay within ~1e-7
-//    relative of the FP64 result where the reference's Float32 loop loses
-//    digits: the state keeps both tails -- lo = Phi(alpha), up = Phi(-beta)
+//  * StepFp32: FP32 arithmetic kept close to the FP64 result where the
+//    reference's Float32 loop loses digits (tail masses from normal32.cuh,
+//    relative error < 3e-6 where they are above 1e-10; Phi^-1 from CUDA's
+//    normcdfinvf): the state keeps both tails -- lo = Phi(alpha), up = Phi(-beta)
 //    -- and dc, so that u (when u <= 1/2) and 1 - u (otherwise) are formed
 //    without cancellation and Phi^-1 is taken of the smaller one; dc is the
 //    difference of two tails of the same side only when the interval lies
@@ -26,6 +27,7 @@
 //    cancel.  The weight product p stays FP64 (no underflow at d = 1000).
 //    u is clamped to [eps64, 1 - eps64] like the Float64 reference.
 #pragma once
+#include "normal32.cuh"
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cfloat>
@@ -157,24 +159,18 @@ struct StepFp32 {
   __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
     float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
     float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
-    float ea = 0.5f * erfcf(fabsf(xa));  // mass beyond |alpha| on its side
-    float eb = 0.5f * erfcf(fabsf(xb));
-    float d;
-    if (xa >= 0.0f) {                   // both bounds in the upper tail
-      d = ea - eb;
-      if (eb > 0.5f * ea) d = same_tail_mass64(xa, xb);
-      lo = 1.0f - ea;
-      up = eb;
-    } else if (xb <= 0.0f) {            // both bounds in the lower tail
-      d = eb - ea;
-      if (ea > 0.5f * eb) d = same_tail_mass64(-xb, -xa);
-      lo = ea;
-      up = 1.0f - eb;
-    } else {                            // alpha < 0 < beta
-      d = (1.0f - ea) - eb;
-      lo = ea;
-      up = eb;
-    }
+    const float ea = tail_mass_f32(fabsf(xa));  // mass beyond |alpha| on its side
+    const float eb = tail_mass_f32(fabsf(xb));
+    // both bounds in the upper tail (hi_t), both in the lower tail (lo_t), or
+    // alpha < 0 < beta; selects rather than branches (the step is a serial
+    // chain per sample, and branch resolution stalls it)
+    const bool hi_t = xa >= 0.0f, lo_t = !hi_t && xb <= 0.0f;
+    float d = hi_t ? ea - eb : (lo_t ? eb - ea : (1.0f - ea) - eb);
+    // the FP32 difference of two close tail masses cancels: FP64 then
+    const bool need64 = (hi_t && eb > 0.5f * ea) || (lo_t && ea > 0.5f * eb);
+    if (need64) d = same_tail_mass64(hi_t ? xa : -xb, hi_t ? xb : -xa);
+    lo = hi_t ? 1.0f - ea : ea;
+    up = lo_t ? 1.0f - eb : eb;
     dc = d;
     p *= (double)d;
   }

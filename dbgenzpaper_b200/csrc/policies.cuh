@@ -299,6 +299,46 @@ struct Adjoint {
     return -(ga + gb);
   }
 
+  // FP32 form of variable() for the FP32 paths: every quantity in FP32.  A
+  // result that leaves FP32 range (dc below 1e-36, or sensitivities beyond
+  // 1e38) is not finite, and emit_from then redoes the warp in FP64.
+  __device__ __forceinline__ float variable32(const typename TgtT<T>::type &tg, float w, bool has_u, float y,
+                                              float s, float dc, bool clamp9, float &ga, float &gb,
+                                              float &gu) const {
+    const float r2 = 1.41421356237f, rpi = 0.398942280401f;
+    const float inv_u = (float)tg.inv_u;
+    const float xa = ((float)tg.a - s) * inv_u, xb = ((float)tg.b - s) * inv_u;
+    const bool pa = !clamp9 || fabsf(xa) < 9.0f, pb = !clamp9 || fabsf(xb) < 9.0f;
+    const float fa = pa ? rpi * expf(-xa * xa) : 0.0f;
+    const float fb = pb ? rpi * expf(-xb * xb) : 0.0f;
+    const float pex = dc > 1e-36f ? __fdividef(1.0f, dc) : (dc > 0.0f ? INFINITY : 0.0f);
+    float ubar = 0.0f;
+    if (has_u && fabsf(y) < 8.12585f) ubar = (float)ybar * __fdividef(1.0f, rpi * expf(-0.5f * y * y));
+    const float eb = fmaf(ubar, w, pex), cb = fmaf(ubar, 1.0f - w, -pex);
+    const float rU = inv_u * r2;
+    ga = fa != 0.0f ? cb * fa * rU : 0.0f;
+    gb = fb != 0.0f ? eb * fb * rU : 0.0f;
+    gu = -((ga != 0.0f ? ga * (xa * r2) : 0.0f) + (gb != 0.0f ? gb * (xb * r2) : 0.0f));
+    return -(ga + gb);
+  }
+
+  // FP32 warp sums of the weighted terms (weights relative to the warp's
+  // largest, scaled back in FP64)
+  __device__ __forceinline__ void accumulate32(int64_t t, float ga, float gb, float gu) const {
+    float f0 = wrel * ga, f1 = wrel * gb, f2 = wrel * gu;
+    for (int o = 16; o > 0; o >>= 1) {
+      f0 += __shfl_down_sync(0xffffffffu, f0, o);
+      f1 += __shfl_down_sync(0xffffffffu, f1, o);
+      f2 += __shfl_down_sync(0xffffffffu, f2, o);
+    }
+    if (lane == 0) {
+      const int64_t row = ((tile - io.tile0) * 4 + warp) * d + t;
+      io.ga[row] = (double)f0 * wmax;
+      io.gb[row] = (double)f1 * wmax;
+      io.gu[row] = (double)f2 * wmax;
+    }
+  }
+
   __device__ __forceinline__ void accumulate(int64_t t, double ga, double gb, double gu) const {
     if (sizeof(T) == 4) {
       float f0 = (float)(wrel * ga), f1 = (float)(wrel * gb), f2 = (float)(wrel * gu);
@@ -337,6 +377,16 @@ struct Adjoint {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
     const double w = has_u ? point_w(sg, li, t) : 0.0;
+    if (sizeof(T) == 4) {
+      float fa, fb, fu;
+      const float sb = variable32(sg.tg[li], (float)w, has_u, (float)y, (float)s, (float)dc, true, fa, fb, fu);
+      const bool fin = isfinite(sb) && isfinite(wrel * fa) && isfinite(wrel * fb) && isfinite(wrel * fu);
+      if (__all_sync(0xffffffffu, fin)) {
+        accumulate32(t, fa, fb, fu);
+        if (io.sbar) io.sbar[t * io.N + g] = (T)(p * (double)sb);
+        return (T)sb;
+      }
+    }
     double ga, gb, gu;
     const double sb = variable(sg.tg[li], w, has_u, y, s, dc, true, ga, gb, gu);
     accumulate(t, ga, gb, gu);
