@@ -305,20 +305,24 @@ struct Adjoint {
   __device__ __forceinline__ float variable32(const typename TgtT<T>::type &tg, float w, bool has_u, float y,
                                               float s, float dc, bool clamp9, float &ga, float &gb,
                                               float &gu) const {
+    // every quantity is formed unconditionally and chosen by selects: the
+    // per-variable code stays free of branches
     const float r2 = 1.41421356237f, rpi = 0.398942280401f;
     const float inv_u = (float)tg.inv_u;
     const float xa = ((float)tg.a - s) * inv_u, xb = ((float)tg.b - s) * inv_u;
-    const bool pa = !clamp9 || fabsf(xa) < 9.0f, pb = !clamp9 || fabsf(xb) < 9.0f;
-    const float fa = pa ? rpi * expf(-xa * xa) : 0.0f;
-    const float fb = pb ? rpi * expf(-xb * xb) : 0.0f;
-    const float pex = dc > 1e-36f ? __fdividef(1.0f, dc) : (dc > 0.0f ? INFINITY : 0.0f);
-    float ubar = 0.0f;
-    if (has_u && fabsf(y) < 8.12585f) ubar = (float)ybar * __fdividef(1.0f, rpi * expf(-0.5f * y * y));
+    const float ea = rpi * expf(-xa * xa), eb_ = rpi * expf(-xb * xb);  // 0 at an infinite bound
+    const float fa = (!clamp9 || fabsf(xa) < 9.0f) ? ea : 0.0f;
+    const float fb = (!clamp9 || fabsf(xb) < 9.0f) ? eb_ : 0.0f;
+    const float rdc = __fdividef(1.0f, dc);
+    const float pex = dc > 1e-36f ? rdc : (dc > 0.0f ? INFINITY : 0.0f);
+    const float ub = (float)ybar * __fdividef(1.0f, rpi * expf(-0.5f * y * y));
+    const float ubar = (has_u && fabsf(y) < 8.12585f) ? ub : 0.0f;
     const float eb = fmaf(ubar, w, pex), cb = fmaf(ubar, 1.0f - w, -pex);
     const float rU = inv_u * r2;
     ga = fa != 0.0f ? cb * fa * rU : 0.0f;
     gb = fb != 0.0f ? eb * fb * rU : 0.0f;
-    gu = -((ga != 0.0f ? ga * (xa * r2) : 0.0f) + (gb != 0.0f ? gb * (xb * r2) : 0.0f));
+    const float ta = ga != 0.0f ? ga * (xa * r2) : 0.0f, tb = gb != 0.0f ? gb * (xb * r2) : 0.0f;
+    gu = -(ta + tb);
     return -(ga + gb);
   }
 
