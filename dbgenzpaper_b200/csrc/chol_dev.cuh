@@ -252,15 +252,28 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
     }
     __syncthreads();
     const int64_t im = sh_im;
-    if (im != i) {  // :525-530: rows over columns i0..n, then full columns
-      for (int64_t k = i0 + tid; k < n; k += blockDim.x) {
-        double t = M[k * n + i];
-        M[k * n + i] = M[k * n + im];
-        M[k * n + im] = t;
-      }
-      __syncthreads();
+    if (im != i) {
+      // :525-530, rows i <-> im over columns i0..n-1, then columns i <-> im,
+      // in one pass: for k outside {i, im} the two swaps touch four distinct
+      // elements; the 2 x 2 block on {i, im} ends up as (i,i) <- (im,im),
+      // (im,im) <- (i,i), (i,im) <- (im,i), (im,i) <- (i,im)
       for (int64_t k = tid; k < n; k += blockDim.x) {
-        double t = M[i * n + k];
+        if (k == i || k == im) {
+          if (k == i) {
+            const double ii = M[i * n + i], mm = M[im * n + im], im_i = M[i * n + im], i_im = M[im * n + i];
+            M[i * n + i] = mm;
+            M[im * n + im] = ii;
+            M[im * n + i] = im_i;
+            M[i * n + im] = i_im;
+          }
+          continue;
+        }
+        if (k >= i0) {
+          const double t = M[k * n + i];
+          M[k * n + i] = M[k * n + im];
+          M[k * n + im] = t;
+        }
+        const double t = M[i * n + k];
         M[i * n + k] = M[im * n + k];
         M[im * n + k] = t;
       }

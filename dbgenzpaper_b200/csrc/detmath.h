@@ -23,7 +23,8 @@
  *         (all terms positive, 51 terms);  2.5 <= |x| < 6:
  *         erf = 1 - erfc, erfc(x) = e^{-x^2}/(sqrt(pi) K(x)) with the
  *         Laplace continued fraction K = x + (1/2)/(x + 1/(x + (3/2)/(...)))
- *         evaluated backwards over 40 terms;  |x| >= 6: +-1.
+ *         truncated at 40 terms, evaluated by the forward recurrence of its
+ *         convergents (one division);  |x| >= 6: +-1.
  *         Max error 5 ulp against libm.
  */
 #pragma once
@@ -145,8 +146,21 @@ DBGZ_HD double det_erf(double x) {
     for (int n = 49; n >= 0; --n) s = dm_fma(s, t, c[n]);
     r = dm_mul(dm_mul(dm_mul(TWO_OVER_SQRTPI, ax), det_exp(-x2)), s);
   } else if (ax < 6.0) {
-    double K = ax;
-    for (int n = 40; n >= 1; --n) K = dm_add(ax, dm_div(dm_mul((double)n, 0.5), K));
+    /* K = x + (1/2)/(x + (2/2)/(x + ... + (40/2)/x)), the 40-term continued
+       fraction of erfc, from the forward recurrence of its convergents
+       A_n = x A_{n-1} + (n/2) A_{n-2} (B_n alike) and one division: the
+       two chains are independent, no division inside the loop. */
+    double A2 = 1.0, A1 = ax, B2 = 0.0, B1 = 1.0;
+    for (int n = 1; n <= 40; ++n) {
+      const double an = dm_mul((double)n, 0.5);
+      const double A = dm_fma(ax, A1, dm_mul(an, A2));
+      const double B = dm_fma(ax, B1, dm_mul(an, B2));
+      A2 = A1;
+      A1 = A;
+      B2 = B1;
+      B1 = B;
+    }
+    const double K = dm_div(A1, B1);
     double erfc_v = dm_div(dm_mul(det_exp(-dm_mul(ax, ax)), INV_SQRTPI), K);
     r = dm_sub(1.0, erfc_v);
   } else {
