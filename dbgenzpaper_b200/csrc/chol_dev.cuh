@@ -226,14 +226,22 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
     }
     if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
     __syncthreads();
-    if (tid == 0) {
-      double v = red_v[0];
-      int64_t im = red_i[0];
-      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-        if (red_i[w] == INT64_MAX) continue;
-        if (im == INT64_MAX) { v = red_v[w]; im = red_i[w]; }
-        else argmin_combine(v, im, red_v[w], red_i[w]);
+    if (wid == 0) {
+      // the warps' minima reduced by warp 0 as a shuffle tree: the order
+      // (value in findmin order, then index) is a strict total order, so the
+      // minimum does not depend on the order of combination
+      const int nw = (int)(blockDim.x >> 5);
+      double v = lane < nw ? red_v[lane] : 0.0;
+      int64_t im = lane < nw ? red_i[lane] : INT64_MAX;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double v2 = __shfl_down_sync(0xffffffffu, v, off);
+        const int64_t i2 = __shfl_down_sync(0xffffffffu, im, off);
+        if (lane + off < 32 && i2 != INT64_MAX) {
+          if (im == INT64_MAX) { v = v2; im = i2; }
+          else argmin_combine(v, im, v2, i2);
+        }
       }
+      if (lane == 0) {
       const int64_t qi = i - i0, qm = im - i0;
       double d_ii = s_o[qm];
       double m_ii = dm_sub(s_g[qm], s_d[qm]);
@@ -249,6 +257,7 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
       sh_im = im;
       sh_mii = m_ii;
       sh_yi = d_ii;  // carried to the y_i step
+      }
     }
     __syncthreads();
     const int64_t im = sh_im;
@@ -319,8 +328,21 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
     } else if (i < ii1) {  // :555-570
       for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
         const int64_t q = j - i0;
+        // the ascending fma chain over l, its operands loaded 8 at a time
+        // ahead of the chain
         double acc = 0.0;
-        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[l * n + j], M[i * n + l], acc);
+        int64_t l = i0;
+        for (; l + 8 <= i; l += 8) {
+          double x[8], y[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            x[u] = M[(l + u) * n + j];
+            y[u] = M[i * n + l + u];
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc = dm_fma(x[u], y[u], acc);
+        }
+        for (; l <= i - 1; ++l) acc = dm_fma(M[l * n + j], M[i * n + l], acc);
         double m_ij = dm_div(dm_sub(M[i * n + j], acc), m_ii);
         M[j * n + i] = m_ij;
         M[i * n + j] = m_ij;
