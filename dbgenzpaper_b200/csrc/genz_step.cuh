@@ -48,7 +48,32 @@ struct GenParams {
   const uint64_t *ushift;// (d-1) x n_reps
 };
 
-// Gray-code Sobol integer of point index idx in dimension l.
+// Gray-code Sobol integer of point index idx in dimension l, computed by
+// the 32 lanes of a warp together.  Precondition: every lane of the warp
+// calls it at once for the same dimension, lane i with index idx0 + i (the
+// loops give a warp 32 consecutive points).  Then
+//   x(idx0) = XOR_k [bit k of gray(idx0)] V[k]   -- lane k supplies term k,
+//   x(idx0 + i) = x(idx0) ^ XOR_{s=1..i} V[ctz(idx0 + s)]   -- Gray-code
+// recurrence x(n) = x(n-1) ^ V[ctz(n)] as a prefix XOR over the lanes:
+// two loads and ten shuffles per point instead of a loop over its set bits
+// (same integers, exactly).
+__device__ __forceinline__ uint32_t sobol_warp(const uint32_t *Vl, uint64_t idx) {
+  const int lane = (int)(threadIdx.x & 31);
+  const uint64_t i0 = idx - (uint64_t)lane;
+  const uint32_t gw = (uint32_t)(i0 ^ (i0 >> 1));
+  uint32_t x = ((gw >> lane) & 1u) ? __ldg(Vl + lane) : 0u;
+  for (int o = 16; o > 0; o >>= 1) x ^= __shfl_xor_sync(0xffffffffu, x, o);
+  const uint32_t lo = (uint32_t)idx;
+  const int c = lo ? __ffs((int)lo) - 1 : 32;  // bits at 32 and above do not enter the 32-bit Gray code
+  uint32_t t = (lane > 0 && c < 32) ? __ldg(Vl + c) : 0u;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t u = __shfl_up_sync(0xffffffffu, t, o);
+    if (lane >= o) t ^= u;
+  }
+  return x ^ t;
+}
+
+// The same integer by one thread alone (loop over the set bits).
 __device__ __forceinline__ uint32_t sobol_int(const uint32_t *Vl, uint64_t idx) {
   uint32_t g = (uint32_t)(idx ^ (idx >> 1));
   uint32_t x = 0;
@@ -82,7 +107,7 @@ struct StepFp64 {
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
-      uint64_t xi = (uint64_t)sobol_int(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
+      uint64_t xi = (uint64_t)sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
       uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
       u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
     }
@@ -141,7 +166,7 @@ struct StepFp32 {
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
-      uint64_t xi = (uint64_t)sobol_int(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
+      uint64_t xi = (uint64_t)sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
       uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
       double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
       w = (float)fabs(fma(u, 2.0, -1.0));

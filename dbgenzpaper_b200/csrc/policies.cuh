@@ -257,7 +257,7 @@ struct Adjoint {
       const int L = gen.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
       const uint64_t xi =
-          (uint64_t)dbgz::sobol_int(gen.V + t * 32, (uint64_t)(gen.sobol_first + gen.gen_base + j)) & mask;
+          (uint64_t)dbgz::sobol_warp(gen.V + t * 32, (uint64_t)(gen.sobol_first + gen.gen_base + j)) & mask;
       const uint64_t sh = gen.ushift[k * (d - 1) + t] & mask;
       u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
     }
