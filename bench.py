@@ -171,7 +171,8 @@ def run_c4(args):
     lib.dbgz_set_profiling(ctx.handle, 1)
     prof = L.DbgzProfile()
     out = {}
-    for name, prec in (("fp32_simt", L.PREC_FP32_SIMT), ("fp64", L.PREC_FP64)):
+    for name, prec in (("fp32_split_bf16", L.PREC_FP32_SPLIT_BF16), ("fp32_simt", L.PREC_FP32_SIMT),
+                       ("fp64", L.PREC_FP64)):
         for _ in range(args.warmup):
             D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=prec)
         wall, dev, loop, prep = [], [], [], []
@@ -187,15 +188,17 @@ def run_c4(args):
                      "loop_ms": statistics.mean(loop), "prepare_ms": statistics.mean(prep), "P": P}
     dims = np.array([w.d for w in ws])
     samples = float(opts.m * opts.n_reps * len(ws))
-    P32, P64 = out["fp32_simt"].pop("P"), out["fp64"].pop("P")
+    Pt, P32, P64 = out["fp32_split_bf16"].pop("P"), out["fp32_simt"].pop("P"), out["fp64"].pop("P")
     line = {
-        "metric": "C4 batch: 4096 MVN probabilities (d ~ U{16..256}) per call", "value": out["fp32_simt"]["e2e_ms"],
+        "metric": "C4 batch: 4096 MVN probabilities (d ~ U{16..256}) per call",
+        "value": out["fp32_split_bf16"]["e2e_ms"],
         "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
         "dtype": "fp32", "data": "synthetic",
         "config": {"workload": f"c4_{len(ws)}_problems_sobol", "points": opts.m, "shifts": opts.n_reps,
                    "sum_d": int(dims.sum()), "sample_dims": samples * float(dims.mean())},
-        "modes": out, "max_abs_err_fp32_vs_fp64": float(np.max(np.abs(P32 - P64))),
-        "sample_dims_per_s_fp32": samples * float(dims.mean() - 1) / (out["fp32_simt"]["loop_ms"] * 1e-3),
+        "modes": out, "max_abs_err_fp32_vs_fp64": float(np.max(np.abs(Pt - P64))),
+        "max_abs_err_fp32_simt_vs_fp64": float(np.max(np.abs(P32 - P64))),
+        "sample_dims_per_s_fp32": samples * float(dims.mean() - 1) / (out["fp32_split_bf16"]["loop_ms"] * 1e-3),
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(256) k_prepare_batch(const BatchProb *probs, d
                                                        double *b_all, int64_t *perm_all, double *scale_all,
                                                        double *work_all, int64_t *rank_all, float *U32_all,
                                                        TargetParams64 *t64_all, TargetParams32 *t32_all,
-                                                       SimtParams<T> *params, int64_t bs1) {
+                                                       SimtParams<T> *params, double *first3, int64_t bs1) {
   const BatchProb P = probs[blockIdx.x];
   const int64_t n = P.d;
   double *M = M_all + P.off2, *a = a_all + P.off1, *b = b_all + P.off1, *scale = scale_all + P.off1;
@@ -133,6 +133,9 @@ __global__ void __launch_bounds__(256) k_prepare_batch(const BatchProb *probs, d
     params[blockIdx.x].c1 = c1;
     params[blockIdx.x].dc1 = dc1;
     params[blockIdx.x].up1 = 1.0 - c1 - dc1;
+    first3[3 * blockIdx.x] = c1;
+    first3[3 * blockIdx.x + 1] = dc1;
+    first3[3 * blockIdx.x + 2] = 1.0 - c1 - dc1;
   }
 }
 
@@ -198,7 +201,10 @@ template <typename T>
 int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigma, const double *a, const double *b,
               const dbgz_opts &o, int qmc_type, const double *shifts, const uint64_t *ushifts,
               const uint32_t *dirnums, int64_t sobol_first, double *results, double *errs, int64_t *ranks,
-              int *any_rank_fail) {
+              int *any_rank_fail, int precision) {
+  // tensor-core loop for the single-phase problems when a tensor-core mode is
+  // asked for (FP32 only); the SIMT loop for everything else
+  const bool tensor = sizeof(T) == 4 && (precision == DBGZ_PREC_FP32_SPLIT_BF16 || precision == DBGZ_PREC_FP32_TF32);
   const int64_t R = o.n_reps, m = o.m;
   const int64_t tps = (m + simt::TS - 1) / simt::TS;
   std::vector<BatchProb> probs(np);
@@ -218,7 +224,12 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return dims[x] > dims[y]; });
   std::vector<BatchItem> items;
+  std::vector<int64_t> tensor_probs;
   for (int64_t k : order) {
+    if (tensor && dims[k] - 1 <= 256) {
+      tensor_probs.push_back(k);
+      continue;
+    }
     const int64_t nt = tps * R;
     const int64_t run = std::max<int64_t>(1, std::min<int64_t>(nt, kItemDims / dims[k]));
     for (int64_t t0 = 0; t0 < nt; t0 += run)
@@ -226,7 +237,7 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
   }
   int64_t grid = 0;
   DBGZ_TRY(batch_grid<T>(ctx, qmc_type, &grid));
-  grid = std::min<int64_t>(grid, (int64_t)items.size());
+  grid = std::max<int64_t>(1, std::min<int64_t>(grid, (int64_t)items.size()));
   // one pooled allocation for everything
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t szM = al(8 * (size_t)s2), sz1 = al(8 * (size_t)s1), szU32 = al(4 * (size_t)s2);
@@ -237,8 +248,9 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
   const size_t szPart = al(8 * (size_t)(np * tps * R)), szReps = al(8 * (size_t)(np * R));
   const size_t szY = al(sizeof(T) * (size_t)Dp * simt::TS * (size_t)grid);
   const size_t szProbs = al(sizeof(BatchProb) * np), szPO = al(8 * (size_t)np), szRank = al(8 * (size_t)np);
+  const size_t szFirst = al(3 * 8 * (size_t)np);
   const size_t total = szM + 5 * sz1 + 3 * sz1 + szU32 + szT64 + szT32 + szP + szI + szS64 + szS32 + szQ + szV +
-                       szPart + szReps + szY + szProbs + szPO + szRank + 256;
+                       szPart + szReps + szY + szProbs + szPO + szRank + szFirst + 512;
   DevBuf buf;
   DBGZ_TRY(dbgz_ensure(ctx, buf, total));
   char *base = (char *)buf.p;
@@ -263,6 +275,7 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
   T *dY = (T *)take(szY);
   BatchProb *dprobs = (BatchProb *)take(szProbs);
   int64_t *dpo = (int64_t *)take(szPO), *drank = (int64_t *)take(szRank);
+  double *dfirst = (double *)take(szFirst);
   uint64_t *dush = (uint64_t *)dsh64;  // Sobol shifts share the Richtmyer slot (8 bytes each)
   unsigned long long *dcounter = (unsigned long long *)take(256);
   cudaStream_t st = ctx->stream;
@@ -339,15 +352,49 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
       const int smb = (int)cholk::genz_block_smem_bytes(dmax);
       cudaFuncSetAttribute(k_prepare_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smb);
       k_prepare_batch<T><<<(unsigned)np, 256, smb, st>>>(dprobs, dM, da, db, dperm, dscale, dwork, drank, dU32,
-                                                         dt64, dt32, dparams, o.chol_block_size);
+                                                         dt64, dt32, dparams, dfirst, o.chol_block_size);
     }
     dbgz_count_launch(ctx);
     if (ctx->profiling) cudaEventRecord(ctx->ev[3], st);
-    if (qmc_type == DBGZ_QMC_SOBOL)
-      rc = launch_batch_loop<T, DBGZ_QMC_SOBOL>(ctx, dparams, ditems, (int64_t)items.size(), dcounter, dY, Dp, grid);
-    else
-      rc = launch_batch_loop<T, DBGZ_QMC_RICHTMYER>(ctx, dparams, ditems, (int64_t)items.size(), dcounter, dY, Dp,
-                                                    grid);
+    if (!tensor_probs.empty()) {
+      UmmaBatchArgs A;
+      A.qmc_type = qmc_type;
+      A.n_bits = (int)o.n_bits;
+      A.m = m;
+      A.n_reps = R;
+      A.tiles_per_shift = tps;
+      A.sobol_first = sobol_first;
+      A.probs = tensor_probs;
+      std::vector<int64_t> h_off2(np), h_off1(np), h_offs(np);
+      for (int64_t k = 0; k < np; ++k) {
+        h_off2[k] = probs[k].off2;
+        h_off1[k] = probs[k].off1;
+        h_offs[k] = probs[k].offs;
+      }
+      A.dims = dims;
+      A.off2 = h_off2.data();
+      A.off1 = h_off1.data();
+      A.offs = h_offs.data();
+      A.part_off = part_off.data();
+      A.dM = dM;
+      A.dfirst = dfirst;
+      A.dq = dq;
+      A.dU32 = dU32;
+      A.dsh32 = qmc_type == DBGZ_QMC_RICHTMYER ? dsh32 : nullptr;
+      A.dt32 = dt32;
+      A.dV = qmc_type == DBGZ_QMC_SOBOL ? dV : nullptr;
+      A.dush = qmc_type == DBGZ_QMC_SOBOL ? dush : nullptr;
+      A.dpart = dpart;
+      if ((rc = dbgz_loop_umma_batch(ctx, precision, A))) break;
+    }
+    if (!items.empty()) {
+      if (qmc_type == DBGZ_QMC_SOBOL)
+        rc = launch_batch_loop<T, DBGZ_QMC_SOBOL>(ctx, dparams, ditems, (int64_t)items.size(), dcounter, dY, Dp,
+                                                  grid);
+      else
+        rc = launch_batch_loop<T, DBGZ_QMC_RICHTMYER>(ctx, dparams, ditems, (int64_t)items.size(), dcounter, dY, Dp,
+                                                      grid);
+    }
     if (rc) break;
     if (ctx->profiling) cudaEventRecord(ctx->ev[4], st);
     k_finalize_batch<<<(unsigned)((np * R + 127) / 128), 128, 0, st>>>(dpart, dpo, tps, R, np, m, dreps);
@@ -361,8 +408,14 @@ int run_batch(dbgz_ctx *ctx, int64_t np, const int64_t *dims, const double *Sigm
       break;
     }
     if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
+    int dev_status = 0;
+    if (!tensor_probs.empty()) cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
       rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_batch: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    if (dev_status != 0) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_TIMEOUT, "pnorm_batch: a bounded wait in the tensor-core loop gave up");
       break;
     }
     for (int64_t k = 0; k < np; ++k) {
@@ -434,10 +487,10 @@ extern "C" int dbgz_pnorm_batch(dbgz_ctx *ctx, int64_t n_problems, const int64_t
   int fail = 0, rc;
   if (precision == DBGZ_PREC_FP64)
     rc = run_batch<double>(ctx, n_problems, dims, Sigma, a, b, o, qmc_type, shifts, ushifts, sobol_dirnums,
-                           sobol_first, results, errs, ranks, &fail);
+                           sobol_first, results, errs, ranks, &fail, precision);
   else
     rc = run_batch<float>(ctx, n_problems, dims, Sigma, a, b, o, qmc_type, shifts, ushifts, sobol_dirnums,
-                          sobol_first, results, errs, ranks, &fail);
+                          sobol_first, results, errs, ranks, &fail, precision);
   if (rc == DBGZ_OK && fail)
     return dbgz_fail(ctx, DBGZ_ERR_RANK_DEFICIENT,
                      "pnorm_batch: some problems are not full rank (their result is NaN; see ranks)");

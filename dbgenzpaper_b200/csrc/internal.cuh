@@ -154,6 +154,25 @@ int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *p
                    int64_t n_tiles);
 int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);
+// Forward tensor-core loop over many single-phase problems (d - 1 <= 256) in
+// one launch (batch.cu).  Host tables cover all problems of the batch;
+// `probs` lists the ones to run here, largest first.  Device pointers: FP64
+// factors (dM + off2[k]), FP32 factors, FP32 targets, 3 first-dimension
+// constants per problem, generator data (shifts at offs[k]) and partial sums
+// (dpart + part_off[k]).  Resets ctx->d_status; the caller reads it.
+struct UmmaBatchArgs {
+  int qmc_type = 0, n_bits = 32;
+  int64_t m = 0, n_reps = 0, tiles_per_shift = 0, sobol_first = 0;
+  std::vector<int64_t> probs;
+  const int64_t *dims = nullptr, *off2 = nullptr, *off1 = nullptr, *offs = nullptr, *part_off = nullptr;
+  const double *dM = nullptr, *dfirst = nullptr, *dq = nullptr;
+  const float *dU32 = nullptr, *dsh32 = nullptr;
+  const TargetParams32 *dt32 = nullptr;
+  const uint32_t *dV = nullptr;
+  const uint64_t *dush = nullptr;
+  double *dpart = nullptr;
+};
+int dbgz_loop_umma_batch(dbgz_ctx *ctx, int precision, const UmmaBatchArgs &A);
 int dbgz_loop_sparse(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                      int64_t n_tiles);
 int dbgz_build_csc(dbgz_problem *p);

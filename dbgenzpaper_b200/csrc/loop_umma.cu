@@ -28,6 +28,9 @@
 // warp 5 TMA producer.  Every wait is bounded (sm100.cuh); a timeout sets
 // DBGZ_ERR_TIMEOUT in the status word and the CTA drains and leaves.
 #include <cuda.h>
+#include <algorithm>
+#include <cstring>
+#include <vector>
 
 #include "internal.cuh"
 #include "genz_step.cuh"
@@ -57,6 +60,19 @@ struct Fmt<DBGZ_PREC_FP32_TF32> {
   static constexpr uint32_t IDESC_FMT = 2;  // TF32
 };
 
+// One problem of a batched launch (global memory): its U^T panel maps and
+// the per-problem fields the kernel otherwise takes from UmmaParams.  Single
+// phase only (d - 1 <= the phase width): no y workspace.
+struct __align__(64) UmmaProb {
+  CUtensorMap tm_u[2];
+  int64_t d, nY, m, tiles_per_shift;
+  dbgz::GenParams gen;
+  const float *U32;
+  const TargetParams32 *tgt;
+  const double *first;  // c1, dc1, up1 of the first dimension (device-computed)
+  double *partials;
+};
+
 struct __align__(64) UmmaParams {
   CUtensorMap tm_u[2];  // U^T panel parts: rows = targets, K = y-index
   CUtensorMap tm_y[2];  // Y workspace parts: rows = slot*128 + sample, K = y-index
@@ -69,17 +85,20 @@ struct __align__(64) UmmaParams {
   double *partials;
   int *status;
   pol::GradIO<float> io;
+  // batched launch: work item `it` is tile item_tile[it] of problem item_prob[it]
+  const UmmaProb *probs;
+  const int32_t *item_prob, *item_tile;
 };
 
 struct Phase {
   int64_t L;
   int Pr, nb;
 };
-__device__ __forceinline__ Phase phase_of(const UmmaParams &p, int64_t ph) {
+__device__ __forceinline__ Phase phase_of(int Pw, int64_t nY, int64_t ph) {
   Phase f;
-  f.L = ph * p.P;
-  int64_t w = p.nY - f.L;
-  if (w > p.P) w = p.P;
+  f.L = ph * Pw;
+  int64_t w = nY - f.L;
+  if (w > Pw) w = Pw;
   f.Pr = (int)((w + BK - 1) / BK) * BK;
   f.nb = f.Pr / BK;
   return f;
@@ -154,7 +173,9 @@ __device__ __forceinline__ void rank8_update(float (&s)[BK], const float (&ys)[8
 }
 
 // Policy: pol::Forward<float, GEN, STORE> or pol::Adjoint<float, GEN>.
-template <int MODE, typename Policy>
+// BATCH: work items are (problem, tile) pairs of a batched launch, each
+// problem single-phase; every role walks the same static item sequence.
+template <int MODE, typename Policy, bool BATCH = false>
 __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ UmmaParams P) {
   using F = Fmt<MODE>;
   using SM = Smem<MODE>;
@@ -165,7 +186,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
   Misc *ms = reinterpret_cast<Misc *>(sm + SM::off_misc(P.P));
   volatile int *abort = &ms->abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t nphase = (P.nY + P.P - 1) / P.P;
+  const int64_t nphase1 = (P.nY + P.P - 1) / P.P;  // phases of the single problem
   const int32_t slot_row = (int32_t)blockIdx.x * TS;
   const int bpart = SM::bpart(P.P);
 
@@ -186,7 +207,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
     tmem_alloc(&ms->tmem_base, (uint32_t)P.P);
     tmem_relinquish();
   }
-  if (warp == kProdWarp && lane == 0) {
+  if (!BATCH && warp == kProdWarp && lane == 0) {
     prefetch_tmap(&P.tm_u[0]);
     prefetch_tmap(&P.tm_y[0]);
     if (F::NPART > 1) {
@@ -205,9 +226,19 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0}, ws_cnt = 0;
       uint32_t ja = 0, jb = 0;
       bool ok = true;
-      for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
+      for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles && ok; it += gridDim.x) {
+        const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
+        const CUtensorMap *tmu = BATCH ? pb->tm_u : P.tm_u;
+        const int64_t nYi = BATCH ? pb->nY : P.nY, nphase = BATCH ? 1 : nphase1;
+        if (BATCH) {
+          // the maps were written by a host copy before the launch: order
+          // them before the tensor-map proxy reads them (system scope, as the
+          // writer is the host)
+          for (int pp = 0; pp < F::NPART; ++pp)
+            asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(&tmu[pp]) : "memory");
+        }
         for (int64_t ph = 0; ph < nphase && ok; ++ph) {
-          const Phase f = phase_of(P, ph);
+          const Phase f = phase_of(P.P, nYi, ph);
           if (ph > 0) {
             ok = mbar_wait(&ms->ws_ready, ws_cnt & 1, abort);
             ++ws_cnt;
@@ -224,7 +255,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
               for (int pp = 0; pp < F::NPART; ++pp)
                 for (int i = 0; i < nbox; ++i)
-                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &P.tm_u[pp],
+                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &tmu[pp],
                               (int32_t)(kc * BK), (int32_t)(f.L + 1 + 64 * i), &ms->b_full[ib]);
               ++a_use[ia];
               ++b_use[ib];
@@ -244,7 +275,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
               for (int pp = 0; pp < F::NPART; ++pp)
                 for (int i = 0; i < nbox; ++i)
-                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &P.tm_u[pp],
+                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &tmu[pp],
                               (int32_t)(f.L + BK * b), (int32_t)(f.L + 1 + BK * (b + 1) + 64 * i),
                               &ms->b_full[ib]);
             } else {
@@ -294,9 +325,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           }
         }
       };
-      for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles && ok; tile += gridDim.x) {
+      for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles && ok; it += gridDim.x) {
+        const int64_t nYi = BATCH ? P.probs[P.item_prob[it]].nY : P.nY, nphase = BATCH ? 1 : nphase1;
         for (int64_t ph = 0; ph < nphase && ok; ++ph) {
-          const Phase f = phase_of(P, ph);
+          const Phase f = phase_of(P.P, nYi, ph);
           const int64_t nkc = ph > 0 ? f.L / BK : 0;
           for (int64_t kc = 0; kc < nkc && ok; ++kc) {
             const int ia = ja & 1, ib = jb & 1;
@@ -355,26 +387,37 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
     const int r = tid;  // sample row = TMEM lane
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
     uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
-    const bool need_ws = nphase > 1;
+    const bool need_ws = !BATCH && nphase1 > 1;
     uint32_t blk = 0;  // blocks run by this CTA (selects the staging buffer)
-    for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
-      const int64_t k_shift = tile / P.tiles_per_shift;
-      const int64_t jt = tile - k_shift * P.tiles_per_shift;
+    for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles; it += gridDim.x) {
+      const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
+      const int64_t tile = BATCH ? (int64_t)P.item_tile[it] : it;
+      const int64_t dI = BATCH ? pb->d : P.d, nYI = BATCH ? pb->nY : P.nY, mI = BATCH ? pb->m : P.m;
+      const int64_t tpsI = BATCH ? pb->tiles_per_shift : P.tiles_per_shift;
+      const float *U32I = BATCH ? pb->U32 : P.U32;
+      const TargetParams32 *tgtI = BATCH ? pb->tgt : P.tgt;
+      double *partsI = BATCH ? pb->partials : P.partials;
+      const int64_t nphase = BATCH ? 1 : nphase1;
+      const int64_t k_shift = tile / tpsI;
+      const int64_t jt = tile - k_shift * tpsI;
       const int64_t j = jt * TS + r;
       Policy pl;
-      pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
+      if (BATCH)
+        pl.tile_begin(pb->gen, dI, tile, tpsI, r, pb->first[0], pb->first[1], pb->first[2], 0, P.io);
+      else
+        pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
       // asynchronous staging of one block into buffer `buf` (one commit group)
       auto stage_block = [&](int buf, int64_t lb, int nv) {
         for (int e = r; e < BK * BK; e += TS) {
           const int li = e % BK, ti = e / BK;
           const bool v = li <= ti && ti < nv;
-          pol::cp_async_or_zero<4>(&ms->ublk[buf][li][ti], v ? P.U32 + (lb + ti + 1) * P.d + lb + li : P.U32, v);
+          pol::cp_async_or_zero<4>(&ms->ublk[buf][li][ti], v ? U32I + (lb + ti + 1) * dI + lb + li : U32I, v);
         }
-        pl.stage_async(ms->sg[buf], P.tgt, r, lb, nv);
+        pl.stage_async(ms->sg[buf], tgtI, r, lb, nv);
         pol::cp_async_commit();
       };
       for (int64_t ph = 0; ph < nphase; ++ph) {
-        const Phase f = phase_of(P, ph);
+        const Phase f = phase_of(P.P, nYI, ph);
         if (ph > 0) {
           for (int64_t kc = 0; kc < f.L / BK; ++kc) {
             ++a_use[ja & 1];
@@ -384,15 +427,15 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         for (int b = 0; b < f.nb; ++b) {
           const int ia = ja & 1;
           const int64_t lbase = f.L + BK * b;
-          const int nval = (int)((P.nY - lbase) < BK ? (P.nY - lbase) : BK);
+          const int nval = (int)((nYI - lbase) < BK ? (nYI - lbase) : BK);
           const int cur = (int)(blk & 1);
           // the block's U triangle and per-dimension constants: staged during
           // the previous block of the tile, or now for the tile's first block
           if (ph == 0 && b == 0) stage_block(cur, lbase, nval);
           pol::cp_async_wait_all();
           named_sync(kBarScalar, TS);
-          if (lbase + BK < P.nY) {
-            const int64_t nb2 = P.nY - lbase - BK;
+          if (lbase + BK < nYI) {
+            const int64_t nb2 = nYI - lbase - BK;
             stage_block(cur ^ 1, lbase + BK, (int)(nb2 < BK ? nb2 : BK));
           }
           float(*ublk)[kUld] = ms->ublk[cur];
@@ -504,12 +547,12 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       }
       // per-tile end and sum of p in a fixed order
       {
-        pl.tile_end(P.tgt, r, warp, tile, j < P.m);
-        double pv = pl.tile_value(j < P.m);
+        pl.tile_end(tgtI, r, warp, tile, j < mI);
+        double pv = pl.tile_value(j < mI);
         for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
         if (lane == 0) ms->red[warp] = pv;
         named_sync(kBarScalar, TS);
-        if (r == 0) P.partials[tile] = ((ms->red[0] + ms->red[1]) + ms->red[2]) + ms->red[3];
+        if (r == 0) partsI[tile] = ((ms->red[0] + ms->red[1]) + ms->red[2]) + ms->red[3];
       }
     }
   done:
@@ -690,7 +733,172 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   return DBGZ_OK;
 }
 
+// U^T panels of many problems: problems blockIdx.y + i gridDim.y, factor at
+// M + off2[k] (d x d), panel at byte offset pan[k] of out0/out1 with leading
+// dimension ldU[k] (rows t = 0..d-1).
+template <int MODE>
+__global__ void k_make_ut_batch(const double *M, int64_t n, const int64_t *dims, const int64_t *off2,
+                                const int64_t *ldU, const int64_t *pan, char *out0, char *out1) {
+  for (int64_t k = blockIdx.y; k < n; k += gridDim.y) {
+  const int64_t d = dims[k], ld = ldU[k];
+  const double *U = M + off2[k];
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < d * ld; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = e / ld, l = e - t * ld;
+    const double u = (l < t) ? U[t * d + l] : 0.0;
+    if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
+      const __nv_bfloat16 h = __double2bfloat16(u);
+      const __nv_bfloat16 lo = __double2bfloat16(u - (double)__bfloat162float(h));
+      reinterpret_cast<__nv_bfloat16 *>(out0 + pan[k])[e] = h;
+      reinterpret_cast<__nv_bfloat16 *>(out1 + pan[k])[e] = lo;
+    } else {
+      reinterpret_cast<uint32_t *>(out0 + pan[k])[e] = to_tf32((float)u);
+    }
+  }
+  }
+}
+
+template <int MODE>
+int launch_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A) {
+  using F = Fmt<MODE>;
+  using SM = Smem<MODE>;
+  const int Pw = 256;
+  const int64_t nsel = (int64_t)A.probs.size();
+  if (nsel == 0) return DBGZ_OK;
+  // panels and per-problem tables
+  std::vector<int64_t> dims(nsel), off2(nsel), ld(nsel), pan(nsel);
+  size_t pan_bytes = 0;
+  int64_t n_items = 0, dmax = 0;
+  for (int64_t i = 0; i < nsel; ++i) {
+    const int64_t k = A.probs[i], d = A.dims[k];
+    if (d - 1 > Pw) return dbgz_fail(ctx, DBGZ_ERR_DIMENSION, "tensor batch: d = %lld needs more than one phase", (long long)d);
+    dims[i] = d;
+    off2[i] = A.off2[k];
+    ld[i] = ((d - 1 + 63) / 64) * 64;
+    pan[i] = (int64_t)pan_bytes;
+    pan_bytes += (size_t)d * ld[i] * F::ESZ;
+    pan_bytes = (pan_bytes + 255) & ~size_t(255);
+    n_items += A.tiles_per_shift * A.n_reps;
+    dmax = std::max(dmax, d);
+  }
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t szTab = al(8 * (size_t)nsel);
+  const size_t szDesc = al(sizeof(UmmaProb) * (size_t)nsel), szItems = al(4 * (size_t)n_items);
+  DevBuf buf;
+  DBGZ_TRY(dbgz_ensure(ctx, buf, pan_bytes * F::NPART + 4 * szTab + szDesc + 2 * szItems + 1024));
+  char *base = (char *)buf.p;
+  auto take = [&](size_t b) {
+    char *r = base;
+    base += al(b);
+    return r;
+  };
+  char *pan0 = take(pan_bytes), *pan1 = F::NPART > 1 ? take(pan_bytes) : nullptr;
+  int64_t *d_dims = (int64_t *)take(szTab), *d_off2 = (int64_t *)take(szTab), *d_ld = (int64_t *)take(szTab),
+          *d_pan = (int64_t *)take(szTab);
+  UmmaProb *d_desc = (UmmaProb *)take(szDesc);
+  int32_t *d_iprob = (int32_t *)take(szItems), *d_itile = (int32_t *)take(szItems);
+  cudaStream_t st = ctx->stream;
+  int rc = DBGZ_OK;
+  do {
+    if (cudaMemcpyAsync(d_dims, dims.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_off2, off2.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_ld, ld.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_pan, pan.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: upload failed");
+      break;
+    }
+    k_make_ut_batch<MODE><<<dim3(8, (unsigned)std::min<int64_t>(nsel, 65535)), 256, 0, st>>>(A.dM, nsel, d_dims,
+                                                                                         d_off2, d_ld, d_pan,
+                                                                                         pan0, pan1);
+    dbgz_count_launch(ctx);
+    // descriptors (maps encoded here, on the host)
+    std::vector<UmmaProb> hd(nsel);
+    for (int64_t i = 0; i < nsel && rc == DBGZ_OK; ++i) {
+      const int64_t k = A.probs[i];
+      UmmaProb &D = hd[i];
+      std::memset(&D, 0, sizeof(D));
+      if ((rc = encode_2d<MODE>(ctx, &D.tm_u[0], pan0 + pan[i], (uint64_t)ld[i], (uint64_t)dims[i], 64))) break;
+      if (F::NPART > 1 && (rc = encode_2d<MODE>(ctx, &D.tm_u[1], pan1 + pan[i], (uint64_t)ld[i], (uint64_t)dims[i], 64)))
+        break;
+      D.d = dims[i];
+      D.nY = dims[i] - 1;
+      D.m = A.m;
+      D.tiles_per_shift = A.tiles_per_shift;
+      D.gen.qmc_type = A.qmc_type;
+      D.gen.n_bits = A.n_bits;
+      D.gen.gen_base = 0;
+      D.gen.sobol_first = A.sobol_first;
+      D.gen.q = A.dq;
+      D.gen.shift32 = A.dsh32 ? A.dsh32 + A.offs[k] : nullptr;
+      D.gen.V = A.dV;
+      D.gen.ushift = A.dush ? A.dush + A.offs[k] : nullptr;
+      D.U32 = A.dU32 + A.off2[k];
+      D.tgt = A.dt32 + A.off1[k];
+      D.first = A.dfirst + 3 * k;
+      D.partials = A.dpart + A.part_off[k];
+    }
+    if (rc) break;
+    // items: every tile of every problem, largest problems first (the
+    // problems come sorted), dealt to CTAs round robin
+    std::vector<int32_t> ip(n_items), itl(n_items);
+    int64_t q = 0;
+    for (int64_t i = 0; i < nsel; ++i)
+      for (int64_t t = 0; t < A.tiles_per_shift * A.n_reps; ++t, ++q) {
+        ip[q] = (int32_t)i;
+        itl[q] = (int32_t)t;
+      }
+    if (cudaMemcpyAsync(d_desc, hd.data(), sizeof(UmmaProb) * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_iprob, ip.data(), 4 * n_items, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_itile, itl.data(), 4 * n_items, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: upload failed");
+      break;
+    }
+    const int smem = SM::total(Pw);
+    auto kern = A.qmc_type == DBGZ_QMC_SOBOL ? k_genz_umma<MODE, pol::Forward<float, DBGZ_QMC_SOBOL, false>, true>
+                                             : k_genz_umma<MODE, pol::Forward<float, DBGZ_QMC_RICHTMYER, false>, true>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: kernel attributes");
+      break;
+    }
+    cudaFuncAttributes fa;
+    cudaFuncGetAttributes(&fa, kern);
+    int smem_per_sm = 0, regs_per_sm = 0;
+    cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
+    cudaDeviceGetAttribute(&regs_per_sm, cudaDevAttrMaxRegistersPerMultiprocessor, ctx->device);
+    int per_sm = std::min(512 / Pw, smem_per_sm / (smem + 1024));
+    per_sm = std::min(per_sm, regs_per_sm / std::max(((fa.numRegs + 7) / 8) * 8 * NT, 1));
+    if (per_sm < 1) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: kernel does not fit on an SM");
+      break;
+    }
+    const int64_t grid = std::min<int64_t>(n_items, (int64_t)per_sm * ctx->num_sms);
+    UmmaParams P{};
+    P.P = Pw;
+    P.n_tiles = n_items;
+    P.tile0 = 0;
+    P.nY = 1;
+    P.status = ctx->d_status;
+    P.probs = d_desc;
+    P.item_prob = d_iprob;
+    P.item_tile = d_itile;
+    if (cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st) != cudaSuccess) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: status reset");
+      break;
+    }
+    kern<<<(unsigned)grid, NT, smem, st>>>(P);
+    dbgz_count_launch(ctx);
+    if (cudaGetLastError() != cudaSuccess) rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: launch failed");
+  } while (0);
+  dbgz_release(buf);  // stream-ordered: later users of the block run after the kernel
+  return rc;
+}
+
 }  // namespace
+
+int dbgz_loop_umma_batch(dbgz_ctx *ctx, int precision, const UmmaBatchArgs &A) {
+  if (precision == DBGZ_PREC_FP32_SPLIT_BF16) return launch_umma_batch<DBGZ_PREC_FP32_SPLIT_BF16>(ctx, A);
+  return launch_umma_batch<DBGZ_PREC_FP32_TF32>(ctx, A);
+}
 
 int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials, int64_t n_tiles) {
   if (precision == DBGZ_PREC_FP32_SPLIT_BF16)

@@ -94,3 +94,48 @@ def test_batch_fp32_accuracy_many_uneven(dbgz):
     P64, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP64)
     P32, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SIMT)
     assert np.all(np.abs(P32 - P64) <= 2e-6 + 1e-5 * np.abs(P64))
+
+
+@pytest.mark.parametrize("qmc", ["Richtmyer", "Sobol"])
+@pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
+def test_batch_tensor_core_matches_one_problem_path(dbgz, qmc, prec):
+    # problems with d - 1 <= 256 run in the batched tensor-core loop, the rest
+    # (d = 300 here) in the SIMT batch loop; each against qmc_pnorm of the same
+    # precision (the first dimension's CDF is computed on the device in the
+    # batch and on the host in the one-problem path, hence not bit for bit)
+    D = dbgz
+    dims = DIMS + [257, 250, 130]
+    probs = _problems(dims, 17)
+    opts = D.QMC_opts(m=1000, n_reps=6, max_pts=1000, max_abs_err=0.0)
+    rng = np.random.default_rng(9)
+    if qmc == "Richtmyer":
+        sh = [rng.random((d - 1, 6)) for d in dims]
+        P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, shifts=sh, precision=prec)
+    else:
+        ush = [rng.integers(0, 2**63, size=(d - 1, 6), dtype=np.uint64) for d in dims]
+        P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, ushifts=ush, precision=prec)
+    for k, (S, a, b) in enumerate(probs):
+        if qmc == "Richtmyer":
+            Q = D.QMCData(S, a, b, opts, qmc_type=qmc, shifts=sh[k])
+        else:
+            Q = D.QMCData(S, a, b, opts, qmc_type=qmc, ushifts=ush[k])
+        P1, e1, _ = D.qmc_pnorm(Q, precision=prec)
+        P64, _, _ = D.qmc_pnorm(Q, precision=L.PREC_FP64)
+        Q.close()
+        assert abs(P[k] - P1) <= 1e-6 * abs(P1) + 1e-12, (k, dims[k], P[k], P1)
+        assert abs(P[k] - P64) <= 2e-6 + 1e-5 * abs(P64), (k, dims[k], P[k], P64)
+
+
+def test_batch_tensor_core_many_problems(dbgz):
+    # more problems than CTAs, all single-phase: the item list spans problems
+    D = dbgz
+    rng = np.random.default_rng(44)
+    dims = list(rng.integers(2, 258, size=400))
+    probs = _problems(dims, 45)
+    opts = D.QMC_opts(m=512, n_reps=4, max_pts=512, max_abs_err=0.0)
+    ush = [rng.integers(0, 2**63, size=(d - 1, 4), dtype=np.uint64) for d in dims]
+    P64, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP64)
+    Pt, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SPLIT_BF16)
+    Ps, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SIMT)
+    assert np.all(np.abs(Pt - P64) <= 2e-6 + 1e-5 * np.abs(P64))
+    assert np.all(np.abs(Pt - Ps) <= 2e-6 + 1e-5 * np.abs(Ps))
