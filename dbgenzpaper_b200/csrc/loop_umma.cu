@@ -492,6 +492,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 }
                 ys[k] = y;
               }
+              pl.chunk_end(lbase + 8 * ch, nval - 8 * ch);
               switch (ch) {
                 case 0: rank8_update<24>(s, ys, &ublk[0][8]); break;
                 case 1: rank8_update<16>(s, ys, &ublk[8][16]); break;

@@ -160,6 +160,7 @@ struct Forward {
   }
   // chunked form (8 steps whose per-sample inputs may be loaded up front)
   __device__ __forceinline__ void chunk_begin(int64_t, int) {}
+  __device__ __forceinline__ void chunk_end(int64_t, int) {}
   __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int) { return emit(sg, li, l); }
   __device__ __forceinline__ void consume(const Staged<T> &sg, T s, int li, int64_t l) {
     const auto tg = sg.tg[li];
@@ -403,8 +404,12 @@ struct Adjoint {
     return emit_from(sg, li, l, y, io.s[t * io.N + g], io.dc[t * io.N + g]);
   }
   // chunked form: the stored state of the chunk's 8 steps (steps l0 .. l0+7,
-  // n of them valid) is loaded before the first, so the loads overlap
+  // n of them valid) is loaded before the first, so the loads overlap; in
+  // the FP32 paths the weighted per-variable terms of the 8 steps are kept
+  // and summed over the warp together in chunk_end
   T pre_y[8], pre_s[8], pre_dc[8];
+  float acc_a[8], acc_b[8], acc_u[8];
+  uint32_t fp64_done;  // steps of the chunk whose sums were written by the FP64 fallback (warp-uniform)
   __device__ __forceinline__ void chunk_begin(int64_t l0, int n) {
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
@@ -413,10 +418,70 @@ struct Adjoint {
       pre_y[kk] = (v && t <= d - 2) ? io.y[t * io.N + g] : T(0);
       pre_s[kk] = v ? io.s[t * io.N + g] : T(0);
       pre_dc[kk] = v ? io.dc[t * io.N + g] : T(0);
+      acc_a[kk] = acc_b[kk] = acc_u[kk] = 0.0f;
     }
+    fp64_done = 0u;
   }
   __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk) {
-    return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk]);
+    if (sizeof(T) != 4) return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk]);
+    const int64_t t = d - 1 - l;
+    const bool has_u = t <= d - 2;
+    const double w = has_u ? point_w(sg, li, t) : 0.0;
+    float fa, fb, fu;
+    const float sb = variable32(sg.tg[li], (float)w, has_u, (float)pre_y[kk], (float)pre_s[kk],
+                                (float)pre_dc[kk], true, fa, fb, fu);
+    const float wa = wrel * fa, wb = wrel * fb, wu = wrel * fu;
+    const bool fin = isfinite(sb) && isfinite(wa) && isfinite(wb) && isfinite(wu);
+    if (__all_sync(0xffffffffu, fin)) {
+      acc_a[kk] = wa;
+      acc_b[kk] = wb;
+      acc_u[kk] = wu;
+      if (io.sbar) io.sbar[t * io.N + g] = (T)(p * (double)sb);
+      return (T)sb;
+    }
+    // a term beyond FP32 range in the warp: this step in FP64, its sums
+    // written at once
+    fp64_done |= 1u << kk;
+    double ga, gb, gu;
+    const double sbd = variable(sg.tg[li], w, has_u, pre_y[kk], pre_s[kk], pre_dc[kk], true, ga, gb, gu);
+    accumulate(t, ga, gb, gu);
+    if (io.sbar) io.sbar[t * io.N + g] = (T)(p * sbd);
+    return (T)sbd;
+  }
+  // sum of 8 values per lane over the 32 lanes of the warp, 8 sums at once:
+  // three exchange-and-add rounds halve the values a lane holds (lanes
+  // 16 apart split the 8 variables 4/4, then 8 apart 2/2, then 4 apart
+  // 1/1), two plain rounds finish the sum; lane L ends with the sum of
+  // variable (L >> 2) & 7.  9 shuffles instead of 40.
+  static __device__ __forceinline__ float warp_sum8(float (&v)[8], int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float send = b4 ? v[i] : v[i + 4], keep = b4 ? v[i + 4] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float send = b3 ? v[i] : v[i + 2], keep = b3 ? v[i + 2] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const float send = b2 ? v[0] : v[1], keep = b2 ? v[1] : v[0];
+    float r = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    r += __shfl_xor_sync(0xffffffffu, r, 2);
+    r += __shfl_xor_sync(0xffffffffu, r, 1);
+    return r;
+  }
+  __device__ __forceinline__ void chunk_end(int64_t l0, int n) {
+    if (sizeof(T) != 4 || n <= 0) return;
+    const float sa = warp_sum8(acc_a, lane), sbv = warp_sum8(acc_b, lane), su = warp_sum8(acc_u, lane);
+    const int kk = (lane >> 2) & 7;
+    if ((lane & 3) == 0 && kk < n && !((fp64_done >> kk) & 1u)) {
+      const int64_t t = d - 1 - (l0 + kk);
+      const int64_t row = ((tile - io.tile0) * 4 + warp) * d + t;
+      io.ga[row] = (double)sa * wmax;
+      io.gb[row] = (double)sbv * wmax;
+      io.gu[row] = (double)su * wmax;
+    }
   }
   __device__ __forceinline__ void consume(const Staged<T> &, T r_sum, int, int64_t) { ybar = (double)r_sum; }
 
