@@ -152,8 +152,13 @@ def cpu_baseline(w, threads: int, target_s: float = 12.0):
 
 def run_c4(args):
     """The batch configuration: 4096 problems, d ~ U{16..256}, Sobol 2^14 x 8
-    each, one dbgz_pnorm_batch call (upload, batched FP64 Cholesky, batched
-    loop, read-back).  Rank 0 only; one JSON line."""
+    each.  The loops' engine per dimension is chosen by the library's
+    autotuner (once, untimed, reported); each mode runs as a batch plan (one
+    CUDA graph per run: upload of Sigma, a, b and shifts from the plan's
+    pinned host buffers, batched FP64 Cholesky, batched loops, reduction,
+    read-back), timed from the host around the run (e2e) and on the device.
+    The one-shot call (Python packing of the problem list, pageable uploads,
+    no graph) is timed beside it.  Rank 0 only; one JSON line."""
     import torch
     import dbgenzpaper_b200 as D
     from dbgenzpaper_b200 import _lib as L
@@ -165,30 +170,48 @@ def run_c4(args):
     ws = W.c4(n_problems=n_prob)
     probs = [(w.Sigma, w.a, w.b) for w in ws]
     ush = [w.ushifts for w in ws]
+    dims = np.array([w.d for w in ws])
     opts = D.QMC_opts(m=ws[0].m, n_reps=ws[0].n_reps, max_pts=ws[0].m, max_abs_err=0.0)
     ctx = D.get_context(0)
     lib = L.lib()
+    t = time.perf_counter()
+    eng, items = D.batch_autotune(opts, L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
+    tune_s = time.perf_counter() - t
+    tensor_from = int(np.argmax(eng[2:] == 1) + 2) if np.any(eng[2:] == 1) else None
     lib.dbgz_set_profiling(ctx.handle, 1)
     prof = L.DbgzProfile()
     out = {}
     for name, prec in (("fp32_split_bf16", L.PREC_FP32_SPLIT_BF16), ("fp32_simt", L.PREC_FP32_SIMT),
                        ("fp64", L.PREC_FP64)):
+        t = time.perf_counter()
+        plan = D.BatchPlan(dims, opts, qmc_type="Sobol", precision=prec, context=ctx)
+        create_ms = 1e3 * (time.perf_counter() - t)
+        plan.fill(probs, ush)
+        info = plan.info()
         for _ in range(args.warmup):
-            D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=prec)
+            plan.run()
         wall, dev, loop, prep = [], [], [], []
         for _ in range(args.steps):
             t = time.perf_counter()
-            P, err = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=prec)
+            P, err = plan.run()
             wall.append(1e3 * (time.perf_counter() - t))
             lib.dbgz_get_profile(ctx.handle, C.byref(prof))
             dev.append(prof.pnorm_ms)
             loop.append(prof.loop_ms)
             prep.append(prof.prepare_ms)
+        plan.close()
         out[name] = {"e2e_ms": statistics.mean(wall), "device_ms": statistics.mean(dev),
-                     "loop_ms": statistics.mean(loop), "prepare_ms": statistics.mean(prep), "P": P}
-    dims = np.array([w.d for w in ws])
+                     "loop_ms": statistics.mean(loop), "prepare_ms": statistics.mean(prep),
+                     "plan_create_ms": create_ms, "plan": info, "P": P}
+    # the one-shot call of the split-BF16 mode (Python list in, no plan)
+    D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SPLIT_BF16, context=ctx)
+    t = time.perf_counter()
+    P1, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SPLIT_BF16,
+                              context=ctx)
+    one_shot_ms = 1e3 * (time.perf_counter() - t)
     samples = float(opts.m * opts.n_reps * len(ws))
     Pt, P32, P64 = out["fp32_split_bf16"].pop("P"), out["fp32_simt"].pop("P"), out["fp64"].pop("P")
+    nR = len(ws) * opts.n_reps
     line = {
         "metric": "C4 batch: 4096 MVN probabilities (d ~ U{16..256}) per call",
         "value": out["fp32_split_bf16"]["e2e_ms"],
@@ -196,6 +219,13 @@ def run_c4(args):
         "dtype": "fp32", "data": "synthetic",
         "config": {"workload": f"c4_{len(ws)}_problems_sobol", "points": opts.m, "shifts": opts.n_reps,
                    "sum_d": int(dims.sum()), "sample_dims": samples * float(dims.mean())},
+        "e2e": {"value": out["fp32_split_bf16"]["e2e_ms"], "unit": "ms",
+                "h2d_bytes_per_step": out["fp32_split_bf16"]["plan"]["host_bytes"],
+                "d2h_bytes_per_step": 8 * nR + 8 * len(ws) + 4 * (len(ws) + 2)},
+        "autotune": {"seconds": tune_s, "tensor_core_loop_from_d": tensor_from,
+                     "simt_item_dims_at_d16": int(items[16]), "simt_item_dims_at_d256": int(items[256])},
+        "one_shot_e2e_ms_fp32_split_bf16": one_shot_ms,
+        "one_shot_equals_plan": bool(np.array_equal(P1, Pt)),
         "modes": out, "max_abs_err_fp32_vs_fp64": float(np.max(np.abs(Pt - P64))),
         "max_abs_err_fp32_simt_vs_fp64": float(np.max(np.abs(P32 - P64))),
         "sample_dims_per_s_fp32": samples * float(dims.mean() - 1) / (out["fp32_split_bf16"]["loop_ms"] * 1e-3),

@@ -43,7 +43,8 @@ __all__ = [
     "QMCOpts", "QMC_opts", "QMCData", "QMCDataSparse", "QMCData_Distributions",
     "qmc_pnorm", "qmc_pnorm_grad", "CholeskyGenz", "cholesky_genz", "cholesky_classic",
     "get_sqrt_primes", "richtmyer_mat", "sobol_mat", "sobol_dirnums", "Context",
-    "get_context", "DbgzError", "PRECISIONS",
+    "get_context", "DbgzError", "PRECISIONS", "qmc_pnorm_batch", "BatchPlan", "batch_autotune",
+    "batch_tuning",
 ]
 
 DbgzError = L.DbgzError
@@ -402,6 +403,130 @@ def qmc_pnorm_batch(problems, opts: Optional[QMCOpts] = None, rng=None, qmc_type
         return P, err, ranks
     L.check(st, ctx.handle)
     return (P, err, ranks) if return_ranks else (P, err)
+
+
+class BatchPlan:
+    """A reusable batch (dbgz_batch_plan_*; no counterpart in the reference):
+    the problems' dimensions, options, generator and precision are fixed at
+    creation, which makes the device buffers, tensor maps and a CUDA graph of
+    one run.  Fill the plan's pinned host buffers -- `fill(problems, ...)`,
+    or write the packed numpy views `Sigma`, `a`, `b`, `shifts` directly --
+    then `run()`: one graph launch uploads them, checks them, factorises,
+    integrates, reduces and reads back.  Richtmyer shifts are doubles in
+    [0, 1], Sobol shifts uint64 digital shifts."""
+
+    def __init__(self, dims, opts: Optional[QMCOpts] = None, qmc_type="Richtmyer", *,
+                 precision: Optional[int] = None, sobol_dirnums=None, sobol_first=None,
+                 device: int = 0, context: Optional[Context] = None):
+        qmc_type = str(qmc_type).lstrip(":")
+        if qmc_type not in ("Richtmyer", "Sobol"):
+            raise ValueError("qmc_type must be 'Richtmyer' or 'Sobol'")
+        self.opts = QMC_opts() if opts is None else opts
+        self.qmc_type = qmc_type
+        self.ctx = get_context(device) if context is None else context
+        self.dims = np.ascontiguousarray(dims, dtype=np.int64)
+        R = self.opts.n_reps
+        self.precision = ((L.PREC_FP64 if self.opts.T == np.float64 else DEFAULT_FP32_PRECISION)
+                          if precision is None else int(precision))
+        V = None if sobol_dirnums is None else np.ascontiguousarray(sobol_dirnums, dtype=np.uint32)
+        first = (2 * self.opts.m - 1) + 1 if sobol_first is None else int(sobol_first)
+        self._lib = L.lib()
+        h = C.c_void_p()
+        co = self.opts.to_c()
+        L.check(self._lib.dbgz_batch_plan_create(
+            self.ctx.handle, len(self.dims), L.ptr(self.dims, C.c_int64), C.byref(co),
+            L.QMC_RICHTMYER if qmc_type == "Richtmyer" else L.QMC_SOBOL, self.precision,
+            L.ptr(V, C.c_uint32), first, C.byref(h)), self.ctx.handle)
+        self.handle = h
+        pS, pa, pb, psh = L._pd(), L._pd(), L._pd(), C.c_void_p()
+        L.check(self._lib.dbgz_batch_plan_buffers(h, C.byref(pS), C.byref(pa), C.byref(pb), C.byref(psh)))
+        d = self.dims
+        s2, s1, ss = int((d * d).sum()), int(d.sum()), int(((d - 1) * R).sum())
+        self.off2 = np.concatenate([[0], np.cumsum(d * d)[:-1]]).astype(np.int64)
+        self.off1 = np.concatenate([[0], np.cumsum(d)[:-1]]).astype(np.int64)
+        self.offs = np.concatenate([[0], np.cumsum((d - 1) * R)[:-1]]).astype(np.int64)
+        self.Sigma = np.ctypeslib.as_array(pS, shape=(s2,))
+        self.a = np.ctypeslib.as_array(pa, shape=(s1,))
+        self.b = np.ctypeslib.as_array(pb, shape=(s1,))
+        sht = C.c_double if qmc_type == "Richtmyer" else C.c_uint64
+        self.shifts = np.ctypeslib.as_array(C.cast(psh, C.POINTER(sht)), shape=(ss,))
+
+    def set_problem(self, k: int, Sigma, a, b, shifts) -> None:
+        """Write problem k's Sigma (d x d), bounds and (d-1, n_reps) shifts."""
+        d = int(self.dims[k])
+        R = self.opts.n_reps
+        self.Sigma[self.off2[k]:self.off2[k] + d * d] = np.ravel(np.asarray(Sigma, dtype=np.float64), order="F")
+        self.a[self.off1[k]:self.off1[k] + d] = _f64(a)
+        self.b[self.off1[k]:self.off1[k] + d] = _f64(b)
+        self.shifts[self.offs[k]:self.offs[k] + (d - 1) * R] = np.ravel(
+            np.asarray(shifts, dtype=self.shifts.dtype), order="F")
+
+    def fill(self, problems, shifts) -> None:
+        """problems: sequence of (Sigma, a, b); shifts: the per-problem (d-1, n_reps) arrays."""
+        for k, (S, a, b) in enumerate(problems):
+            self.set_problem(k, S, a, b, shifts[k])
+
+    def run(self, return_ranks: bool = False):
+        """One graph launch; -> (P, err) (and the ranks with return_ranks)."""
+        n = len(self.dims)
+        P, err = np.zeros(n), np.zeros(n)
+        ranks = np.zeros(n, dtype=np.int64)
+        st = self._lib.dbgz_batch_plan_run(self.handle, L.ptr(P), L.ptr(err), L.ptr(ranks, C.c_int64))
+        if return_ranks and st == L.ERR_RANK_DEFICIENT:
+            return P, err, ranks
+        L.check(st, self.ctx.handle)
+        return (P, err, ranks) if return_ranks else (P, err)
+
+    def info(self) -> dict:
+        """Tensor-core problems, SIMT work items, kernels per run, pinned input bytes."""
+        v = [C.c_int64() for _ in range(4)]
+        L.check(self._lib.dbgz_batch_plan_info(self.handle, *[C.byref(x) for x in v]))
+        return dict(zip(("tensor_problems", "simt_items", "kernels_per_run", "host_bytes"),
+                        [int(x.value) for x in v]))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.dbgz_batch_plan_destroy(self.handle)
+            self.handle = None
+            self.Sigma = self.a = self.b = self.shifts = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_autotune(opts: Optional[QMCOpts] = None, precision: Optional[int] = None, qmc_type="Sobol", *,
+                   device: int = 0, context: Optional[Context] = None):
+    """dbgz_batch_autotune: time the batch loops per dimension bucket on pilot
+    batches of opts' point and shift counts and keep the fastest choice in
+    the context.  -> (engine, item_dims), arrays indexed by d = 0..512
+    (engine 1 = tensor-core loop, 0 = SIMT loop)."""
+    opts = QMC_opts() if opts is None else opts
+    ctx = get_context(device) if context is None else context
+    prec = ((L.PREC_FP64 if opts.T == np.float64 else DEFAULT_FP32_PRECISION)
+            if precision is None else int(precision))
+    qmc_type = str(qmc_type).lstrip(":")
+    eng = np.zeros(513, dtype=np.int32)
+    items = np.zeros(513, dtype=np.int32)
+    co = opts.to_c()
+    L.check(L.lib().dbgz_batch_autotune(ctx.handle, prec, L.QMC_RICHTMYER if qmc_type == "Richtmyer" else L.QMC_SOBOL,
+                                        C.byref(co), L.ptr(eng, C.c_int32), L.ptr(items, C.c_int32)), ctx.handle)
+    return eng, items
+
+
+def batch_tuning(precision: int, qmc_type="Sobol", *, device: int = 0, context: Optional[Context] = None):
+    """The batch engine table in use: -> (engine, item_dims, tuned)."""
+    ctx = get_context(device) if context is None else context
+    qmc_type = str(qmc_type).lstrip(":")
+    eng = np.zeros(513, dtype=np.int32)
+    items = np.zeros(513, dtype=np.int32)
+    tuned = C.c_int()
+    L.check(L.lib().dbgz_batch_tuning(ctx.handle, int(precision),
+                                      L.QMC_RICHTMYER if qmc_type == "Richtmyer" else L.QMC_SOBOL,
+                                      L.ptr(eng, C.c_int32), L.ptr(items, C.c_int32), C.byref(tuned)), ctx.handle)
+    return eng, items, bool(tuned.value)
 
 
 # ---- primitives -------------------------------------------------------------

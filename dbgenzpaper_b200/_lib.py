@@ -98,6 +98,16 @@ SIGNATURES = {
     "dbgz_pnorm_batch": (C.c_int, [_vp, C.c_int64, _pi64, _pd, _pd, _pd, C.POINTER(DbgzOpts), C.c_int, C.c_int,
                                    _pd, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.c_int64, _pd, _pd,
                                    _pi64]),
+    "dbgz_batch_plan_create": (C.c_int, [_vp, C.c_int64, _pi64, C.POINTER(DbgzOpts), C.c_int, C.c_int, _pu32,
+                                         C.c_int64, C.POINTER(_vp)]),
+    "dbgz_batch_plan_buffers": (C.c_int, [_vp, C.POINTER(_pd), C.POINTER(_pd), C.POINTER(_pd), C.POINTER(_vp)]),
+    "dbgz_batch_plan_run": (C.c_int, [_vp, _pd, _pd, _pi64]),
+    "dbgz_batch_plan_info": (C.c_int, [_vp, _pi64, _pi64, _pi64, _pi64]),
+    "dbgz_batch_plan_destroy": (C.c_int, [_vp]),
+    "dbgz_batch_autotune": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(DbgzOpts), C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32)]),
+    "dbgz_batch_tuning": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int)]),
     "dbgz_pnorm_pass_noalloc": (C.c_int, [C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int64,
                                           C.c_int64, C.c_int64, _vp, _vp]),
     "dbgz_cholesky_genz": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,

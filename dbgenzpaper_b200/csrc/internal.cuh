@@ -35,6 +35,16 @@ struct DevBuf {
   dbgz_ctx *owner = nullptr;
 };
 
+// Batch engine choices per dimension (dbgz_batch_autotune): engine[d] = 1
+// for the tensor-core loop, 0 for the SIMT loop; item_dims[d] = size of the
+// SIMT loop's work items in tile-dimensions.
+constexpr int64_t kBatchMaxD = 512;
+struct BatchTuning {
+  bool tuned = false;
+  int8_t engine[kBatchMaxD + 1] = {};
+  int32_t item_dims[kBatchMaxD + 1] = {};
+};
+
 struct dbgz_ctx {
   int device = 0;
   int num_sms = 0;
@@ -55,6 +65,7 @@ struct dbgz_ctx {
   size_t pool_bytes = 0;
   int64_t live_problems = 0;  // problems created on this context and not yet freed
   size_t state_budget = size_t(48) << 30;  // bytes of stored forward state a gradient call may hold
+  BatchTuning batch_tune[4][2];            // [precision][qmc_type]
 };
 
 // Counts a kernel launch of the library (for dbgz_profile).
@@ -172,7 +183,24 @@ struct UmmaBatchArgs {
   const uint64_t *dush = nullptr;
   double *dpart = nullptr;
 };
-int dbgz_loop_umma_batch(dbgz_ctx *ctx, int precision, const UmmaBatchArgs &A);
+// Tensor-core part of a batch plan: the U^T panels, per-problem descriptors
+// (tensor maps of the plan's fixed buffers) and the item list, set up once;
+// enqueue issues the panel conversion, the status reset and the loop on
+// ctx->stream (no allocation, no host synchronisation: capturable).
+struct UmmaBatchPlan {
+  dbgz_ctx *ctx = nullptr;
+  int mode = 0, qmc_type = 0;
+  DevBuf buf;
+  char *pan0 = nullptr, *pan1 = nullptr, *d_desc = nullptr;
+  int64_t nsel = 0, n_items = 0, grid = 0;
+  int smem = 0;
+  int64_t *d_dims = nullptr, *d_off2 = nullptr, *d_ld = nullptr, *d_pan = nullptr;
+  int32_t *d_iprob = nullptr, *d_itile = nullptr;
+  const double *dM = nullptr;
+};
+int dbgz_umma_batch_setup(dbgz_ctx *ctx, int precision, const UmmaBatchArgs &A, UmmaBatchPlan **out);
+int dbgz_umma_batch_enqueue(UmmaBatchPlan *B);
+void dbgz_umma_batch_free(UmmaBatchPlan *B);
 int dbgz_loop_sparse(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                      int64_t n_tiles);
 int dbgz_build_csc(dbgz_problem *p);

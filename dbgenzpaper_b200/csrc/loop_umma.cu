@@ -758,17 +758,21 @@ __global__ void k_make_ut_batch(const double *M, int64_t n, const int64_t *dims,
   }
 }
 
+template <int MODE, int GEN>
+auto batch_kernel() {
+  return k_genz_umma<MODE, pol::Forward<float, GEN, false>, true>;
+}
+
 template <int MODE>
-int launch_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A) {
+int setup_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A, UmmaBatchPlan *B) {
   using F = Fmt<MODE>;
   using SM = Smem<MODE>;
   const int Pw = 256;
   const int64_t nsel = (int64_t)A.probs.size();
-  if (nsel == 0) return DBGZ_OK;
   // panels and per-problem tables
   std::vector<int64_t> dims(nsel), off2(nsel), ld(nsel), pan(nsel);
   size_t pan_bytes = 0;
-  int64_t n_items = 0, dmax = 0;
+  int64_t n_items = 0;
   for (int64_t i = 0; i < nsel; ++i) {
     const int64_t k = A.probs[i], d = A.dims[k];
     if (d - 1 > Pw) return dbgz_fail(ctx, DBGZ_ERR_DIMENSION, "tensor batch: d = %lld needs more than one phase", (long long)d);
@@ -779,126 +783,149 @@ int launch_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A) {
     pan_bytes += (size_t)d * ld[i] * F::ESZ;
     pan_bytes = (pan_bytes + 255) & ~size_t(255);
     n_items += A.tiles_per_shift * A.n_reps;
-    dmax = std::max(dmax, d);
   }
+  if (n_items > INT32_MAX) return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "tensor batch: too many tiles");
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t szTab = al(8 * (size_t)nsel);
   const size_t szDesc = al(sizeof(UmmaProb) * (size_t)nsel), szItems = al(4 * (size_t)n_items);
-  DevBuf buf;
-  DBGZ_TRY(dbgz_ensure(ctx, buf, pan_bytes * F::NPART + 4 * szTab + szDesc + 2 * szItems + 1024));
-  char *base = (char *)buf.p;
+  DBGZ_TRY(dbgz_ensure(ctx, B->buf, al(pan_bytes) * F::NPART + 4 * szTab + szDesc + 2 * szItems + 1024));
+  char *base = (char *)B->buf.p;
   auto take = [&](size_t b) {
     char *r = base;
     base += al(b);
     return r;
   };
-  char *pan0 = take(pan_bytes), *pan1 = F::NPART > 1 ? take(pan_bytes) : nullptr;
-  int64_t *d_dims = (int64_t *)take(szTab), *d_off2 = (int64_t *)take(szTab), *d_ld = (int64_t *)take(szTab),
-          *d_pan = (int64_t *)take(szTab);
-  UmmaProb *d_desc = (UmmaProb *)take(szDesc);
-  int32_t *d_iprob = (int32_t *)take(szItems), *d_itile = (int32_t *)take(szItems);
+  B->pan0 = take(pan_bytes);
+  B->pan1 = F::NPART > 1 ? take(pan_bytes) : nullptr;
+  B->d_dims = (int64_t *)take(szTab);
+  B->d_off2 = (int64_t *)take(szTab);
+  B->d_ld = (int64_t *)take(szTab);
+  B->d_pan = (int64_t *)take(szTab);
+  B->d_desc = take(szDesc);
+  B->d_iprob = (int32_t *)take(szItems);
+  B->d_itile = (int32_t *)take(szItems);
+  B->nsel = nsel;
+  B->n_items = n_items;
+  B->dM = A.dM;
+  // descriptors (maps encoded here, on the host, for the plan's fixed buffers)
+  std::vector<UmmaProb> hd(nsel);
+  for (int64_t i = 0; i < nsel; ++i) {
+    const int64_t k = A.probs[i];
+    UmmaProb &D = hd[i];
+    std::memset(&D, 0, sizeof(D));
+    DBGZ_TRY(encode_2d<MODE>(ctx, &D.tm_u[0], B->pan0 + pan[i], (uint64_t)ld[i], (uint64_t)dims[i], 64));
+    if (F::NPART > 1)
+      DBGZ_TRY(encode_2d<MODE>(ctx, &D.tm_u[1], B->pan1 + pan[i], (uint64_t)ld[i], (uint64_t)dims[i], 64));
+    D.d = dims[i];
+    D.nY = dims[i] - 1;
+    D.m = A.m;
+    D.tiles_per_shift = A.tiles_per_shift;
+    D.gen.qmc_type = A.qmc_type;
+    D.gen.n_bits = A.n_bits;
+    D.gen.gen_base = 0;
+    D.gen.sobol_first = A.sobol_first;
+    D.gen.q = A.dq;
+    D.gen.shift32 = A.dsh32 ? A.dsh32 + A.offs[k] : nullptr;
+    D.gen.V = A.dV;
+    D.gen.ushift = A.dush ? A.dush + A.offs[k] : nullptr;
+    D.U32 = A.dU32 + A.off2[k];
+    D.tgt = A.dt32 + A.off1[k];
+    D.first = A.dfirst + 3 * k;
+    D.partials = A.dpart + A.part_off[k];
+  }
+  // items: every tile of every problem, largest problems first (the caller
+  // sorts them), dealt to CTAs round robin
+  std::vector<int32_t> ip(n_items), itl(n_items);
+  int64_t q = 0;
+  for (int64_t i = 0; i < nsel; ++i)
+    for (int64_t t = 0; t < A.tiles_per_shift * A.n_reps; ++t, ++q) {
+      ip[q] = (int32_t)i;
+      itl[q] = (int32_t)t;
+    }
+  // static tables: uploaded once (pageable sources; the stream is synchronised
+  // before the host vectors go out of scope)
   cudaStream_t st = ctx->stream;
-  int rc = DBGZ_OK;
-  do {
-    if (cudaMemcpyAsync(d_dims, dims.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_off2, off2.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_ld, ld.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_pan, pan.data(), 8 * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: upload failed");
-      break;
-    }
-    k_make_ut_batch<MODE><<<dim3(8, (unsigned)std::min<int64_t>(nsel, 65535)), 256, 0, st>>>(A.dM, nsel, d_dims,
-                                                                                         d_off2, d_ld, d_pan,
-                                                                                         pan0, pan1);
-    dbgz_count_launch(ctx);
-    // descriptors (maps encoded here, on the host)
-    std::vector<UmmaProb> hd(nsel);
-    for (int64_t i = 0; i < nsel && rc == DBGZ_OK; ++i) {
-      const int64_t k = A.probs[i];
-      UmmaProb &D = hd[i];
-      std::memset(&D, 0, sizeof(D));
-      if ((rc = encode_2d<MODE>(ctx, &D.tm_u[0], pan0 + pan[i], (uint64_t)ld[i], (uint64_t)dims[i], 64))) break;
-      if (F::NPART > 1 && (rc = encode_2d<MODE>(ctx, &D.tm_u[1], pan1 + pan[i], (uint64_t)ld[i], (uint64_t)dims[i], 64)))
-        break;
-      D.d = dims[i];
-      D.nY = dims[i] - 1;
-      D.m = A.m;
-      D.tiles_per_shift = A.tiles_per_shift;
-      D.gen.qmc_type = A.qmc_type;
-      D.gen.n_bits = A.n_bits;
-      D.gen.gen_base = 0;
-      D.gen.sobol_first = A.sobol_first;
-      D.gen.q = A.dq;
-      D.gen.shift32 = A.dsh32 ? A.dsh32 + A.offs[k] : nullptr;
-      D.gen.V = A.dV;
-      D.gen.ushift = A.dush ? A.dush + A.offs[k] : nullptr;
-      D.U32 = A.dU32 + A.off2[k];
-      D.tgt = A.dt32 + A.off1[k];
-      D.first = A.dfirst + 3 * k;
-      D.partials = A.dpart + A.part_off[k];
-    }
-    if (rc) break;
-    // items: every tile of every problem, largest problems first (the
-    // problems come sorted), dealt to CTAs round robin
-    std::vector<int32_t> ip(n_items), itl(n_items);
-    int64_t q = 0;
-    for (int64_t i = 0; i < nsel; ++i)
-      for (int64_t t = 0; t < A.tiles_per_shift * A.n_reps; ++t, ++q) {
-        ip[q] = (int32_t)i;
-        itl[q] = (int32_t)t;
-      }
-    if (cudaMemcpyAsync(d_desc, hd.data(), sizeof(UmmaProb) * nsel, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_iprob, ip.data(), 4 * n_items, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-        cudaMemcpyAsync(d_itile, itl.data(), 4 * n_items, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: upload failed");
-      break;
-    }
-    const int smem = SM::total(Pw);
-    auto kern = A.qmc_type == DBGZ_QMC_SOBOL ? k_genz_umma<MODE, pol::Forward<float, DBGZ_QMC_SOBOL, false>, true>
-                                             : k_genz_umma<MODE, pol::Forward<float, DBGZ_QMC_RICHTMYER, false>, true>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess) {
-      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: kernel attributes");
-      break;
-    }
-    cudaFuncAttributes fa;
-    cudaFuncGetAttributes(&fa, kern);
-    int smem_per_sm = 0, regs_per_sm = 0;
-    cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
-    cudaDeviceGetAttribute(&regs_per_sm, cudaDevAttrMaxRegistersPerMultiprocessor, ctx->device);
-    int per_sm = std::min(512 / Pw, smem_per_sm / (smem + 1024));
-    per_sm = std::min(per_sm, regs_per_sm / std::max(((fa.numRegs + 7) / 8) * 8 * NT, 1));
-    if (per_sm < 1) {
-      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: kernel does not fit on an SM");
-      break;
-    }
-    const int64_t grid = std::min<int64_t>(n_items, (int64_t)per_sm * ctx->num_sms);
-    UmmaParams P{};
-    P.P = Pw;
-    P.n_tiles = n_items;
-    P.tile0 = 0;
-    P.nY = 1;
-    P.status = ctx->d_status;
-    P.probs = d_desc;
-    P.item_prob = d_iprob;
-    P.item_tile = d_itile;
-    if (cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st) != cudaSuccess) {
-      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: status reset");
-      break;
-    }
-    kern<<<(unsigned)grid, NT, smem, st>>>(P);
-    dbgz_count_launch(ctx);
-    if (cudaGetLastError() != cudaSuccess) rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: launch failed");
-  } while (0);
-  dbgz_release(buf);  // stream-ordered: later users of the block run after the kernel
-  return rc;
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_dims, dims.data(), 8 * nsel, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_off2, off2.data(), 8 * nsel, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_ld, ld.data(), 8 * nsel, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_pan, pan.data(), 8 * nsel, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_desc, hd.data(), sizeof(UmmaProb) * nsel, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_iprob, ip.data(), 4 * n_items, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_itile, itl.data(), 4 * n_items, cudaMemcpyHostToDevice, st));
+  DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  // kernel configuration (attributes set here, outside any stream capture)
+  const int smem = SM::total(Pw);
+  auto kern = A.qmc_type == DBGZ_QMC_SOBOL ? batch_kernel<MODE, DBGZ_QMC_SOBOL>()
+                                           : batch_kernel<MODE, DBGZ_QMC_RICHTMYER>();
+  DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  cudaFuncAttributes fa;
+  DBGZ_CUDA_TRY(ctx, cudaFuncGetAttributes(&fa, kern));
+  int smem_per_sm = 0, regs_per_sm = 0;
+  cudaDeviceGetAttribute(&smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device);
+  cudaDeviceGetAttribute(&regs_per_sm, cudaDevAttrMaxRegistersPerMultiprocessor, ctx->device);
+  int per_sm = std::min(512 / Pw, smem_per_sm / (smem + 1024));
+  per_sm = std::min(per_sm, regs_per_sm / std::max(((fa.numRegs + 7) / 8) * 8 * NT, 1));
+  if (per_sm < 1) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor batch: kernel does not fit on an SM");
+  B->grid = std::min<int64_t>(n_items, (int64_t)per_sm * ctx->num_sms);
+  B->smem = smem;
+  return DBGZ_OK;
+}
+
+template <int MODE>
+int enqueue_umma_batch(UmmaBatchPlan *B) {
+  dbgz_ctx *ctx = B->ctx;
+  cudaStream_t st = ctx->stream;
+  k_make_ut_batch<MODE><<<dim3(8, (unsigned)std::min<int64_t>(B->nsel, 65535)), 256, 0, st>>>(
+      B->dM, B->nsel, B->d_dims, B->d_off2, B->d_ld, B->d_pan, B->pan0, B->pan1);
+  dbgz_count_launch(ctx);
+  UmmaParams P{};
+  P.P = 256;
+  P.n_tiles = B->n_items;
+  P.tile0 = 0;
+  P.nY = 1;
+  P.status = ctx->d_status;
+  P.probs = (const UmmaProb *)B->d_desc;
+  P.item_prob = B->d_iprob;
+  P.item_tile = B->d_itile;
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), st));
+  auto kern = B->qmc_type == DBGZ_QMC_SOBOL ? batch_kernel<MODE, DBGZ_QMC_SOBOL>()
+                                            : batch_kernel<MODE, DBGZ_QMC_RICHTMYER>();
+  kern<<<(unsigned)B->grid, NT, B->smem, st>>>(P);
+  dbgz_count_launch(ctx);
+  DBGZ_CUDA_TRY(ctx, cudaGetLastError());
+  return DBGZ_OK;
 }
 
 }  // namespace
 
-int dbgz_loop_umma_batch(dbgz_ctx *ctx, int precision, const UmmaBatchArgs &A) {
-  if (precision == DBGZ_PREC_FP32_SPLIT_BF16) return launch_umma_batch<DBGZ_PREC_FP32_SPLIT_BF16>(ctx, A);
-  return launch_umma_batch<DBGZ_PREC_FP32_TF32>(ctx, A);
+int dbgz_umma_batch_setup(dbgz_ctx *ctx, int precision, const UmmaBatchArgs &A, UmmaBatchPlan **out) {
+  *out = nullptr;
+  if (A.probs.empty()) return DBGZ_OK;
+  UmmaBatchPlan *B = new UmmaBatchPlan;
+  B->ctx = ctx;
+  B->mode = precision;
+  B->qmc_type = A.qmc_type;
+  const int rc = precision == DBGZ_PREC_FP32_SPLIT_BF16 ? setup_umma_batch<DBGZ_PREC_FP32_SPLIT_BF16>(ctx, A, B)
+                                                        : setup_umma_batch<DBGZ_PREC_FP32_TF32>(ctx, A, B);
+  if (rc != DBGZ_OK) {
+    dbgz_umma_batch_free(B);
+    return rc;
+  }
+  *out = B;
+  return DBGZ_OK;
+}
+
+int dbgz_umma_batch_enqueue(UmmaBatchPlan *B) {
+  if (!B) return DBGZ_OK;
+  return B->mode == DBGZ_PREC_FP32_SPLIT_BF16 ? enqueue_umma_batch<DBGZ_PREC_FP32_SPLIT_BF16>(B)
+                                             : enqueue_umma_batch<DBGZ_PREC_FP32_TF32>(B);
+}
+
+void dbgz_umma_batch_free(UmmaBatchPlan *B) {
+  if (!B) return;
+  dbgz_release(B->buf);
+  delete B;
 }
 
 int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials, int64_t n_tiles) {

@@ -268,8 +268,13 @@ int dbgz_pnorm_pass_noalloc(int64_t d, const double *U, const double *a, const d
  * bounds one after another, shifts (Richtmyer) or ushifts (Sobol) the
  * (d_k - 1) x n_reps blocks one after another; sobol_dirnums is one table
  * for the largest d - 1 (NULL: the library's own) and sobol_first the
- * first Sobol index (as in dbgz_prepare).  precision: DBGZ_PREC_FP64, or any
- * FP32 mode (the batch runs the FP32 SIMT loop for all of them).  results
+ * first Sobol index (as in dbgz_prepare).  precision: DBGZ_PREC_FP64 (FP64
+ * SIMT loop), DBGZ_PREC_FP32_SIMT, or a tensor-core mode: problems with
+ * d - 1 <= 256 then run in the batched tcgen05 loop and the others in the
+ * FP32 SIMT loop, as the context's tuning table (dbgz_batch_autotune) or the
+ * default (tensor-core loop from d = 25) says.  Inputs are checked on the
+ * device (non-finite Sigma, NaN bounds or a > b: DBGZ_ERR_NONFINITE_INPUT;
+ * Richtmyer shifts outside [0,1]: DBGZ_ERR_INVALID_ARGUMENT).  results
  * and errs (may be NULL) receive P and 3 SEM per problem, ranks (may be
  * NULL) the Cholesky rank; a problem that is not full rank gets NaN and the
  * call returns DBGZ_ERR_RANK_DEFICIENT after finishing the others. */
@@ -278,6 +283,41 @@ int dbgz_pnorm_batch(dbgz_ctx *ctx, int64_t n_problems, const int64_t *dims, con
                      int precision, const double *shifts, const uint64_t *ushifts,
                      const uint32_t *sobol_dirnums, int64_t sobol_first, double *results,
                      double *errs, int64_t *ranks);
+
+/* A reusable batch (the same problems' dimensions, options, generator and
+ * precision every run; new Sigma, a, b and shifts each run).  Creation makes
+ * the device buffers, tables, tensor maps and kernel configurations and
+ * captures one run as a CUDA graph that reads pinned host buffers of the
+ * plan: dbgz_batch_plan_buffers returns them (packed as for
+ * dbgz_pnorm_batch; shifts are doubles for Richtmyer, uint64 for Sobol), the
+ * caller fills them, and each dbgz_batch_plan_run launches the graph (upload,
+ * checks, factorisation, loops, reduction, read-back) and waits for it.
+ * Results and errors as dbgz_pnorm_batch.  The plan holds its context (like
+ * a problem): destroy it before the context. */
+typedef struct dbgz_batch_plan dbgz_batch_plan;
+int dbgz_batch_plan_create(dbgz_ctx *ctx, int64_t n_problems, const int64_t *dims,
+                           const dbgz_opts *opts, int qmc_type, int precision,
+                           const uint32_t *sobol_dirnums, int64_t sobol_first,
+                           dbgz_batch_plan **out);
+int dbgz_batch_plan_buffers(dbgz_batch_plan *plan, double **Sigma, double **a, double **b,
+                            void **shifts);
+int dbgz_batch_plan_run(dbgz_batch_plan *plan, double *results, double *errs, int64_t *ranks);
+int dbgz_batch_plan_info(const dbgz_batch_plan *plan, int64_t *n_tensor_problems,
+                         int64_t *n_simt_items, int64_t *kernels_per_run, int64_t *host_bytes);
+int dbgz_batch_plan_destroy(dbgz_batch_plan *plan);
+
+/* Autotuner of the batch loops: for dimension buckets of 2..512, times the
+ * SIMT loop with work items of 256, 1024 and 4096 tile-dimensions and (in
+ * the tensor-core precisions, d - 1 <= 256) the batched tensor-core loop on
+ * pilot batches of the options' point and shift counts, and stores the
+ * fastest choice per dimension in the context (used by later batch calls and
+ * plans of this precision and generator).  engine_out and item_dims_out (may
+ * be NULL) receive the table, indexed by d = 0..512 (1 = tensor-core loop).
+ * dbgz_batch_tuning reads the table in use (the default when not tuned). */
+int dbgz_batch_autotune(dbgz_ctx *ctx, int precision, int qmc_type, const dbgz_opts *opts,
+                        int32_t *engine_out, int32_t *item_dims_out);
+int dbgz_batch_tuning(const dbgz_ctx *ctx, int precision, int qmc_type, int32_t *engine_out,
+                      int32_t *item_dims_out, int *tuned);
 
 /* ---- primitives of the path (device compute, host buffers) ---------- */
 

@@ -139,3 +139,88 @@ def test_batch_tensor_core_many_problems(dbgz):
     Ps, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SIMT)
     assert np.all(np.abs(Pt - P64) <= 2e-6 + 1e-5 * np.abs(P64))
     assert np.all(np.abs(Pt - Ps) <= 2e-6 + 1e-5 * np.abs(Ps))
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_FP32_SIMT, L.PREC_FP32_SPLIT_BF16])
+@pytest.mark.parametrize("qmc", ["Richtmyer", "Sobol"])
+def test_batch_plan_graph_matches_one_shot(dbgz, prec, qmc):
+    # the graph of a plan runs the same kernels on the same inputs: the same
+    # bits as the one-shot call, run after run, with new inputs each run
+    D = dbgz
+    dims = [40, 7, 200, 33, 300, 16]
+    opts = D.QMC_opts(m=700, n_reps=5, max_pts=700, max_abs_err=0.0)
+    plan = D.BatchPlan(dims, opts, qmc_type=qmc, precision=prec)
+    try:
+        info = plan.info()
+        assert info["tensor_problems"] + info["simt_items"] > 0 and info["kernels_per_run"] >= 3
+        for seed in (21, 22):
+            probs = _problems(dims, seed)
+            rng = np.random.default_rng(seed)
+            if qmc == "Richtmyer":
+                sh = [rng.random((d - 1, 5)) for d in dims]
+                P1, e1 = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, shifts=sh, precision=prec)
+            else:
+                sh = [rng.integers(0, 2**63, size=(d - 1, 5), dtype=np.uint64) for d in dims]
+                P1, e1 = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, ushifts=sh, precision=prec)
+            plan.fill(probs, sh)
+            P, err = plan.run()
+            assert np.array_equal(P, P1) and np.array_equal(err, e1), (P - P1, err - e1)
+    finally:
+        plan.close()
+
+
+def test_batch_input_checks_on_device(dbgz):
+    D = dbgz
+    dims = [12, 30, 9]
+    opts = D.QMC_opts(m=256, n_reps=4, max_pts=256)
+    probs = _problems(dims, 31)
+    rng = np.random.default_rng(3)
+    sh = [rng.random((d - 1, 4)) for d in dims]
+    bad_S = [(S.copy(), a, b) for S, a, b in probs]
+    bad_S[1][0][3, 4] = np.nan
+    bad_ab = [(S, a.copy(), b.copy()) for S, a, b in probs]
+    bad_ab[2][1][0] = bad_ab[2][2][0] + 1.0  # a > b
+    bad_sh = [x.copy() for x in sh]
+    bad_sh[0][2, 1] = 1.5
+    for pr, shx, code in ((bad_S, sh, L.ERR_NONFINITE_INPUT), (bad_ab, sh, L.ERR_NONFINITE_INPUT),
+                          (probs, bad_sh, L.ERR_INVALID_ARGUMENT)):
+        with pytest.raises(L.DbgzError) as ei:
+            D.qmc_pnorm_batch(pr, opts, shifts=shx, precision=L.PREC_FP32_SIMT)
+        assert ei.value.status == code
+    plan = D.BatchPlan(dims, opts, precision=L.PREC_FP32_SPLIT_BF16)
+    try:
+        plan.fill(bad_S, sh)
+        with pytest.raises(L.DbgzError) as ei:
+            plan.run()
+        assert ei.value.status == L.ERR_NONFINITE_INPUT
+        plan.fill(probs, sh)  # the plan stays usable
+        P, _ = plan.run()
+        P1, _ = D.qmc_pnorm_batch(probs, opts, shifts=sh, precision=L.PREC_FP32_SPLIT_BF16)
+        assert np.array_equal(P, P1)
+    finally:
+        plan.close()
+
+
+def test_batch_autotune_table_and_results(dbgz):
+    # own context: the table is per context
+    D = dbgz
+    ctx = D.Context(0)
+    try:
+        opts = D.QMC_opts(m=1024, n_reps=4, max_pts=1024, max_abs_err=0.0)
+        eng0, it0, tuned0 = D.batch_tuning(L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
+        assert not tuned0 and eng0[24] == 0 and eng0[25] == 1 and eng0[258] == 0 and it0[100] == 1024
+        eng, items = D.batch_autotune(opts, L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
+        assert set(np.unique(eng[2:])) <= {0, 1} and np.all(eng[258:] == 0)
+        assert set(np.unique(items[2:])) <= {256, 1024, 4096}
+        eng2, items2, tuned = D.batch_tuning(L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
+        assert tuned and np.array_equal(eng2[2:], eng[2:]) and np.array_equal(items2[2:], items[2:])
+        dims = [10, 20, 60, 130, 250, 400]
+        probs = _problems(dims, 51)
+        rng = np.random.default_rng(52)
+        ush = [rng.integers(0, 2**63, size=(d - 1, 4), dtype=np.uint64) for d in dims]
+        Pt, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP32_SPLIT_BF16,
+                                  context=ctx)
+        P64, _ = D.qmc_pnorm_batch(probs, opts, qmc_type="Sobol", ushifts=ush, precision=L.PREC_FP64, context=ctx)
+        assert np.all(np.abs(Pt - P64) <= 2e-6 + 1e-5 * np.abs(P64))
+    finally:
+        ctx.close()
