@@ -234,6 +234,98 @@ def run_c4(args):
     return 0
 
 
+def run_small(args):
+    """The d = 10 (c1: Richtmyer 10^4 x 10, FP64, reordering on) and d = 500
+    (c2: Sobol 2^16 x 12; FP64, FP32+TF32 and split-BF16) configurations:
+    per mode the pass on the device (CUDA events on the library's stream)
+    and end to end through the API from host buffers (QMCData + qmc_pnorm,
+    wall clock), |P - P_FP64|; for c1 also the CPU checker (the C
+    restatement of the reference's Float64 path, all host threads) on the
+    full workload and |P_GPU - P_checker|.  Rank 0 only; one JSON line."""
+    import torch
+    import dbgenzpaper_b200 as D
+    from dbgenzpaper_b200 import _lib as L
+    from dbgenzpaper_b200 import workloads as W
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    w = W.c1() if args.workload == "c1" else W.c2()
+    ctx = D.get_context(0)
+    lib = L.lib()
+    lib.dbgz_set_profiling(ctx.handle, 1)
+    prof = L.DbgzProfile()
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device="cuda:0")
+    opts = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0)
+    kw = dict(qmc_type=w.qmc_type, shifts=w.shifts) if w.qmc_type == "Richtmyer" else \
+        dict(qmc_type=w.qmc_type, ushifts=w.ushifts)
+    modes = [("fp64", L.PREC_FP64)]
+    if args.workload == "c2":
+        modes += [("fp32_tf32", L.PREC_FP32_TF32), ("fp32_split_bf16", L.PREC_FP32_SPLIT_BF16),
+                  ("fp32_simt", L.PREC_FP32_SIMT)]
+    out = {}
+    for name, prec in modes:
+        Q = D.QMCData(w.Sigma, w.a, w.b, opts, precision=prec, **kw)
+        for _ in range(args.warmup):
+            D.qmc_pnorm(Q, precision=prec)
+        dev = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            P, err, _ = D.qmc_pnorm(Q, precision=prec)
+            lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+            dev.append(prof.pnorm_ms)
+        Q.close()
+        e2e = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            Q2 = D.QMCData(w.Sigma, w.a, w.b, opts, precision=prec, **kw)
+            P2, _, _ = D.qmc_pnorm(Q2, precision=prec)
+            e2e.append(1e3 * (time.perf_counter() - t))
+            Q2.close()
+        out[name] = {"pass_ms": statistics.median(dev), "e2e_ms": statistics.median(e2e), "P": P, "err": err}
+    P64 = out["fp64"]["P"]
+    for name in out:
+        out[name]["abs_err_vs_fp64"] = abs(out[name]["P"] - P64)
+    head = modes[-1][0] if args.workload == "c1" else "fp32_split_bf16"
+    line = {
+        "metric": f"{args.workload} (d={w.d}) MVN probability: one pass, end to end through the API",
+        "value": out[head]["e2e_ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": False, "dtype": "f64" if args.workload == "c1" else "fp32", "data": "synthetic",
+        "config": {"workload": w.name, "d": w.d, "points": w.m, "shifts": w.n_reps, "generator": w.qmc_type},
+        "modes": out,
+    }
+    if args.workload == "c2":
+        line["fp64_over_split_bf16_pass"] = out["fp64"]["pass_ms"] / out["fp32_split_bf16"]["pass_ms"]
+    if args.workload == "c1":
+        from oracle import oracle as O
+        O.build()
+        t = time.perf_counter()
+        F = O.cholesky_genz(w.Sigma, w.a, w.b, 64, 512)
+        Pc = O.qmc_pnorm(O.truncate_U(F["U"]), F["a"], F["b"], m=w.m, n_reps=w.n_reps, shifts=w.shifts,
+                         max_pts=w.m, max_abs_err=0.0, threads=os.cpu_count() or 1)[0]
+        cpu_ms = 1e3 * (time.perf_counter() - t)
+        line["cpu_baseline"] = {"value": cpu_ms, "unit": "ms", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": "the full c1 workload (factorisation and one pass)"}
+        line["abs_err_gpu_fp64_vs_checker"] = abs(P64 - Pc)
+        # the adaptive loop over 100 passes (max_pts = 100 m, no tolerance
+        # stop): host-driven passes against one device-driven graph launch
+        ad = {}
+        opts_ad = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=100 * w.m, max_abs_err=0.0)
+        for drv in ("host", "graph"):
+            Qa = D.QMCData(w.Sigma, w.a, w.b, opts_ad, precision=L.PREC_FP64, **kw)
+            D.qmc_pnorm(Qa, precision=L.PREC_FP64, driver=drv)
+            ts, r = [], None
+            for _ in range(max(args.steps, 3)):
+                t = time.perf_counter()
+                r = D.qmc_pnorm(Qa, precision=L.PREC_FP64, driver=drv)
+                ts.append(1e3 * (time.perf_counter() - t))
+            Qa.close()
+            ad[drv] = {"ms": statistics.median(ts), "n_pts": r[2], "P": r[0]}
+        line["adaptive_100_passes"] = ad
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_c5(args):
     """The banded configuration: d = 10^4 AR(1) (rho = 0.9), factor truncated to
     64 super-diagonals, a = -inf, Sobol 2^18 x 10; P (FP32 and FP64 banded
@@ -346,9 +438,10 @@ def main():
     ap.add_argument("--only", action="store_true",
                     help="time only --precision (no FP64/other modes/accuracy/e2e/CPU legs); for profiling")
     ap.add_argument("--grad", action="store_true", help="with --only: time the gradient call instead")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c5"],
-                    help="c3: the headline line (default); c4: the 4096-problem batch; c5: the banded "
-                         "d = 10^4 problem (separate lines)")
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c3: the headline line (default); c1: d = 10 with the CPU checker; c2: d = 500 "
+                         "precision modes; c4: the 4096-problem batch; c5: the banded d = 10^4 problem "
+                         "(separate lines)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -356,6 +449,8 @@ def main():
         return run_c4(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload in ("c1", "c2"):
+        return run_small(args)
 
     import torch
     import dbgenzpaper_b200 as D

@@ -280,12 +280,17 @@ class QMCData_Distributions:
         return getattr(self.D, name)
 
 
-def qmc_pnorm(D, use_AppleBLAS=None, *, precision: Optional[int] = None, return_reps=False):
+def qmc_pnorm(D, use_AppleBLAS=None, *, precision: Optional[int] = None, return_reps=False,
+              driver: str = "host"):
     """qmc_pnorm!(D) (src/qmc.jl:783-850) -> (result, err, n_pts).
 
     ``use_AppleBLAS`` is accepted for signature compatibility (it only steers
     CPU BLAS threading in the reference).  With ``return_reps`` the per-shift
-    running means are returned as a fourth element."""
+    running means are returned as a fourth element.  ``driver="graph"`` runs
+    the adaptive loop on the device (dbgz_pnorm_graph: one CUDA graph launch
+    for all passes); the results are the same bits."""
+    if driver not in ("host", "graph"):
+        raise ValueError("driver must be 'host' or 'graph'")
     dist = isinstance(D, QMCData_Distributions)
     base = D.D if dist else D
     prec = base.resolved_precision() if precision is None else int(precision)
@@ -295,7 +300,8 @@ def qmc_pnorm(D, use_AppleBLAS=None, *, precision: Optional[int] = None, return_
     if dist:
         lib.dbgz_problem_set_cdf_form(base.handle, L.CDF_ERFC)
     try:
-        st = lib.dbgz_pnorm(base.handle, prec, C.byref(res), C.byref(err), C.byref(npts), L.ptr(reps))
+        fn = lib.dbgz_pnorm_graph if driver == "graph" else lib.dbgz_pnorm
+        st = fn(base.handle, prec, C.byref(res), C.byref(err), C.byref(npts), L.ptr(reps))
     finally:
         if dist:
             lib.dbgz_problem_set_cdf_form(base.handle, int(base.cdf_form))

@@ -92,6 +92,7 @@ SIGNATURES = {
     "dbgz_problem_truncate_band": (C.c_int, [_vp, C.c_int64]),
     "dbgz_problem_factor": (C.c_int, [_vp, _pd, _pi64, _pd, _pd, _pd, _pi64]),
     "dbgz_pnorm": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
+    "dbgz_pnorm_graph": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
     "dbgz_pnorm_grad": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
     "dbgz_problem_sigma_adjoint": (C.c_int, [_vp, _pd, _pd, _pd, _pd]),
     "dbgz_pnorm_grad_sigma": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),

@@ -430,6 +430,8 @@ int dbgz_problem_free(dbgz_problem *p) {
                     &p->grad_buf, &p->yws, &p->partials, &p->reps,      &p->csc_colptr, &p->csc_row, &p->csc_val64,
                     &p->csc_val32, &p->cscb_colptr, &p->cscb_row, &p->cscb_val64, &p->cscb_val32};
   for (DevBuf *b : bufs) dbgz_release(*b);
+  dbgz_drop_graphs(p);
+  dbgz_release(p->drv_state);
   if (p->ctx) p->ctx->live_problems -= 1;
   delete p;
   return DBGZ_OK;
@@ -439,7 +441,10 @@ int dbgz_problem_set_cdf_form(dbgz_problem *p, int cdf_form) {
   if (!p) return DBGZ_ERR_INVALID_ARGUMENT;
   if (cdf_form != DBGZ_CDF_ERF && cdf_form != DBGZ_CDF_ERFC)
     return dbgz_fail(p->ctx, DBGZ_ERR_INVALID_ARGUMENT, "set_cdf_form: bad form %d", cdf_form);
-  if (p->cdf_form != cdf_form) p->c1_ready = false;
+  if (p->cdf_form != cdf_form) {
+    p->c1_ready = false;
+    dbgz_drop_graphs(p);
+  }
   p->cdf_form = cdf_form;
   return DBGZ_OK;
 }
@@ -454,6 +459,7 @@ int dbgz_problem_truncate_band(dbgz_problem *p, int64_t bandwidth) {
                        &p->Ublo, &p->Ubtf, &p->csc_colptr, &p->csc_row, &p->csc_val64, &p->csc_val32,
                        &p->cscb_colptr, &p->cscb_row, &p->cscb_val64, &p->cscb_val32};
   for (DevBuf *b : derived) dbgz_release(*b);
+  dbgz_drop_graphs(p);
   p->ldU = 0;
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return DBGZ_OK;

@@ -46,6 +46,7 @@ struct GenParams {
   const float *shift32;  // (d-1) x n_reps
   const uint32_t *V;     // Sobol direction numbers (d-1) x 32
   const uint64_t *ushift;// (d-1) x n_reps
+  const int64_t *gen_base_dev;  // when set, gen_base is read from here (device-driven passes)
 };
 
 // Gray-code Sobol integer of point index idx in dimension l, computed by

@@ -96,6 +96,12 @@ struct dbgz_problem {
   DevBuf q, shifts, shifts32, V, ushifts;
   int64_t sobol_first = 0;
   int64_t gen_base = 0;  // offset of the current point block (next_points! state)
+  // device-driven adaptive loop (driver_graph.cu): a graph per precision and
+  // the buffers and constants it was captured with
+  cudaGraph_t drv_graph[4] = {};
+  cudaGraphExec_t drv_exec[4] = {};
+  std::vector<uint64_t> drv_sig[4];
+  DevBuf drv_state;
   // derived operands (device, built on first use)
   DevBuf tgt64, tgt32, U32;
   DevBuf Uhi, Ulo, Utf;  // tensor-core operands of the contraction
@@ -160,6 +166,8 @@ struct PassArgs {
   int cdf_form;
   double c1, dc1;
   int64_t tile0 = 0;  // run tiles [tile0, n_tiles) only (sample chunks of the adjoint)
+  const int64_t *gen_base_dev = nullptr;  // device copy of gen_base (device-driven passes)
+  bool setup_only = false;  // make the launch's buffers and operands, launch nothing
 };
 int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);
@@ -204,5 +212,6 @@ void dbgz_umma_batch_free(UmmaBatchPlan *B);
 int dbgz_loop_sparse(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                      int64_t n_tiles);
 int dbgz_build_csc(dbgz_problem *p);
+void dbgz_drop_graphs(dbgz_problem *p);
 int dbgz_finalize_pass(dbgz_problem *p, const double *partials, int64_t tiles_per_shift,
                        int64_t n_pts0, int64_t m, double *reps);

@@ -43,6 +43,7 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.qmc_type = pa.qmc_type;
   P.gen.n_bits = pa.n_bits;
   P.gen.gen_base = pa.gen_base;
+  P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
@@ -82,6 +83,7 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   int64_t grid = std::min<int64_t>(n_tiles - pa.tile0, (int64_t)per_sm * ctx->num_sms);
   DBGZ_TRY(dbgz_ensure(ctx, p->yws, sizeof(T) * (size_t)P.Dp * TS * grid));
   P.yws = (T *)p->yws.p;
+  if (pa.setup_only) return DBGZ_OK;
   kern<<<(unsigned)grid, NT, smem, ctx->stream>>>(P);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());

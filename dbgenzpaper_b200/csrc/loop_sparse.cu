@@ -210,6 +210,7 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.gen.qmc_type = pa.qmc_type;
   P.gen.n_bits = pa.n_bits;
   P.gen.gen_base = pa.gen_base;
+  P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
@@ -257,6 +258,7 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
     DBGZ_TRY(dbgz_ensure(ctx, p->yws, sizeof(T) * (size_t)grid * W * TS));
     P.yglob = (T *)p->yws.p;
   }
+  if (pa.setup_only) return DBGZ_OK;
   kern<<<(unsigned)grid, TS, smem, ctx->stream>>>(P);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());

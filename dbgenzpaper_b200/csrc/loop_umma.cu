@@ -694,6 +694,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.qmc_type = pa.qmc_type;
   P.gen.n_bits = pa.n_bits;
   P.gen.gen_base = pa.gen_base;
+  P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
@@ -727,6 +728,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   for (int pp = 0; pp < F::NPART; ++pp)
     DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_y[pp], (char *)p->yws.p + pp * part_bytes, (uint64_t)Dp,
                              (uint64_t)grid * TS, TS));
+  if (pa.setup_only) return DBGZ_OK;
   DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
   kern<<<(unsigned)grid, NT, smem, ctx->stream>>>(P);
   dbgz_count_launch(ctx);

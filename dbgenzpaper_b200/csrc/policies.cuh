@@ -123,6 +123,7 @@ struct Forward {
                                              double up1, int cdf_form_, const GradIO<T> &io_) {
     gen = gp;
     gen.qmc_type = GEN;
+    if (gp.gen_base_dev) gen.gen_base = *gp.gen_base_dev;
     d = d_;
     k = tile / tiles_per_shift;
     j = (tile - k * tiles_per_shift) * 128 + r;
@@ -198,6 +199,7 @@ struct Adjoint {
                                              const GradIO<T> &io_) {
     gen = gp;
     gen.qmc_type = GEN;
+    if (gp.gen_base_dev) gen.gen_base = *gp.gen_base_dev;
     d = d_;
     tile = tile_;
     k = tile / tiles_per_shift;

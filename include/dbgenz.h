@@ -192,6 +192,16 @@ int dbgz_problem_factor(const dbgz_problem *p, double *U, int64_t *perm, double 
 int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err,
                int64_t *n_pts, double *qmc_reps);
 
+/* dbgz_pnorm with the adaptive loop driven on the device: one CUDA graph
+ * launch per call runs every pass -- a conditional while node whose body is
+ * one pass and a one-block step that updates the running means, forms the
+ * estimate and 3*SEM, advances the point offset and decides on another pass
+ * -- with no host round trip between passes.  Same results (bit for bit),
+ * generator state and errors as dbgz_pnorm; the graph is kept with the
+ * problem for later calls. */
+int dbgz_pnorm_graph(dbgz_problem *p, int precision, double *result, double *err,
+                     int64_t *n_pts, double *qmc_reps);
+
 /* Gradient of the estimate (no counterpart in the reference).  Runs one
  * pass of m points x n_reps shifts on the problem's current point set (the
  * first pass of dbgz_pnorm; the generator is not advanced), keeps the
