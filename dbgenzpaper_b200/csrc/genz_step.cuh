@@ -18,8 +18,9 @@
 //    the CDF, the clamp to [-9, 9] in erf units, the same fma pattern).
 //  * StepFp32: FP32 arithmetic kept close to the FP64 result where the
 //    reference's Float32 loop loses digits (tail masses from normal32.cuh,
-//    relative error < 3e-6 where they are above 1e-10; Phi^-1 from CUDA's
-//    normcdfinvf): the state keeps both tails -- lo = Phi(alpha), up = Phi(-beta)
+//    relative error < 3e-6 where they are above 1e-10; Phi^-1 of the smaller
+//    tail from normal32.cuh, relative error < 4e-7): the state keeps both
+//    tails -- lo = Phi(alpha), up = Phi(-beta)
 //    -- and dc, so that u (when u <= 1/2) and 1 - u (otherwise) are formed
 //    without cancellation and Phi^-1 is taken of the smaller one; dc is the
 //    difference of two tails of the same side only when the interval lies
@@ -179,7 +180,7 @@ struct StepFp32 {
     const float t = fmaf(w, dc, lo);
     const bool lower = t <= 0.5f;
     const float arg = lower ? t : fmaf(w1, dc, up);
-    const float y = normcdfinvf(fmaxf(arg, kEps));
+    const float y = phi_inv_lower_f32(fmaxf(arg, kEps));
     return lower ? y : -y;
   }
   __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
