@@ -313,12 +313,15 @@ struct Adjoint {
     const float r2 = 1.41421356237f, rpi = 0.398942280401f;
     const float inv_u = (float)tg.inv_u;
     const float xa = ((float)tg.a - s) * inv_u, xb = ((float)tg.b - s) * inv_u;
-    const float ea = rpi * expf(-xa * xa), eb_ = rpi * expf(-xb * xb);  // 0 at an infinite bound
+    // normal densities by the SFU's 2^z (0 at an infinite bound)
+    const float ea = rpi * dbgz::exp2_sfu((xa * xa) * -1.44269504089f);
+    const float eb_ = rpi * dbgz::exp2_sfu((xb * xb) * -1.44269504089f);
     const float fa = (!clamp9 || fabsf(xa) < 9.0f) ? ea : 0.0f;
     const float fb = (!clamp9 || fabsf(xb) < 9.0f) ? eb_ : 0.0f;
     const float rdc = __fdividef(1.0f, dc);
     const float pex = dc > 1e-36f ? rdc : (dc > 0.0f ? INFINITY : 0.0f);
-    const float ub = (float)ybar * __fdividef(1.0f, rpi * expf(-0.5f * y * y));
+    // ybar / phi(y) = ybar sqrt(2 pi) exp(y^2 / 2) (used for |y| < 8.13: below 2^48)
+    const float ub = (float)ybar * 2.50662827463f * dbgz::exp2_sfu((y * y) * 0.72134752045f);
     const float ubar = (has_u && fabsf(y) < 8.12585f) ? ub : 0.0f;
     const float eb = fmaf(ubar, w, pex), cb = fmaf(ubar, 1.0f - w, -pex);
     const float rU = inv_u * r2;
