@@ -159,8 +159,9 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   // the adjoint pass writes per-tile values too (zeros); keep them away from
   // the forward pass's tile sums, which are reduced after the last chunk
   double *adj_tiles = (double *)take(8 * (size_t)n_tiles);
-  if (!sparse) {
-    // rows the passes leave unwritten enter the dU GEMM: clear them
+  if (!sparse && precision == DBGZ_PREC_FP64) {
+    // rows the passes leave unwritten (y row d-1, sbar row 0) enter the DGEMM:
+    // clear them (the FP32 GEMM computes l < t only, which never reads them)
     DBGZ_CUDA_TRY(ctx, cudaMemsetAsync((char *)ga.y + esz * (size_t)(d - 1) * N, 0, esz * N, ctx->stream));
     DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ga.sbar, 0, esz * N, ctx->stream));
   }
@@ -168,6 +169,7 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   DBGZ_TRY(dbgz_ensure(ctx, p->partials, sizeof(double) * n_tiles));
   DBGZ_TRY(dbgz_ensure(ctx, p->reps, sizeof(double) * n_reps));
   DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(p->reps.p, 0, sizeof(double) * n_reps, ctx->stream));
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
   const bool prof = ctx->profiling;
   const int64_t launches0 = ctx->launch_count;
   if (prof) cudaEventRecord(ctx->ev[0], ctx->stream);
@@ -194,6 +196,11 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
     return dbgz_loop_simt(p, pa, precision, tiles, t1);
   };
   const bool want_U = dP_dU || dP_dSigma;
+  DevBuf du_work;  // split partial tiles of the FP32 dU GEMM (back to the pool at the end, stream-ordered)
+  struct Release {
+    DevBuf &b;
+    ~Release() { dbgz_release(b); }
+  } release_du{du_work};
   for (int64_t t0 = 0; t0 < n_tiles; t0 += chunk) {
     const int64_t t1 = std::min(n_tiles, t0 + chunk);
     // forward keeping the state, then the adjoint on the anti-transposed factor
@@ -209,24 +216,21 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
     // dU[l, t] += sum_n y[l][n] (p sbar)[t][n] over the chunk's samples:
     // (d x Nc) x (Nc x d), sample-contiguous rows of leading dimension N
     if (want_U) {
-      // one GEMM over the full d x d (cuBLAS TF32 on this shape is faster than
-      // the block upper triangle alone: measured 10 ms against 23 ms)
-      cublasHandle_t h;
-      DBGZ_TRY(dbgz_get_cublas(ctx, &h));
-      cublasStatus_t cs;
       const int nc = (int)((t1 - t0) * 128);
       if (precision == DBGZ_PREC_FP64) {
+        cublasHandle_t h;
+        DBGZ_TRY(dbgz_get_cublas(ctx, &h));
         const double one = 1.0, beta = t0 > 0 ? 1.0 : 0.0;
-        cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, nc, &one, (const double *)ga.y, (int)N,
-                         (const double *)ga.sbar, (int)N, &beta, (double *)dU, (int)d);
+        const cublasStatus_t cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, nc, &one,
+                                              (const double *)ga.y, (int)N, (const double *)ga.sbar, (int)N, &beta,
+                                              (double *)dU, (int)d);
+        if (cs != CUBLAS_STATUS_SUCCESS)
+          return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
       } else {
-        const float one = 1.0f, beta = t0 > 0 ? 1.0f : 0.0f;
-        cs = cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, nc, &one, ga.y, CUDA_R_32F, (int)N, ga.sbar,
-                          CUDA_R_32F, (int)N, &beta, dU, CUDA_R_32F, (int)d, CUBLAS_COMPUTE_32F_FAST_TF32,
-                          CUBLAS_GEMM_DEFAULT);
+        // the strict upper triangle only, on tcgen05 (du_gemm.cu)
+        DBGZ_TRY(dbgz_du_gemm_tf32(ctx, d, (const float *)ga.y, (const float *)ga.sbar, nc, (float *)dU, t0 > 0,
+                                   du_work));
       }
-      if (cs != CUBLAS_STATUS_SUCCESS)
-        return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
     }
   }
   DBGZ_TRY(dbgz_finalize_pass(p, (const double *)p->partials.p, tps, 0, m, (double *)p->reps.p));
@@ -243,11 +247,12 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   if (dP_da) cudaMemcpyAsync(dP_da, da_o, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
   if (dP_db) cudaMemcpyAsync(dP_db, db_o, 8 * d, cudaMemcpyDeviceToHost, ctx->stream);
   if (dP_dU) cudaMemcpyAsync(dP_dU, dU64, 8 * (size_t)d * d, cudaMemcpyDeviceToHost, ctx->stream);
-  if (tensor) cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (tensor || (want_U && precision != DBGZ_PREC_FP64))
+    cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
   if (prof) cudaEventRecord(ctx->ev[1], ctx->stream);
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (dev_status != 0)
-    return dbgz_fail(ctx, DBGZ_ERR_TIMEOUT, "pnorm_grad: a bounded wait in the tensor-core loop gave up");
+    return dbgz_fail(ctx, DBGZ_ERR_TIMEOUT, "pnorm_grad: a bounded wait in a tensor-core kernel gave up");
   if (prof) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);

@@ -213,5 +213,11 @@ int dbgz_loop_sparse(dbgz_problem *p, const PassArgs &pa, int precision, double 
                      int64_t n_tiles);
 int dbgz_build_csc(dbgz_problem *p);
 void dbgz_drop_graphs(dbgz_problem *p);
+// dU[t*d + l] (+)= sum_n Y(l, n) S(t, n) over the nc samples, for l < t only,
+// Y and S tile-major ([tile][row < d][128 samples], the FP32 layout of
+// GradIO) (du_gemm.cu: tcgen05 TF32, split over samples, fixed-order sum of
+// the splits).  work: scratch taken from the context's pool.
+int dbgz_du_gemm_tf32(dbgz_ctx *ctx, int64_t d, const float *Y, const float *S, int64_t nc, float *dU,
+                      bool accumulate, DevBuf &work);
 int dbgz_finalize_pass(dbgz_problem *p, const double *partials, int64_t tiles_per_shift,
                        int64_t n_pts0, int64_t m, double *reps);

@@ -64,6 +64,7 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
     P.tgt = (const typename TgtOf<T>::type *)p->tgt32.p;
   }
   P.io.N = pa.grad.N;
+  P.io.rows = pa.d;
   P.io.y = (T *)pa.grad.y;
   P.io.s = (T *)pa.grad.s;
   P.io.dc = (T *)pa.grad.dc;

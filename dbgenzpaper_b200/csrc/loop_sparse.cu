@@ -227,6 +227,7 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.up1 = 1.0 - pa.c1 - pa.dc1;
   P.partials = partials;
   P.io.N = pa.grad.N;
+  P.io.rows = pa.d;
   P.io.y = (T *)pa.grad.y;
   P.io.s = (T *)pa.grad.s;
   P.io.dc = (T *)pa.grad.dc;

@@ -703,6 +703,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.ushift = (const uint64_t *)p->ushifts.p;
   P.U32 = (const float *)(adj ? p->Ub32.p : p->U32.p);
   P.io.N = pa.grad.N;
+  P.io.rows = pa.d;
   P.io.y = (float *)pa.grad.y;
   P.io.s = (float *)pa.grad.s;
   P.io.dc = (float *)pa.grad.dc;
