@@ -41,8 +41,8 @@ METRIC = "d=1000 MVN P time at |err|<=1e-5 vs FP64: mixed-prec vs FP64 GPU; grad
 UNIT = "ms"
 MIXED = "fp32_split_bf16"   # mixed-precision mode of the headline number
 # DRAM bytes of one 2^21-sample launch of the split-BF16 loop at d=1000 (ncu capture of a
-# 131,072-sample launch: 0.276 GB read + 0.349 GB written, scaled by the sample count)
-TRAFFIC_PER_LAUNCH = 16 * (276.29e6 + 349.16e6)
+# 131,072-sample launch: 0.239 GB read + 0.347 GB written, scaled by the sample count)
+TRAFFIC_PER_LAUNCH = 16 * (238.68e6 + 347.43e6)
 
 
 def _peaks():
