@@ -29,6 +29,7 @@
 // DBGZ_ERR_TIMEOUT in the status word and the CTA drains and leaves.
 #include <cuda.h>
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 #include <vector>
 
@@ -476,11 +477,14 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               uint32_t hi[4], lo[4];
               float ys[8];
               pl.chunk_begin(lbase + 8 * ch, nval - 8 * ch);
+              // full chunks (all but the last of a problem) run without the
+              // per-step bounds test: one uniform branch per chunk instead of 8
+              auto steps = [&](auto checked) {
 #pragma unroll
               for (int k = 0; k < 8; ++k) {
                 const int li = 8 * ch + k;
                 float y = 0.f;
-                if (li < nval) {
+                if (!decltype(checked)::value || li < nval) {
                   const int64_t l = lbase + li;
                   y = pl.emit_k(sgc, li, l, k);
                   const float4 *urow = reinterpret_cast<const float4 *>(&ublk[li][8 * ch]);
@@ -492,6 +496,9 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 }
                 ys[k] = y;
               }
+              };
+              if (nval - 8 * ch >= 8) steps(std::false_type{});
+              else steps(std::true_type{});
               pl.chunk_end(lbase + 8 * ch, nval - 8 * ch);
               switch (ch) {
                 case 0: rank8_update<24>(s, ys, &ublk[0][8]); break;
