@@ -190,6 +190,13 @@ struct Forward {
   __device__ __forceinline__ void tile_end(const typename TgtT<T>::type *, int, int, int64_t, bool) {}
 };
 
+// x rounded to the nearest TF32 value (low 13 mantissa bits zero)
+__device__ __forceinline__ float tf32_rn(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
 // ---------------------------------------------------------------- adjoint ---
 template <typename T, int GEN>
 struct Adjoint {
@@ -394,6 +401,17 @@ struct Adjoint {
     }
   }
 
+  // the factor-gradient GEMM's operand p * sbar_t (dense path); in FP32
+  // rounded to the nearest TF32 value: the TF32 tensor cores drop the low 13
+  // mantissa bits, which biases the products towards zero.  (The stored y's,
+  // the other operand, are still truncated by the tensor cores; rounding them
+  // too -- a write-back after the step has used y -- took the FP32
+  // dP/dSigma error vs FP64 from 8.3e-4 to 6.5e-4 at d = 1000 for 2.2 ms, and
+  // is not done.)
+  __device__ __forceinline__ void store_gemm(int64_t t, bool, T, double psb) const {
+    if (!io.sbar) return;
+    io.sbar[io.at(t, g)] = sizeof(T) == 4 ? (T)tf32_rn((float)psb) : (T)psb;
+  }
   __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc) {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
@@ -404,14 +422,14 @@ struct Adjoint {
       const bool fin = isfinite(sb) && isfinite(wrel * fa) && isfinite(wrel * fb) && isfinite(wrel * fu);
       if (__all_sync(0xffffffffu, fin)) {
         accumulate32(t, fa, fb, fu);
-        if (io.sbar) io.sbar[io.at(t, g)] = (T)(p * (double)sb);
+        store_gemm(t, has_u, y, p * (double)sb);
         return (T)sb;
       }
     }
     double ga, gb, gu;
     const double sb = variable(sg.tg[li], w, has_u, y, s, dc, true, ga, gb, gu);
     accumulate(t, ga, gb, gu);
-    if (io.sbar) io.sbar[io.at(t, g)] = (T)(p * sb);
+    store_gemm(t, has_u, y, p * sb);
     return (T)sb;
   }
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
@@ -452,7 +470,7 @@ struct Adjoint {
       acc_a[kk] = wa;
       acc_b[kk] = wb;
       acc_u[kk] = wu;
-      if (io.sbar) io.sbar[io.at(t, g)] = (T)(p * (double)sb);
+      store_gemm(t, has_u, pre_y[kk], p * (double)sb);
       return (T)sb;
     }
     // a term beyond FP32 range in the warp: this step in FP64, its sums
@@ -461,7 +479,7 @@ struct Adjoint {
     double ga, gb, gu;
     const double sbd = variable(sg.tg[li], w, has_u, pre_y[kk], pre_s[kk], pre_dc[kk], true, ga, gb, gu);
     accumulate(t, ga, gb, gu);
-    if (io.sbar) io.sbar[io.at(t, g)] = (T)(p * sbd);
+    store_gemm(t, has_u, pre_y[kk], p * sbd);
     return (T)sbd;
   }
   // sum of 8 values per lane over the 32 lanes of the warp, 8 sums at once:
