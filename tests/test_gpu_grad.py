@@ -96,9 +96,11 @@ def test_fp64_gradient_matches_finite_differences(dbgz, n, a_inf):
 
 @pytest.mark.parametrize("prec,tol", [(L.PREC_FP32_SIMT, 2e-3), (L.PREC_FP32_SPLIT_BF16, 2e-3),
                                       (L.PREC_FP32_TF32, 2e-2)])
-@pytest.mark.parametrize("n", [50, 300])
+@pytest.mark.parametrize("n", [50, 300, 700])
 def test_fp32_gradients_close_to_fp64(dbgz, prec, tol, n):
-    # n = 300 crosses the tensor loop's 256-wide phases in both directions
+    # n = 300 crosses the tensor loop's 256-wide phases in both directions;
+    # n = 700 gives the factor-gradient GEMM a 6 x 3 grid of 128 x 256 tiles
+    # with partial tiles at both edges
     D = dbgz
     Q = _problem(D, n, 2000 + n)
     P64, _, _, da64, db64, dU64 = D.qmc_pnorm_grad(Q, precision=L.PREC_FP64)
