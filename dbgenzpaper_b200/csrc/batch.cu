@@ -854,25 +854,35 @@ extern "C" int dbgz_batch_autotune(dbgz_ctx *ctx, int precision, int qmc_type, c
     std::vector<double> S, a, b;
     std::vector<uint64_t> sh;
     pilot_inputs(n, d, o.n_reps, qmc_type, S, a, b, sh);
-    double best_simt = 1e30, t = 0.0;
+    // a choice replaces the default only when it is at least kMargin faster
+    // on the pilot: the pilot stands in for the caller's problems, and a few
+    // percent are within the difference between the two
+    const double kMargin = 0.97;
+    double best_simt = 1e30, t_def = 1e30, t = 0.0;
     int64_t best_items = kDefaultItemDims;
     for (int64_t it : items) {
       ForcedChoice f;
       f.engine = 0;
       f.item_dims = it;
       if ((rc = pilot_time(ctx, n, d, o, qmc_type, precision, f, S, a, b, sh, 2, &t))) break;
+      if (it == kDefaultItemDims) t_def = t;
       if (t < best_simt) {
         best_simt = t;
         best_items = it;
       }
     }
     if (rc) break;
+    if (best_simt > kMargin * t_def) {
+      best_simt = t_def;
+      best_items = kDefaultItemDims;
+    }
     int engine = 0;
     if (tensor_precision(precision) && d - 1 <= 256) {
       ForcedChoice f;
       f.engine = 1;
       if ((rc = pilot_time(ctx, n, d, o, qmc_type, precision, f, S, a, b, sh, 2, &t))) break;
-      engine = t < best_simt ? 1 : 0;
+      const bool def_tensor = d >= kDefaultTensorMinD;
+      engine = def_tensor ? (best_simt < kMargin * t ? 0 : 1) : (t < kMargin * best_simt ? 1 : 0);
     }
     for (int64_t dd = lo[bk]; dd <= hi[bk]; ++dd) {
       T.engine[dd] = (int8_t)(engine && dd - 1 <= 256);
