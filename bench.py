@@ -175,7 +175,10 @@ def run_c4(args):
     ctx = D.get_context(0)
     lib = L.lib()
     t = time.perf_counter()
-    eng, items = D.batch_autotune(opts, L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
+    if args.no_autotune:
+        eng, items, _ = D.batch_tuning(L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
+    else:
+        eng, items = D.batch_autotune(opts, L.PREC_FP32_SPLIT_BF16, "Sobol", context=ctx)
     tune_s = time.perf_counter() - t
     tensor_from = int(np.argmax(eng[2:] == 1) + 2) if np.any(eng[2:] == 1) else None
     lib.dbgz_set_profiling(ctx.handle, 1)
@@ -222,7 +225,7 @@ def run_c4(args):
         "e2e": {"value": out["fp32_split_bf16"]["e2e_ms"], "unit": "ms",
                 "h2d_bytes_per_step": out["fp32_split_bf16"]["plan"]["host_bytes"],
                 "d2h_bytes_per_step": 8 * nR + 8 * len(ws) + 4 * (len(ws) + 2)},
-        "autotune": {"seconds": tune_s, "tensor_core_loop_from_d": tensor_from,
+        "autotune": {"seconds": tune_s, "tuned": not args.no_autotune, "tensor_core_loop_from_d": tensor_from,
                      "simt_item_dims_at_d16": int(items[16]), "simt_item_dims_at_d256": int(items[256])},
         "one_shot_e2e_ms_fp32_split_bf16": one_shot_ms,
         "one_shot_equals_plan": bool(np.array_equal(P1, Pt)),
@@ -438,6 +441,8 @@ def main():
     ap.add_argument("--only", action="store_true",
                     help="time only --precision (no FP64/other modes/accuracy/e2e/CPU legs); for profiling")
     ap.add_argument("--grad", action="store_true", help="with --only: time the gradient call instead")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="c4: keep the library's default engine table (no autotuning; for profiling)")
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c3: the headline line (default); c1: d = 10 with the CPU checker; c2: d = 500 "
                          "precision modes; c4: the 4096-problem batch; c5: the banded d = 10^4 problem "
