@@ -318,13 +318,34 @@ def _ar1(n, rho=0.9):
     return rho ** np.abs(i[:, None] - i[None, :])
 
 
+def _blocks(sizes, seed):
+    # block-diagonal SPD with irregular blocks: the classic factor keeps the
+    # blocks, so its CSC has columns of every length from 0 up (a general
+    # sparsity pattern, not a band)
+    rng = np.random.default_rng(seed)
+    n = sum(sizes)
+    S = np.zeros((n, n))
+    o = 0
+    for k in sizes:
+        A = rng.standard_normal((k, k + 3))
+        S[o:o + k, o:o + k] = W.correlation(A @ A.T)
+        o += k
+    return S
+
+
 @pytest.mark.parametrize("n,band,qmc", [(60, None, "Richtmyer"), (300, 16, "Richtmyer"),
-                                         (300, 64, "Sobol"), (600, None, "Richtmyer")])
+                                         (300, 64, "Sobol"), (600, None, "Richtmyer"),
+                                         (120, "blocks", "Sobol")])
 def test_pnorm_sparse_vs_checker(D, oracle, n, band, qmc):
     # classic factor, CSC of the strict upper triangle (optionally band-limited);
     # n = 600 without a band exceeds the shared-memory ring (global ring path)
-    S = _spd(n, n) if band is None else _ar1(n)
+    blocks = band == "blocks"
+    if blocks:
+        band = None
+    S = _blocks([5, 17, 1, 40, 9, 48], 7) if blocks else (_spd(n, n) if band is None else _ar1(n))
     rng = np.random.default_rng(n + 1)
+    if blocks:
+        assert np.count_nonzero(np.triu(S, 1)) < n * (n - 1) // 4
     a = np.full(n, -np.inf) if band else W.bounds_quarter(S)[0]
     b = rng.uniform(-0.5, 2.5, n) if band else W.bounds_quarter(S)[1]
     m, n_reps = 500, 3
@@ -340,6 +361,8 @@ def test_pnorm_sparse_vs_checker(D, oracle, n, band, qmc):
     U = F.U.copy()
     if band:
         assert np.all(np.triu(U, band + 1) == 0)
+    if blocks:
+        assert np.all(U[S == 0] == 0)  # the factor keeps the block pattern
     P, err, npts, reps = D.qmc_pnorm(Q, precision=L.PREC_FP64, return_reps=True)
     okw = dict(m=m, n_reps=n_reps, sparse=True, max_pts=m)
     if qmc == "Richtmyer":
