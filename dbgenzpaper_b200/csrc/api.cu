@@ -78,6 +78,13 @@ void dbgz_release(DevBuf &b) {
   b.owner = nullptr;
 }
 
+// Smallest index of a non-finite entry of x[0..n) into *first (which starts
+// at INT64_MAX); the prepare's check of Sigma on the device.
+__global__ void k_first_nonfinite(const double *x, int64_t n, unsigned long long *first) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(x[i])) atomicMin(first, (unsigned long long)i);
+}
+
 static int upload(dbgz_ctx *ctx, DevBuf &b, const void *src, size_t bytes) {
   DBGZ_TRY(dbgz_ensure(ctx, b, bytes));
   DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
@@ -322,9 +329,8 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
       return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "prepare: n_bits must be in 1..32");
     if (sobol_first < 0) return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "prepare: sobol_first < 0");
   }
-  for (int64_t i = 0; i < d * d; ++i)
-    if (std::isnan(Sigma[i]) || std::isinf(Sigma[i]))
-      return dbgz_fail(ctx, DBGZ_ERR_NONFINITE_INPUT, "prepare: Sigma has a non-finite entry at %lld", (long long)i);
+  // (Sigma itself is checked on the device after its upload: a host pass over
+  // the d^2 entries cost about 1 ms at d = 1000)
   for (int64_t i = 0; i < d; ++i) {
     if (std::isnan(a[i]) || std::isnan(b[i]))
       return dbgz_fail(ctx, DBGZ_ERR_NONFINITE_INPUT, "prepare: NaN bound at %lld", (long long)i);
@@ -350,8 +356,28 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
   const size_t nn = (size_t)d * d;
   const int64_t launches0 = ctx->launch_count;
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], ctx->stream);
+  DevBuf chk;  // first non-finite index of Sigma (UINT64_MAX: none)
   do {
     if ((rc = upload(ctx, p->U, Sigma, nn * 8))) break;
+    if ((rc = dbgz_ensure(ctx, chk, 8))) break;
+    if (cudaMemsetAsync(chk.p, 0xff, 8, ctx->stream) != cudaSuccess) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "prepare: memset failed");
+      break;
+    }
+    k_first_nonfinite<<<(unsigned)std::min<int64_t>(((int64_t)nn + 255) / 256, 2048), 256, 0, ctx->stream>>>(
+        (const double *)p->U.p, (int64_t)nn, (unsigned long long *)chk.p);
+    dbgz_count_launch(ctx);
+    // the factorisation runs on whatever Sigma holds (its loops are bounded);
+    // a non-finite entry is reported before its rank
+    auto sigma_ok = [&]() -> int {
+      unsigned long long first = ~0ull;
+      if (cudaMemcpy(&first, chk.p, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return dbgz_fail(ctx, DBGZ_ERR_CUDA, "prepare: %s", cudaGetErrorString(cudaGetLastError()));
+      if (first != ~0ull)
+        return dbgz_fail(ctx, DBGZ_ERR_NONFINITE_INPUT, "prepare: Sigma has a non-finite entry at %lld",
+                         (long long)first);
+      return DBGZ_OK;
+    };
     if ((rc = upload(ctx, p->a, a, d * 8))) break;
     if ((rc = upload(ctx, p->b, b, d * 8))) break;
     if ((rc = dbgz_ensure(ctx, p->perm, d * 8))) break;
@@ -361,6 +387,7 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
                               o.chol_block_size, o.chol_block_size2, 1024, 2048,
                               (int64_t *)p->perm.p, (double *)p->scale.p, &p->rank);
       if (rc) break;
+      if ((rc = sigma_ok())) break;
       if (p->rank != d) {
         rc = dbgz_fail(ctx, DBGZ_ERR_RANK_DEFICIENT, "QMCData requires a full-rank Cholesky factorization. (rank %lld of %lld)",
                        (long long)p->rank, (long long)d);
@@ -371,6 +398,7 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
                                  o.chol_block_size, o.chol_block_size2, 1024, 2048,
                                  (double *)p->scale.p);
       if (rc) break;
+      if ((rc = sigma_ok())) break;
       p->rank = d;
       std::vector<int64_t> id(d);
       for (int64_t i = 0; i < d; ++i) id[i] = i;
@@ -406,6 +434,7 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
       break;
     }
   } while (0);
+  dbgz_release(chk);
   if (rc != DBGZ_OK) {
     dbgz_problem_free(p);
     return rc;

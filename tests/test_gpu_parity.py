@@ -240,6 +240,11 @@ def test_error_statuses(D):
     with pytest.raises(D.DbgzError) as e:
         D.QMCData(S, lo, up, opts)
     assert e.value.status == L.ERR_NONFINITE_INPUT
+    S = np.eye(n)
+    S[4, 4] = np.inf  # checked on the device, classic factor too
+    with pytest.raises(D.DbgzError) as e:
+        D.QMCDataSparse(S, lo, up, opts)
+    assert e.value.status == L.ERR_NONFINITE_INPUT and "at 28" in str(e.value)
     with pytest.raises(D.DbgzError) as e:
         D.QMCData(np.eye(n), up, lo, opts)
     assert e.value.status == L.ERR_NONFINITE_INPUT
