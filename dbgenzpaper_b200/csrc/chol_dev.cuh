@@ -261,6 +261,33 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
     }
     __syncthreads();
     const int64_t im = sh_im;
+    // the y_i step (:533-546) by the block's last thread, which has no element
+    // of the swap below when n < blockDim: its arithmetic overlaps the swap,
+    // its write of the diagonal waits for it (same operations as in order)
+    const bool yt = tid == (int)blockDim.x - 1;
+    double y_mii = 0.0;
+    int y_stop = 0;
+    if (yt) {
+      double m_ii = sh_mii;
+      double d_ii = sh_yi;
+      if (m_ii > eps0) {
+        m_ii = dm_sqrt(m_ii);
+      } else {
+        rank[0] = i;  // 0-based i == reference's i - 1
+        y_stop = 1;
+      }
+      if (!y_stop) {
+        const int64_t qi = i - i0;
+        double a_norm = dm_div(dm_sub(s_a[qi], s_s[qi]), m_ii);
+        double b_norm = dm_div(dm_sub(s_b[qi], s_s[qi]), m_ii);
+        double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
+        double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
+        sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), d_ii);
+        sh_mii = m_ii;
+      }
+      sh_stop = y_stop;
+      y_mii = m_ii;
+    }
     if (im != i) {
       // :525-530, rows i <-> im over columns i0..n-1, then columns i <-> im,
       // in one pass: for k outside {i, im} the two swaps touch four distinct
@@ -288,28 +315,7 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
       }
       __syncthreads();
     }
-    if (tid == 0) {
-      double m_ii = sh_mii;
-      double d_ii = sh_yi;
-      int stop = 0;
-      if (m_ii > eps0) {
-        m_ii = dm_sqrt(m_ii);
-      } else {
-        rank[0] = i;  // 0-based i == reference's i - 1
-        stop = 1;
-      }
-      if (!stop) {
-        const int64_t qi = i - i0;
-        M[i * n + i] = m_ii;
-        double a_norm = dm_div(dm_sub(s_a[qi], s_s[qi]), m_ii);
-        double b_norm = dm_div(dm_sub(s_b[qi], s_s[qi]), m_ii);
-        double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
-        double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
-        sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), d_ii);
-        sh_mii = m_ii;
-      }
-      sh_stop = stop;
-    }
+    if (yt && !y_stop) M[i * n + i] = y_mii;
     __syncthreads();
     if (sh_stop) {
       write_back();
