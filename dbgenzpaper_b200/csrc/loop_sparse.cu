@@ -9,11 +9,14 @@
 //
 // Work decomposition: one thread per sample, 128 samples per CTA, several
 // CTAs per SM (no tensor cores: the dot has at most `bandwidth` terms).  The
-// y history a sample needs is the last W values (W = the factor's
-// bandwidth rounded up to a power of two); it lives in a shared-memory ring
-// buffer [W][128] when W fits (W <= 256 in FP32, 128 in FP64) and otherwise
-// in a per-CTA slot of global memory.  The CSC entries of 32 columns are
-// staged in shared memory per block of 32 dimensions.
+// y history a sample needs is the last W = bandwidth + 1 values; it lives in
+// a shared-memory ring buffer [W][128] when W fits (W <= 257 in FP32, 129 in
+// FP64) and otherwise in a per-CTA slot of global memory.  W is not rounded
+// to a power of two (at bandwidth 64 that halves the ring and doubles the
+// CTAs per SM): the CSC entries of 32 columns are staged in shared memory per
+// block of 32 dimensions with their ring slot (row mod W) in place of the row.
+// In FP32 the dot runs as 4 interleaved partial sums (the FP64 loop keeps
+// the reference's single ascending chain, so that it matches bit for bit).
 #include "internal.cuh"
 #include "genz_step.cuh"
 #include "policies.cuh"
@@ -47,7 +50,7 @@ struct SparseParams {
   double c1, dc1, up1;
   double *partials;
   T *yglob;                // global ring slots (gridDim.x x W x TS) when W is large
-  int W;                   // ring size (power of two)
+  int W;                   // ring size (bandwidth + 1)
   int ring_in_smem;
   int max_block_nnz;       // staging capacity (entries)
   int64_t tile0;           // tiles [tile0, n_tiles) of the pass
@@ -68,7 +71,7 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   __shared__ pol::Staged<T> sg;
   __shared__ double red[TS / 32];
   const int r = threadIdx.x;
-  const int Wm = P.W - 1;
+  const int W = P.W;
   T *yr = P.ring_in_smem ? ring : P.yglob + (int64_t)blockIdx.x * P.W * TS;
 
   for (int64_t tile = P.tile0 + blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
@@ -76,6 +79,7 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
     const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
     Policy pl;
     pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
+    int wslot = 0;  // ring slot of y-index i (i mod W)
     for (int64_t i0 = 0; i0 < P.nY; i0 += CB) {
       const int nb = (int)(P.nY - i0 < CB ? P.nY - i0 : CB);
       // stage the CSC columns i0+1 .. i0+nb (targets of y-indices i0..i0+nb-1)
@@ -85,7 +89,7 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
       const bool staged = cnt <= P.max_block_nnz;
       if (staged)
         for (int e = r; e < cnt; e += TS) {
-          srow[e] = P.rowval[p0 + e];
+          srow[e] = P.rowval[p0 + e] % W;  // the row's ring slot
           sval[e] = P.nzval[p0 + e];
         }
       if (r <= nb) scol[r] = (int)(P.colptr[i0 + 1 + r] - p0);
@@ -95,14 +99,30 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
       for (int li = 0; li < nb; ++li) {
         const int64_t i = i0 + li;
         const T y = pl.emit(sg, li, i);
-        yr[(i & Wm) * TS + r] = y;
+        yr[wslot * TS + r] = y;
+        wslot = wslot + 1 == W ? 0 : wslot + 1;
         T s = T(0);
         const int q0 = scol[li], q1 = scol[li + 1];
         if (staged) {
-          for (int q = q0; q < q1; ++q) s = fma(yr[(srow[q] & Wm) * TS + r], sval[q], s);
+          if (sizeof(T) == 4) {
+            // 4 independent partial sums: the chain of up to `bandwidth`
+            // dependent FMAs becomes 4 chains a quarter as long
+            T s1 = T(0), s2 = T(0), s3 = T(0);
+            int q = q0;
+            for (; q + 4 <= q1; q += 4) {
+              s = fma(yr[srow[q] * TS + r], sval[q], s);
+              s1 = fma(yr[srow[q + 1] * TS + r], sval[q + 1], s1);
+              s2 = fma(yr[srow[q + 2] * TS + r], sval[q + 2], s2);
+              s3 = fma(yr[srow[q + 3] * TS + r], sval[q + 3], s3);
+            }
+            for (; q < q1; ++q) s = fma(yr[srow[q] * TS + r], sval[q], s);
+            s = (s + s1) + (s2 + s3);
+          } else {
+            for (int q = q0; q < q1; ++q) s = fma(yr[srow[q] * TS + r], sval[q], s);
+          }
         } else {
           for (int q = q0; q < q1; ++q)
-            s = fma(yr[(P.rowval[p0 + q] & Wm) * TS + r], P.nzval[p0 + q], s);
+            s = fma(yr[(P.rowval[p0 + q] % W) * TS + r], P.nzval[p0 + q], s);
         }
         pl.consume(sg, s, li, i);
       }
@@ -239,10 +259,9 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.io.dc1 = pa.grad.dc1;
   P.io.tile0 = pa.tile0;
   const int64_t bwid = adj ? p->bandwidth_b : p->bandwidth;
-  int W = 1;
-  while (W < bwid + 1) W <<= 1;
+  const int W = (int)std::min<int64_t>(bwid + 1, INT32_MAX / 2);
   P.W = W;
-  const int ring_cap = sizeof(T) == 8 ? 128 : 256;
+  const int ring_cap = sizeof(T) == 8 ? 129 : 257;
   P.ring_in_smem = W <= ring_cap;
   P.max_block_nnz = (int)std::min<int64_t>(CB * std::min<int64_t>(bwid, 256), 8192);
   const size_t stage = ((sizeof(int32_t) * P.max_block_nnz + 15) & ~size_t(15)) +
