@@ -39,6 +39,14 @@ struct TgtT<float> {
   using type = TargetParams32;
 };
 
+// A staged CSC entry: the offset of its row's ring slot (slot * 128) and its
+// value, read together by one shared-memory load.
+template <typename T>
+struct __align__(sizeof(T) == 4 ? 8 : 16) SlotVal {
+  int off;
+  T val;
+};
+
 template <typename T>
 struct SparseParams {
   int64_t d, nY, m, n_reps, tiles_per_shift, n_tiles;
@@ -62,11 +70,17 @@ struct SparseParams {
 template <typename T, typename Policy>
 __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  // layout: [staged rowval int32 x cap][staged nzval T x cap][colptr of block (CB+1)][ring]
-  int32_t *srow = reinterpret_cast<int32_t *>(smem_raw);
+  // layout: [staged entries x cap][colptr of block (CB+1)][ring].  The staged
+  // entries are (slot offset, value) pairs, read by one load each, or -- in
+  // the FP32 forward pass without stored state -- two arrays of offsets and
+  // values (measured at C5: pairs 947 ms, arrays 863 ms for that pass; pairs
+  // faster for the FP64 pass, 1552 against 1588 ms, and the FP32 gradient,
+  // 1744 against 2002 ms)
+  constexpr bool kPairs = sizeof(T) == 8 || !Policy::kPlain;
+  SlotVal<T> *sent = reinterpret_cast<SlotVal<T> *>(smem_raw);
+  int32_t *soff = reinterpret_cast<int32_t *>(smem_raw);
   T *sval = reinterpret_cast<T *>(smem_raw + ((sizeof(int32_t) * P.max_block_nnz + 15) & ~size_t(15)));
-  int *scol = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sval) +
-                                      ((sizeof(T) * P.max_block_nnz + 15) & ~size_t(15)));
+  int *scol = reinterpret_cast<int *>(smem_raw + ((sizeof(SlotVal<T>) * P.max_block_nnz + 15) & ~size_t(15)));
   T *ring = reinterpret_cast<T *>(scol + CB + 4);
   __shared__ pol::Staged<T> sg;
   __shared__ double red[TS / 32];
@@ -89,8 +103,14 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
       const bool staged = cnt <= P.max_block_nnz;
       if (staged)
         for (int e = r; e < cnt; e += TS) {
-          srow[e] = P.rowval[p0 + e] % W;  // the row's ring slot
-          sval[e] = P.nzval[p0 + e];
+          const int off = (P.rowval[p0 + e] % W) * TS;  // the row's ring slot
+          if (kPairs) {
+            sent[e].off = off;
+            sent[e].val = P.nzval[p0 + e];
+          } else {
+            soff[e] = off;
+            sval[e] = P.nzval[p0 + e];
+          }
         }
       if (r <= nb) scol[r] = (int)(P.colptr[i0 + 1 + r] - p0);
       pl.stage(sg, P.tgt, r, i0, nb);
@@ -109,16 +129,28 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
             // dependent FMAs becomes 4 chains a quarter as long
             T s1 = T(0), s2 = T(0), s3 = T(0);
             int q = q0;
-            for (; q + 4 <= q1; q += 4) {
-              s = fma(yr[srow[q] * TS + r], sval[q], s);
-              s1 = fma(yr[srow[q + 1] * TS + r], sval[q + 1], s1);
-              s2 = fma(yr[srow[q + 2] * TS + r], sval[q + 2], s2);
-              s3 = fma(yr[srow[q + 3] * TS + r], sval[q + 3], s3);
+            const T *yrr = yr + r;
+            if (kPairs) {
+              for (; q + 4 <= q1; q += 4) {
+                const SlotVal<T> e0 = sent[q], e1 = sent[q + 1], e2 = sent[q + 2], e3 = sent[q + 3];
+                s = fma(yrr[e0.off], e0.val, s);
+                s1 = fma(yrr[e1.off], e1.val, s1);
+                s2 = fma(yrr[e2.off], e2.val, s2);
+                s3 = fma(yrr[e3.off], e3.val, s3);
+              }
+              for (; q < q1; ++q) s = fma(yrr[sent[q].off], sent[q].val, s);
+            } else {
+              for (; q + 4 <= q1; q += 4) {
+                s = fma(yrr[soff[q]], sval[q], s);
+                s1 = fma(yrr[soff[q + 1]], sval[q + 1], s1);
+                s2 = fma(yrr[soff[q + 2]], sval[q + 2], s2);
+                s3 = fma(yrr[soff[q + 3]], sval[q + 3], s3);
+              }
+              for (; q < q1; ++q) s = fma(yrr[soff[q]], sval[q], s);
             }
-            for (; q < q1; ++q) s = fma(yr[srow[q] * TS + r], sval[q], s);
             s = (s + s1) + (s2 + s3);
           } else {
-            for (int q = q0; q < q1; ++q) s = fma(yr[srow[q] * TS + r], sval[q], s);
+            for (int q = q0; q < q1; ++q) s = fma(yr[sent[q].off + r], sent[q].val, s);
           }
         } else {
           for (int q = q0; q < q1; ++q)
@@ -264,8 +296,7 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   const int ring_cap = sizeof(T) == 8 ? 129 : 257;
   P.ring_in_smem = W <= ring_cap;
   P.max_block_nnz = (int)std::min<int64_t>(CB * std::min<int64_t>(bwid, 256), 8192);
-  const size_t stage = ((sizeof(int32_t) * P.max_block_nnz + 15) & ~size_t(15)) +
-                       ((sizeof(T) * P.max_block_nnz + 15) & ~size_t(15)) + sizeof(int) * (CB + 4);
+  const size_t stage = ((sizeof(SlotVal<T>) * P.max_block_nnz + 15) & ~size_t(15)) + sizeof(int) * (CB + 4);
   const size_t smem = stage + (P.ring_in_smem ? sizeof(T) * (size_t)W * TS : 0) + 64;
   auto kern = k_genz_sparse<T, Policy>;
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -122,6 +122,7 @@ struct StepOf<float> {
 // ---------------------------------------------------------------- forward ---
 template <typename T, int GEN, bool STORE, typename Step = typename StepOf<T>::type>
 struct Forward {
+  static constexpr bool kPlain = !STORE;  // a forward pass that keeps no state
   Step st;
   dbgz::GenParams gen;
   int64_t j, k, g;  // point index in the pass, shift, global sample index
@@ -200,6 +201,7 @@ __device__ __forceinline__ float tf32_rn(float x) {
 // ---------------------------------------------------------------- adjoint ---
 template <typename T, int GEN>
 struct Adjoint {
+  static constexpr bool kPlain = false;
   dbgz::GenParams gen;
   int64_t j, k, g, d, tile;
   GradIO<T> io;
