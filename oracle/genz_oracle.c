@@ -127,6 +127,12 @@ static double max_abs_diag(int64_t n, const double *M) {
 void orc_cholesky_genz(int64_t n, double *M, double *a, double *b,
                        int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
                        int64_t *perm, double *scale_vec, int64_t *rank_out) {
+  orc_cholesky_genz_margins(n, M, a, b, bs1, bs2, bs3, bs4, perm, scale_vec, rank_out, NULL);
+}
+
+void orc_cholesky_genz_margins(int64_t n, double *M, double *a, double *b,
+                               int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
+                               int64_t *perm, double *scale_vec, int64_t *rank_out, double *margins) {
   const double c2 = 1.0 / sqrt(2.0);
   const double is2pi = 2.0 / sqrt(2.0 * M_PI);
   const double eps0 = DBL_EPSILON * max_abs_diag(n, M);
@@ -165,6 +171,16 @@ void orc_cholesky_genz(int64_t n, double *M, double *a, double *b,
             for (int64_t k = i + 1; k <= ii1; ++k) {
               double v = O1(k);
               if (julia_min_less(v, best)) { best = v; i_m = k; }
+            }
+            if (margins) {
+              /* diagnostics, not part of the reference: the gap between the
+               * winning score and the best other candidate (+inf when alone);
+               * a gap near rounding size marks a pivot that a different
+               * summation order could flip */
+              double second = INFINITY;
+              for (int64_t k = i; k <= ii1; ++k)
+                if (k != i_m && O1(k) < second) second = O1(k);
+              margins[i - 1] = second - best;
             }
             double d_ii = O1(i_m);
             double m_ii = M1(i_m, i_m) - D1(i_m);

@@ -53,6 +53,12 @@ double orc_erfinv(double x);
 void orc_cholesky_genz(int64_t n, double *M, double *a, double *b,
                        int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
                        int64_t *perm, double *scale_vec, int64_t *rank);
+/* the same, and (when margins is not NULL) for every pivot step i the gap
+ * between the winning score and the best other candidate of the panel
+ * (diagnostics of near-ties; +inf where the panel has one candidate) */
+void orc_cholesky_genz_margins(int64_t n, double *M, double *a, double *b,
+                               int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
+                               int64_t *perm, double *scale_vec, int64_t *rank, double *margins);
 /* src/cholesky.jl:144-242 */
 void orc_cholesky_classic(int64_t n, double *M, double *a, double *b,
                           int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,

@@ -77,6 +77,7 @@ def lib():
         L.orc_erfinv.restype = d
         L.orc_erfinv.argtypes = [d]
         L.orc_cholesky_genz.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pi64, pd, pi64]
+        L.orc_cholesky_genz_margins.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pi64, pd, pi64, pd]
         L.orc_cholesky_classic.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pd]
         L.orc_truncate_U.argtypes = [i64, pd, d]
         L.orc_sqrt_primes.argtypes = [i64, pd]
@@ -103,8 +104,10 @@ def erfinv(x: float) -> float:
     return lib().orc_erfinv(float(x))
 
 
-def cholesky_genz(Sigma, a, b, bs1=64, bs2=512, bs3=1024, bs4=2048):
-    """cholesky_genz!(copy(Σ), copy(a), copy(b), bs1, bs2) -> dict (src/cholesky.jl:445)."""
+def cholesky_genz(Sigma, a, b, bs1=64, bs2=512, bs3=1024, bs4=2048, margins=False):
+    """cholesky_genz!(copy(Σ), copy(a), copy(b), bs1, bs2) -> dict (src/cholesky.jl:445).
+    With margins=True the dict also holds, per pivot step, the gap between the
+    winning score and the best other candidate (a diagnostic of near-ties)."""
     n = Sigma.shape[0]
     M = np.array(Sigma, dtype=np.float64, order="F", copy=True)
     a = np.array(a, dtype=np.float64, copy=True)
@@ -112,9 +115,14 @@ def cholesky_genz(Sigma, a, b, bs1=64, bs2=512, bs3=1024, bs4=2048):
     perm = np.zeros(n, dtype=np.int64)
     scale = np.zeros(n, dtype=np.float64)
     rank = C.c_int64(0)
-    lib().orc_cholesky_genz(n, _pd(M), _pd(a), _pd(b), bs1, bs2, bs3, bs4,
-                            perm.ctypes.data_as(C.POINTER(C.c_int64)), _pd(scale), C.byref(rank))
-    return dict(U=M, perm=perm, rank=rank.value, a=a, b=b, scale_vec=scale)
+    mg = np.full(n, np.nan) if margins else None
+    lib().orc_cholesky_genz_margins(n, _pd(M), _pd(a), _pd(b), bs1, bs2, bs3, bs4,
+                                    perm.ctypes.data_as(C.POINTER(C.c_int64)), _pd(scale), C.byref(rank),
+                                    _pd(mg) if margins else None)
+    out = dict(U=M, perm=perm, rank=rank.value, a=a, b=b, scale_vec=scale)
+    if margins:
+        out["margins"] = mg
+    return out
 
 
 def cholesky_classic(Sigma, a, b, bs1=128, bs2=512, bs3=1024, bs4=2048):

@@ -71,6 +71,23 @@ def test_cholesky_genz_ties_pick_first_index(D, oracle):
     assert np.array_equal(G.perm, F["perm"]) and np.array_equal(G.U, F["U"])
 
 
+def test_cholesky_genz_near_ties(D, oracle):
+    # random covariances with the reference's symmetric bound design: the
+    # checker's pivot log shows a step whose two best scores tie exactly (and
+    # others within 1e-9), where any other rounding could flip the pivot; the
+    # GPU factorisation (the same deterministic FP64 arithmetic) still agrees
+    # bit for bit
+    near = 0
+    for seed in range(4):
+        S = _spd(120, 50 + seed)
+        lo, up = W.bounds_quarter(S)
+        F = oracle.cholesky_genz(S, lo, up, 32, 64, margins=True)
+        G = D.cholesky_genz(S, lo, up, 32, 64)
+        near += int(np.sum(F["margins"] < 1e-12))
+        assert np.array_equal(G.perm, F["perm"]) and np.array_equal(G.U, F["U"])
+    assert near > 0  # the case is exercised
+
+
 def test_cholesky_genz_rank_deficient(D, oracle):
     rng = np.random.default_rng(9)
     B = rng.standard_normal((20, 5))

@@ -209,3 +209,21 @@ def test_continuation_matches_longer_run(oracle):
     _, _, _, r1 = oracle.qmc_pnorm(U, F["a"], F["b"], m=300, n_reps=4, shifts=sh)
     _, _, _, rb = oracle.qmc_pnorm(U, F["a"], F["b"], m=300, n_reps=4, shifts=sh, gen_base0=300)
     assert np.allclose(r2, 0.5 * (r1 + rb), rtol=1e-14, atol=0)
+
+
+def test_pivot_margins_log(oracle):
+    # ties (equicorrelated, equal bounds) log a zero margin and keep the
+    # lowest index; the log changes nothing in the factorisation
+    n = 8
+    S = 0.5 * np.ones((n, n)) + 0.5 * np.eye(n)
+    F = oracle.cholesky_genz(S, -np.ones(n), np.ones(n), margins=True)
+    assert np.array_equal(F["perm"], np.arange(n))
+    assert np.all(F["margins"][:-1] == 0.0) and np.isinf(F["margins"][-1])
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((30, 40))
+    S = A @ A.T
+    lo, up = -rng.uniform(0.5, 2, 30), rng.uniform(0.5, 2, 30)
+    F1 = oracle.cholesky_genz(S, lo, up, margins=True)
+    F2 = oracle.cholesky_genz(S, lo, up)
+    assert np.array_equal(F1["U"], F2["U"]) and np.array_equal(F1["perm"], F2["perm"])
+    assert np.all(F1["margins"][np.isfinite(F1["margins"])] >= 0.0)
