@@ -48,6 +48,13 @@ struct GenParams {
   const uint32_t *V;     // Sobol direction numbers (d-1) x 32
   const uint64_t *ushift;// (d-1) x n_reps
   const int64_t *gen_base_dev;  // when set, gen_base is read from here (device-driven passes)
+  // Sobol, nonzero when every tile starts at a multiple of 128 (the pass's
+  // first index sobol_first + gen_base is one): the integer of index
+  // base + r (r < 128) is x(base) ^ XOR_{k<7} [bit k of gray(r)] V[k], since
+  // gray(base + r) = gray(base) ^ gray(r) and the integer is linear in the
+  // Gray code's bits.  Loops that stage x(base) and V[0..6] per block pass the
+  // integer in (the tensor-core loop); zero: sobol_warp per step
+  int sobol_tile128;
 };
 
 // Gray-code Sobol integer of point index idx in dimension l, computed by
@@ -99,7 +106,7 @@ struct StepFp64 {
   // Returns y_l for QMC dimension l of sample (point index j in the pass,
   // 0-based; shift k).
   __device__ __forceinline__ double quantile(const GenParams &g, int64_t d, int64_t j, int64_t k,
-                                             int64_t l, double qv, double shiftv) const {
+                                             int64_t l, double qv, double shiftv, uint32_t x0) const {
     double u;
     if (g.qmc_type == 0) {
       double x = __dmul_rn((double)(g.gen_base + j + 1), qv);
@@ -109,7 +116,8 @@ struct StepFp64 {
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
-      uint64_t xi = (uint64_t)sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
+      const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
+      uint64_t xi = (uint64_t)xw & mask;
       uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
       u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
     }
@@ -156,7 +164,7 @@ struct StepFp32 {
     p = dc1;
   }
   __device__ __forceinline__ float quantile(const GenParams &g, int64_t d, int64_t j, int64_t k,
-                                            int64_t l, double qv, float shiftv) const {
+                                            int64_t l, double qv, float shiftv, uint32_t x0) const {
     float w, w1;
     if (g.qmc_type == 0) {
       double x = __dmul_rn((double)(g.gen_base + j + 1), qv);
@@ -168,7 +176,8 @@ struct StepFp32 {
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
-      uint64_t xi = (uint64_t)sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j)) & mask;
+      const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
+      uint64_t xi = (uint64_t)xw & mask;
       uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
       double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
       w = (float)fabs(fma(u, 2.0, -1.0));

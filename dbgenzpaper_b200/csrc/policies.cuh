@@ -123,6 +123,7 @@ struct StepOf<float> {
 template <typename T, int GEN, bool STORE, typename Step = typename StepOf<T>::type>
 struct Forward {
   static constexpr bool kPlain = !STORE;  // a forward pass that keeps no state
+  static constexpr bool kSobolTable = true;  // takes staged Sobol integers (GenParams::sobol_tile128)
   Step st;
   dbgz::GenParams gen;
   int64_t j, k, g;  // point index in the pass, shift, global sample index
@@ -166,15 +167,19 @@ struct Forward {
                           gen.shift32 != nullptr);
     }
   }
-  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l) {
-    const T y = st.quantile(gen, d, j, k, l, sg.qv[li], sg.shv[li]);
+  // xs: the Sobol integer of this point in dimension l when the loop stages
+  // them (GenParams::sobol_tile128), else unused
+  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
+    const T y = st.quantile(gen, d, j, k, l, sg.qv[li], sg.shv[li], xs);
     if (STORE) io.y[io.at(l, g)] = y;
     return y;
   }
   // chunked form (8 steps whose per-sample inputs may be loaded up front)
   __device__ __forceinline__ void chunk_begin(int64_t, int) {}
   __device__ __forceinline__ void chunk_end(int64_t, int) {}
-  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int) { return emit(sg, li, l); }
+  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int, uint32_t xs) {
+    return emit(sg, li, l, xs);
+  }
   __device__ __forceinline__ void consume(const Staged<T> &sg, T s, int li, int64_t l) {
     const auto tg = sg.tg[li];
     st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
@@ -202,6 +207,7 @@ __device__ __forceinline__ float tf32_rn(float x) {
 template <typename T, int GEN>
 struct Adjoint {
   static constexpr bool kPlain = false;
+  static constexpr bool kSobolTable = false;
   dbgz::GenParams gen;
   int64_t j, k, g, d, tile;
   GradIO<T> io;
@@ -470,7 +476,7 @@ struct Adjoint {
       }
     }
   }
-  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk) {
+  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk, uint32_t) {
     if (sizeof(T) != 4) return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk]);
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;

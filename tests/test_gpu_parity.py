@@ -313,6 +313,38 @@ def test_pnorm_tensor_core_phases(D, n, m, n_reps, prec):
 
 
 @pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
+@pytest.mark.parametrize("n,m,first", [(200, 1024, 2048), (600, 1024, 128 * 37), (300, 1000, 2048),
+                                       (300, 1024, 2048 + 37)])
+def test_pnorm_tensor_core_sobol_points(D, n, m, first, prec):
+    # Sobol points in the tensor-core loop: from the per-block tables when a
+    # pass starts at a multiple of 128 (first and m aligned), per step
+    # otherwise (the third case switches after its first pass); three passes
+    # against the FP64 loop and the FP32 SIMT loop on the same points.  Other
+    # points would move P by about the QMC error, which the test requires to
+    # be far above its tolerance.
+    S = _spd(n, n + 11)
+    lo, up = W.bounds_quarter(S)
+    R = 3
+    us = np.random.default_rng(n + m).integers(0, 2**64, size=(n - 1, R), dtype=np.uint64)
+    opts = D.QMC_opts(m=m, n_reps=R, max_pts=3 * m, max_abs_err=0.0)
+    out = {}
+    for pr in (L.PREC_FP64, L.PREC_FP32_SIMT, prec):
+        Q = D.QMCData(S, lo, up, opts, qmc_type="Sobol", ushifts=us, sobol_first=first)
+        try:
+            out[pr] = D.qmc_pnorm(Q, precision=pr, return_reps=True)
+        finally:
+            Q.close()
+    P64, e64, n64, r64 = out[L.PREC_FP64]
+    Ps, Pt, rt_ = out[L.PREC_FP32_SIMT][0], out[prec][0], out[prec][3]
+    # same points: both precisions stay within 1e-6 here (d <= 600)
+    tol = 5e-6 + 4e-5 * abs(P64)
+    assert out[prec][2] == n64 == 3 * m
+    assert e64 > 5 * tol, (e64, tol)
+    assert abs(Pt - P64) <= tol and abs(Pt - Ps) <= tol, (Pt, Ps, P64)
+    np.testing.assert_allclose(rt_, r64, rtol=0, atol=3 * tol)
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
 def test_identity_known_answer_tensor_core(D, prec):
     n = 40
     lo, up = W.bounds_quarter(np.eye(n))
