@@ -53,7 +53,8 @@ struct GenParams {
   // base + r (r < 128) is x(base) ^ XOR_{k<7} [bit k of gray(r)] V[k], since
   // gray(base + r) = gray(base) ^ gray(r) and the integer is linear in the
   // Gray code's bits.  Loops that stage x(base) and V[0..6] per block pass the
-  // integer in (the tensor-core loop); zero: sobol_warp per step
+  // integer in, already XORed with the shift's low 32 bits (n_bits <= 32:
+  // the shift enters only there); zero: sobol_warp and the shift per step
   int sobol_tile128;
 };
 
@@ -118,7 +119,7 @@ struct StepFp64 {
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
       const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
       uint64_t xi = (uint64_t)xw & mask;
-      uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
+      uint64_t sh = g.sobol_tile128 ? 0ull : g.ushift[k * (d - 1) + l] & mask;
       u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
     }
     u = fabs(fma(u, 2.0, -1.0));
@@ -178,7 +179,7 @@ struct StepFp32 {
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
       const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
       uint64_t xi = (uint64_t)xw & mask;
-      uint64_t sh = g.ushift[k * (d - 1) + l] & mask;
+      uint64_t sh = g.sobol_tile128 ? 0ull : g.ushift[k * (d - 1) + l] & mask;
       double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
       w = (float)fabs(fma(u, 2.0, -1.0));
       w1 = (float)(2.0 * fmin(u, 1.0 - u));

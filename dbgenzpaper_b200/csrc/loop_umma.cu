@@ -129,11 +129,11 @@ struct Misc {
   float ublk[2][BK][kUld];
   pol::Staged<float> sg[2];
   // Sobol integers of the block's dimensions (GenParams::sobol_tile128), per
-  // dimension li: [w] = x(tile base + 32 w) for warp w < 4, [4 + a] = the
-  // XOR of V[0], V[1] selected by the bits of a, [8 + b] = that of V[2..4]
-  // by the bits of b.  Lane i of warp w (gray(i) = a + 4 b) takes
-  // x = [w] ^ [4 + a] ^ [8 + b]: gray(base + 32 w + i) = gray(base + 32 w) ^
-  // gray(i) for a 32-aligned base.
+  // dimension li: [w] = x(tile base + 32 w) ^ the tile's shift for warp
+  // w < 4, [4 + a] = the XOR of V[0], V[1] selected by the bits of a,
+  // [8 + b] = that of V[2..4] by the bits of b.  Lane i of warp w
+  // (gray(i) = a + 4 b) takes x = [w] ^ [4 + a] ^ [8 + b]:
+  // gray(base + 32 w + i) = gray(base + 32 w) ^ gray(i) for a 32-aligned base.
   uint32_t sob[2][BK][16];
   double red[4];
   uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
@@ -445,11 +445,13 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               uint32_t v[7];
 #pragma unroll
               for (int e = 0; e < 7; ++e) v[e] = __shfl_sync(0xffffffffu, vk, e);
+              // the sample's random shift (low 32 bits; shift k of the tile)
+              const uint32_t ush = (ln < 4 && li < nv) ? (uint32_t)__ldg(pl.gen.ushift + pl.k * (dI - 1) + lb + li) : 0u;
               // lanes 0..3: gray(32 w) = 32 w ^ 16 w, bits 4..6 of it
               const uint32_t sel = ln < 4 ? (uint32_t)((ln << 1) ^ ln) : (uint32_t)(ln < 8 ? ln - 4 : ln - 8);
               uint32_t x;
               if (ln < 4)
-                x = t ^ ((sel & 1u) ? v[4] : 0u) ^ ((sel & 2u) ? v[5] : 0u) ^ ((sel & 4u) ? v[6] : 0u);
+                x = t ^ ((sel & 1u) ? v[4] : 0u) ^ ((sel & 2u) ? v[5] : 0u) ^ ((sel & 4u) ? v[6] : 0u) ^ ush;
               else if (ln < 8)
                 x = ((sel & 1u) ? v[0] : 0u) ^ ((sel & 2u) ? v[1] : 0u);
               else
