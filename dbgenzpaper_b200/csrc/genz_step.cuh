@@ -83,6 +83,65 @@ __device__ __forceinline__ uint32_t sobol_warp(const uint32_t *Vl, uint64_t idx)
   return x ^ t;
 }
 
+// Staged Sobol integers for 128-sample tiles that start at a multiple of 128
+// (GenParams::sobol_tile128).  Since gray(B + i) = gray(B) ^ gray(i) when B is
+// a multiple of 2^k and i < 2^k, and the integer is linear in the Gray code's
+// bits, the integer of index base + 32 w + i (warp w of the tile, lane i) is
+//   x(base + 32 w) ^ x(gray(i) & 3) ^ x(gray(i) & 28),
+// with gray(32 w) = 32 w ^ 16 w bringing V[4..6] into the first term.  Per
+// dimension li of a block, tab[li][0..15] holds: [w] = x(base + 32 w) ^ the
+// tile's shift (low 32 bits: n_bits <= 32, so the shift enters only there),
+// [4 + a] = V[0], V[1] XORed by the bits of a, [8 + b] = V[2..4] by the bits of
+// b.  A step then reads three words (sobol_staged).
+//
+// sobol_stage_block: the 128 threads r of a tile together (all lanes of
+// their four warps), warp w filling dimensions 8w..8w+7 of a block of 32:
+// dimensions lb..lb+nv-1, tile base index base0, shift row ush (the shift of
+// dimension l at ush[l]).
+__device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[16], const uint32_t *V, const uint64_t *ush,
+                                                  uint64_t base0, int64_t lb, int nv, int r) {
+  const uint32_t gw = (uint32_t)(base0 ^ (base0 >> 1));
+  const int wid = r >> 5, ln = r & 31;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int li = wid * 8 + q;
+    // x(base): lane k contributes V[k] when bit k of gray(base) is set
+    const uint32_t vk = li < nv ? __ldg(V + (lb + li) * 32 + ln) : 0u;
+    uint32_t t = ((gw >> ln) & 1u) ? vk : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t ^= __shfl_xor_sync(0xffffffffu, t, o);
+    uint32_t v[7];
+#pragma unroll
+    for (int e = 0; e < 7; ++e) v[e] = __shfl_sync(0xffffffffu, vk, e);
+    const uint32_t sh = (ln < 4 && li < nv) ? (uint32_t)__ldg(ush + lb + li) : 0u;
+    // lanes 0..3: bits 4..6 of gray(32 w) = 32 w ^ 16 w
+    const uint32_t sel = ln < 4 ? (uint32_t)((ln << 1) ^ ln) : (uint32_t)(ln < 8 ? ln - 4 : ln - 8);
+    uint32_t x;
+    if (ln < 4)
+      x = t ^ ((sel & 1u) ? v[4] : 0u) ^ ((sel & 2u) ? v[5] : 0u) ^ ((sel & 4u) ? v[6] : 0u) ^ sh;
+    else if (ln < 8)
+      x = ((sel & 1u) ? v[0] : 0u) ^ ((sel & 2u) ? v[1] : 0u);
+    else
+      x = ((sel & 1u) ? v[2] : 0u) ^ ((sel & 2u) ? v[3] : 0u) ^ ((sel & 4u) ? v[4] : 0u);
+    if (ln < 16) tab[li][ln] = x;
+  }
+}
+
+// The shifted integer of tile row r in block dimension li (sobol_stage_block).
+struct SobolLane {
+  uint32_t w, a, b;  // warp, gray(lane) & 3, gray(lane) >> 2
+  __device__ __forceinline__ explicit SobolLane(int r) {
+    const uint32_t g = (uint32_t)((r & 31) ^ ((r & 31) >> 1));
+    w = (uint32_t)(r >> 5);
+    a = g & 3u;
+    b = g >> 2;
+  }
+  __device__ __forceinline__ uint32_t at(const uint32_t (*tab)[16], int li) const {
+    const uint32_t *t = tab[li];
+    return t[w] ^ t[4 + a] ^ t[8 + b];
+  }
+};
+
 // The same integer by one thread alone (loop over the set bits).
 __device__ __forceinline__ uint32_t sobol_int(const uint32_t *Vl, uint64_t idx) {
   uint32_t g = (uint32_t)(idx ^ (idx >> 1));

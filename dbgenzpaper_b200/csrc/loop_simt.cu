@@ -45,6 +45,9 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.gen_base = pa.gen_base;
   P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
+  // staged Sobol integers when every tile starts at a multiple of 128
+  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && pa.kind != kLoopAdjoint &&
+                        (pa.sobol_first + pa.gen_base) % 128 == 0 && (!pa.gen_base_dev || pa.m % 128 == 0);
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
   P.gen.shift32 = (const float *)p->shifts32.p;

@@ -51,6 +51,7 @@ struct SimtSmem {
   } u;
   T Ublk[SB][SB + 1];         // coefficients of the sub-block (and of the cross block)
   pol::Staged<T> sg;
+  uint32_t sob[SB][16];       // Sobol integers of the sub-block (dbgz::sobol_stage_block)
   double red[NT / 32];
 };
 
@@ -68,6 +69,7 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
     const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
     Policy pl;
     if (tid < TS) pl.tile_begin(P.gen, d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, P.cdf_form, P.io);
+    const dbgz::SobolLane sob_lane(r);
 
     for (int64_t g0 = 0; g0 < nY; g0 += G) {
       const int ng = (int)(nY - g0 < (int64_t)G ? nY - g0 : (int64_t)G);
@@ -123,7 +125,13 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
           int64_t l = l_base + li, t = l_base + ti + 1;
           sm.Ublk[li][ti] = (li <= ti && li < nsb && ti < nsb) ? P.U[t * d + l] : T(0);
         }
-        if (tid < TS) pl.stage(sm.sg, P.tgt, tid, l_base, nsb);
+        if (tid < TS) {
+          pl.stage(sm.sg, P.tgt, tid, l_base, nsb);
+          if constexpr (Policy::kSobolTable)
+            if (P.gen.sobol_tile128)
+              dbgz::sobol_stage_block(sm.sob, P.gen.V, P.gen.ushift + k * (d - 1),
+                                      (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)), l_base, nsb, r);
+        }
         __syncthreads();
         if (tid < TS) {
           // in-block dot in the reference's order (src/qmc.jl:394-403):
@@ -131,7 +139,10 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
 #pragma unroll 1
           for (int li = 0; li < nsb; ++li) {
             const int64_t l = l_base + li;
-            T v = pl.emit(sm.sg, li, l);
+            uint32_t xs = 0u;
+            if constexpr (Policy::kSobolTable)
+              if (P.gen.sobol_tile128) xs = sob_lane.at(sm.sob, li);
+            T v = pl.emit(sm.sg, li, l, xs);
             sm.u.Ysub[li][r] = v;
             if (g0 < last_g0) Yw[l * TS + r] = v;
             T acc = sm.Ss[sb + li][r];

@@ -83,8 +83,10 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   int *scol = reinterpret_cast<int *>(smem_raw + ((sizeof(SlotVal<T>) * P.max_block_nnz + 15) & ~size_t(15)));
   T *ring = reinterpret_cast<T *>(scol + CB + 4);
   __shared__ pol::Staged<T> sg;
+  __shared__ uint32_t sob[Policy::kSobolTable ? CB : 1][16];  // Sobol integers of the block (dbgz::sobol_stage_block)
   __shared__ double red[TS / 32];
   const int r = threadIdx.x;
+  const dbgz::SobolLane sob_lane(r);
   const int W = P.W;
   T *yr = P.ring_in_smem ? ring : P.yglob + (int64_t)blockIdx.x * P.W * TS;
 
@@ -114,11 +116,18 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
         }
       if (r <= nb) scol[r] = (int)(P.colptr[i0 + 1 + r] - p0);
       pl.stage(sg, P.tgt, r, i0, nb);
+      if constexpr (Policy::kSobolTable)
+        if (P.gen.sobol_tile128)
+          dbgz::sobol_stage_block(sob, P.gen.V, P.gen.ushift + k * (P.d - 1),
+                                  (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)), i0, nb, r);
       __syncthreads();
 #pragma unroll 1
       for (int li = 0; li < nb; ++li) {
         const int64_t i = i0 + li;
-        const T y = pl.emit(sg, li, i);
+        uint32_t xs = 0u;
+        if constexpr (Policy::kSobolTable)
+          if (P.gen.sobol_tile128) xs = sob_lane.at(sob, li);
+        const T y = pl.emit(sg, li, i, xs);
         yr[wslot * TS + r] = y;
         wslot = wslot + 1 == W ? 0 : wslot + 1;
         T s = T(0);
@@ -264,6 +273,9 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.gen.gen_base = pa.gen_base;
   P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
+  // staged Sobol integers when every tile starts at a multiple of 128
+  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && !adj && (pa.sobol_first + pa.gen_base) % 128 == 0 &&
+                        (!pa.gen_base_dev || pa.m % 128 == 0);
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
   P.gen.shift32 = (const float *)p->shifts32.p;

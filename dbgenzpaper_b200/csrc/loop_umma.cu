@@ -128,19 +128,20 @@ struct Misc {
   // block's per-dimension constants; two buffers: the next block stages while this one runs
   float ublk[2][BK][kUld];
   pol::Staged<float> sg[2];
-  // Sobol integers of the block's dimensions (GenParams::sobol_tile128), per
-  // dimension li: [w] = x(tile base + 32 w) ^ the tile's shift for warp
-  // w < 4, [4 + a] = the XOR of V[0], V[1] selected by the bits of a,
-  // [8 + b] = that of V[2..4] by the bits of b.  Lane i of warp w
-  // (gray(i) = a + 4 b) takes x = [w] ^ [4 + a] ^ [8 + b]:
-  // gray(base + 32 w + i) = gray(base + 32 w) ^ gray(i) for a 32-aligned base.
-  uint32_t sob[2][BK][16];
   double red[4];
   uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
   uint32_t tmem_base;
   int abort;
+  // Sobol integers of the block's dimensions (dbgz::sobol_stage_block); last,
+  // so that kernels that do not stage them are launched without it
+  uint32_t sob[2][BK][16];
 };
 static_assert(sizeof(Misc) <= Smem<DBGZ_PREC_FP32_TF32>::MISC, "shared scalars exceed their budget");
+// dynamic shared memory of a launch: the Sobol staging only where it is used
+template <int MODE>
+int umma_smem_bytes(int P, bool sobol_staged) {
+  return Smem<MODE>::total(P) - (sobol_staged ? 0 : (int)sizeof(Misc::sob));
+}
 
 __device__ __forceinline__ void set_abort(Misc *ms, int *status) {
   ms->abort = 1;
@@ -399,9 +400,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
     uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
     const bool need_ws = !BATCH && nphase1 > 1;
     uint32_t blk = 0;  // blocks run by this CTA (selects the staging buffer)
-    // this lane's Gray code gray(i) = sob_a + 4 sob_b (staged Sobol integers)
-    const uint32_t sob_g = (uint32_t)((r & 31) ^ ((r & 31) >> 1));
-    const uint32_t sob_a = sob_g & 3u, sob_b = sob_g >> 2, sob_w = (uint32_t)(r >> 5);
+    const dbgz::SobolLane sob_lane(r);  // this row's terms of the staged Sobol integers
     for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles; it += gridDim.x) {
       const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
       const int64_t tile = BATCH ? (int64_t)P.item_tile[it] : it;
@@ -427,39 +426,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           pol::cp_async_or_zero<4>(&ms->ublk[buf][li][ti], v ? U32I + (lb + ti + 1) * dI + lb + li : U32I, v);
         }
         pl.stage_async(ms->sg[buf], tgtI, r, lb, nv);
-        if constexpr (Policy::kSobolTable) {
-          if (pl.gen.sobol_tile128) {
-            // warp w fills dimensions 8w..8w+7: x(base) as the XOR over the
-            // lanes of the Gray-code terms (lane k: V[k] if bit k of
-            // gray(base) is set), then lanes 0..15 one entry each
-            const uint64_t base0 = (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r));
-            const uint32_t gw = (uint32_t)(base0 ^ (base0 >> 1));
-            const int wid = r >> 5, ln = r & 31;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int li = wid * 8 + q;
-              const uint32_t vk = li < nv ? __ldg(pl.gen.V + (lb + li) * 32 + ln) : 0u;
-              uint32_t t = ((gw >> ln) & 1u) ? vk : 0u;
-#pragma unroll
-              for (int o = 16; o > 0; o >>= 1) t ^= __shfl_xor_sync(0xffffffffu, t, o);
-              uint32_t v[7];
-#pragma unroll
-              for (int e = 0; e < 7; ++e) v[e] = __shfl_sync(0xffffffffu, vk, e);
-              // the sample's random shift (low 32 bits; shift k of the tile)
-              const uint32_t ush = (ln < 4 && li < nv) ? (uint32_t)__ldg(pl.gen.ushift + pl.k * (dI - 1) + lb + li) : 0u;
-              // lanes 0..3: gray(32 w) = 32 w ^ 16 w, bits 4..6 of it
-              const uint32_t sel = ln < 4 ? (uint32_t)((ln << 1) ^ ln) : (uint32_t)(ln < 8 ? ln - 4 : ln - 8);
-              uint32_t x;
-              if (ln < 4)
-                x = t ^ ((sel & 1u) ? v[4] : 0u) ^ ((sel & 2u) ? v[5] : 0u) ^ ((sel & 4u) ? v[6] : 0u) ^ ush;
-              else if (ln < 8)
-                x = ((sel & 1u) ? v[0] : 0u) ^ ((sel & 2u) ? v[1] : 0u);
-              else
-                x = ((sel & 1u) ? v[2] : 0u) ^ ((sel & 2u) ? v[3] : 0u) ^ ((sel & 4u) ? v[4] : 0u);
-              if (ln < 16) ms->sob[buf][li][ln] = x;
-            }
-          }
-        }
+        if constexpr (Policy::kSobolTable)
+          if (pl.gen.sobol_tile128)
+            dbgz::sobol_stage_block(ms->sob[buf], pl.gen.V, pl.gen.ushift + pl.k * (dI - 1),
+                                    (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)), lb, nv, r);
         pol::cp_async_commit();
       };
       for (int64_t ph = 0; ph < nphase; ++ph) {
@@ -532,12 +502,8 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 if (!decltype(checked)::value || li < nval) {
                   const int64_t l = lbase + li;
                   uint32_t xs = 0u;
-                  if constexpr (Policy::kSobolTable) {
-                    if (pl.gen.sobol_tile128) {
-                      const uint32_t *sb = ms->sob[cur][li];
-                      xs = sb[sob_w] ^ sb[4 + sob_a] ^ sb[8 + sob_b];
-                    }
-                  }
+                  if constexpr (Policy::kSobolTable)
+                    if (pl.gen.sobol_tile128) xs = sob_lane.at(ms->sob[cur], li);
                   y = pl.emit_k(sgc, li, l, k, xs);
                   const float4 *urow = reinterpret_cast<const float4 *>(&ublk[li][8 * ch]);
                   const float4 u0 = urow[0], u1 = urow[1];
@@ -718,7 +684,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   }
   if (!p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
   const int Pw = 256;
-  const int smem = SM::total(Pw);
+  const int smem = umma_smem_bytes<MODE>(Pw, pa.qmc_type == DBGZ_QMC_SOBOL && !adj);
   auto kern = pick_kernel<MODE>(pa);
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
@@ -922,7 +888,7 @@ int setup_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A, UmmaBatchPlan *B) {
   DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_itile, itl.data(), 4 * n_items, cudaMemcpyHostToDevice, st));
   DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   // kernel configuration (attributes set here, outside any stream capture)
-  const int smem = SM::total(Pw);
+  const int smem = umma_smem_bytes<MODE>(Pw, A.qmc_type == DBGZ_QMC_SOBOL);
   auto kern = A.qmc_type == DBGZ_QMC_SOBOL ? batch_kernel<MODE, DBGZ_QMC_SOBOL>()
                                            : batch_kernel<MODE, DBGZ_QMC_RICHTMYER>();
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));

@@ -344,6 +344,37 @@ def test_pnorm_tensor_core_sobol_points(D, n, m, first, prec):
     np.testing.assert_allclose(rt_, r64, rtol=0, atol=3 * tol)
 
 
+@pytest.mark.parametrize("sparse", [False, True])
+@pytest.mark.parametrize("m,first", [(1000, 2048), (1024, 128 * 19), (1000, 2085)])
+def test_sobol_staged_points_fp64_vs_checker(D, oracle, sparse, m, first):
+    # the FP64 loops (dense SIMT, banded) against the checker on Sobol points:
+    # staged per-block integers when a pass starts at a multiple of 128 (the
+    # first pass of the first case, with a partial last tile, and every pass
+    # of the second), per step otherwise
+    n, R = 160, 3
+    S = _spd(n, 5 + m)
+    lo, up = W.bounds_quarter(S)
+    us = np.random.default_rng(m + first).integers(0, 2**64, size=(n - 1, R), dtype=np.uint64)
+    opts = D.QMC_opts(m=m, n_reps=R, max_pts=2 * m, max_abs_err=0.0)
+    cls = D.QMCDataSparse if sparse else D.QMCData
+    Q = cls(S, lo, up, opts, qmc_type="Sobol", ushifts=us, sobol_first=first)
+    Q32 = cls(S, lo, up, opts, qmc_type="Sobol", ushifts=us, sobol_first=first)  # the same points again
+    try:
+        P, err, npts, reps = D.qmc_pnorm(Q, precision=L.PREC_FP64, return_reps=True)
+        F = Q.C
+        Pc, ec, nc, rc = oracle.qmc_pnorm(F.U, F.a, F.b, m=m, n_reps=R, max_pts=2 * m, max_abs_err=0.0,
+                                          sparse=sparse, qmc_type=oracle.SOBOL, V=D.sobol_dirnums(n - 1),
+                                          ushifts=us, sobol_first=Q.sobol_first)
+        P32, _, _, r32 = D.qmc_pnorm(Q32, precision=L.PREC_FP32_SIMT, return_reps=True)
+    finally:
+        Q.close()
+        Q32.close()
+    assert npts == nc == 2 * m
+    np.testing.assert_allclose(reps, rc, rtol=1e-12, atol=1e-300)
+    assert ec > 5 * (5e-6 + 4e-5 * abs(Pc))  # other points would be seen below
+    np.testing.assert_allclose(r32, rc, rtol=0, atol=5e-6 + 4e-5 * abs(Pc))
+
+
 @pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
 def test_identity_known_answer_tensor_core(D, prec):
     n = 40
