@@ -28,24 +28,28 @@ def _problems(dims, seed):
 DIMS = [2, 3, 16, 17, 64, 65, 100, 129, 256, 300, 5, 33]
 
 
-@pytest.mark.parametrize("qmc", ["Richtmyer", "Sobol"])
+# "Sobol2048": Sobol from index 2048, a multiple of 128 (the loops' staged
+# integers) with a partial last tile (m = 1000); "Sobol": from 2m = 2000
+@pytest.mark.parametrize("qmc", ["Richtmyer", "Sobol", "Sobol2048"])
 @pytest.mark.parametrize("prec,rtol", [(L.PREC_FP64, 1e-13), (L.PREC_FP32_SIMT, 1e-6)])
 def test_batch_matches_one_problem_path(dbgz, qmc, prec, rtol):
     D = dbgz
     probs = _problems(DIMS, 11)
     opts = D.QMC_opts(m=1000, n_reps=6, max_pts=1000, max_abs_err=0.0)
     rng = np.random.default_rng(5)
+    first = 2048 if qmc == "Sobol2048" else None
+    qmc = qmc[:5] if first else qmc
     if qmc == "Richtmyer":
         sh = [rng.random((d - 1, 6)) for d in DIMS]
         P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, shifts=sh, precision=prec)
     else:
         ush = [rng.integers(0, 2**63, size=(d - 1, 6), dtype=np.uint64) for d in DIMS]
-        P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, ushifts=ush, precision=prec)
+        P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, ushifts=ush, precision=prec, sobol_first=first)
     for k, (S, a, b) in enumerate(probs):
         if qmc == "Richtmyer":
             Q = D.QMCData(S, a, b, opts, qmc_type=qmc, shifts=sh[k])
         else:
-            Q = D.QMCData(S, a, b, opts, qmc_type=qmc, ushifts=ush[k])
+            Q = D.QMCData(S, a, b, opts, qmc_type=qmc, ushifts=ush[k], sobol_first=first)
         P1, e1, _ = D.qmc_pnorm(Q, precision=prec)
         Q.close()
         assert abs(P[k] - P1) <= rtol * abs(P1) + 1e-300, (k, DIMS[k], P[k], P1)
@@ -96,7 +100,7 @@ def test_batch_fp32_accuracy_many_uneven(dbgz):
     assert np.all(np.abs(P32 - P64) <= 2e-6 + 1e-5 * np.abs(P64))
 
 
-@pytest.mark.parametrize("qmc", ["Richtmyer", "Sobol"])
+@pytest.mark.parametrize("qmc", ["Richtmyer", "Sobol", "Sobol2048"])
 @pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
 def test_batch_tensor_core_matches_one_problem_path(dbgz, qmc, prec):
     # problems with d - 1 <= 256 run in the batched tensor-core loop, the rest
@@ -108,17 +112,19 @@ def test_batch_tensor_core_matches_one_problem_path(dbgz, qmc, prec):
     probs = _problems(dims, 17)
     opts = D.QMC_opts(m=1000, n_reps=6, max_pts=1000, max_abs_err=0.0)
     rng = np.random.default_rng(9)
+    first = 2048 if qmc == "Sobol2048" else None
+    qmc = qmc[:5] if first else qmc
     if qmc == "Richtmyer":
         sh = [rng.random((d - 1, 6)) for d in dims]
         P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, shifts=sh, precision=prec)
     else:
         ush = [rng.integers(0, 2**63, size=(d - 1, 6), dtype=np.uint64) for d in dims]
-        P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, ushifts=ush, precision=prec)
+        P, err = D.qmc_pnorm_batch(probs, opts, qmc_type=qmc, ushifts=ush, precision=prec, sobol_first=first)
     for k, (S, a, b) in enumerate(probs):
         if qmc == "Richtmyer":
             Q = D.QMCData(S, a, b, opts, qmc_type=qmc, shifts=sh[k])
         else:
-            Q = D.QMCData(S, a, b, opts, qmc_type=qmc, ushifts=ush[k])
+            Q = D.QMCData(S, a, b, opts, qmc_type=qmc, ushifts=ush[k], sobol_first=first)
         P1, e1, _ = D.qmc_pnorm(Q, precision=prec)
         P64, _, _ = D.qmc_pnorm(Q, precision=L.PREC_FP64)
         Q.close()
