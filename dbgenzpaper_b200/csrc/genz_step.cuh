@@ -142,6 +142,20 @@ struct SobolLane {
   }
 };
 
+// w = |2u - 1| and w1 = 2 min(u, 1 - u) of the Sobol point u = X 2^-L
+// (X < 2^L, 1 <= L <= 32), rounded to FP32.  Both are exact multiples of
+// 2^-(L-1) with integer parts |X - 2^(L-1)| and min(X, 2^L - X) <= 2^31, so
+// forming them on the integer and rounding once gives the same floats as
+// forming u in FP64 first (checked for every L on random and edge X).
+__device__ __forceinline__ void sobol_tent_f32(uint32_t X, int L, float &w, float &w1) {
+  const uint32_t half = 1u << (L - 1);
+  const uint32_t dd = X >= half ? X - half : half - X;
+  const uint32_t mm = X <= half ? X : (uint32_t)((1ull << L) - X);
+  const float sc = __int_as_float((127 - (L - 1)) << 23);  // 2^-(L-1)
+  w = __uint2float_rn(dd) * sc;
+  w1 = __uint2float_rn(mm) * sc;
+}
+
 // The same integer by one thread alone (loop over the set bits).
 __device__ __forceinline__ uint32_t sobol_int(const uint32_t *Vl, uint64_t idx) {
   uint32_t g = (uint32_t)(idx ^ (idx >> 1));
@@ -165,6 +179,7 @@ struct StepFp64 {
   }
   // Returns y_l for QMC dimension l of sample (point index j in the pass,
   // 0-based; shift k).
+  template <bool kIntTent = true>  // (no effect in FP64)
   __device__ __forceinline__ double quantile(const GenParams &g, int64_t d, int64_t j, int64_t k,
                                              int64_t l, double qv, double shiftv, uint32_t x0) const {
     double u;
@@ -223,6 +238,11 @@ struct StepFp32 {
     up = (float)up1;
     p = dc1;
   }
+  // kIntTent: the Sobol tent transform on the integer (sobol_tent_f32), else
+  // through an FP64 u -- the same floats; the pass that stores its state for
+  // the adjoint keeps the FP64 form (measured at C5 shapes, 2^14 points: its
+  // gradient call 125.1 ms against 146.4 ms with the integer form)
+  template <bool kIntTent = true>
   __device__ __forceinline__ float quantile(const GenParams &g, int64_t d, int64_t j, int64_t k,
                                             int64_t l, double qv, float shiftv, uint32_t x0) const {
     float w, w1;
@@ -233,13 +253,20 @@ struct StepFp32 {
       u = u > 1.0f ? u - 1.0f : u;
       w = fabsf(fmaf(u, 2.0f, -1.0f));
       w1 = 2.0f * fminf(u, 1.0f - u);  // 1 - |2u - 1|
+    } else if (kIntTent) {
+      // n_bits <= 32: the shifted integer has at most 32 bits
+      const int L = g.n_bits;
+      const uint32_t mask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+      const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
+      const uint32_t sh = g.sobol_tile128 ? 0u : (uint32_t)g.ushift[k * (d - 1) + l];
+      sobol_tent_f32((xw ^ sh) & mask, L, w, w1);
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
       const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
-      uint64_t xi = (uint64_t)xw & mask;
-      uint64_t sh = g.sobol_tile128 ? 0ull : g.ushift[k * (d - 1) + l] & mask;
-      double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
+      const uint64_t xi = (uint64_t)xw & mask;
+      const uint64_t sh = g.sobol_tile128 ? 0ull : g.ushift[k * (d - 1) + l] & mask;
+      const double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
       w = (float)fabs(fma(u, 2.0, -1.0));
       w1 = (float)(2.0 * fmin(u, 1.0 - u));
     }

@@ -174,7 +174,7 @@ struct Forward {
   // xs: the Sobol integer of this point in dimension l when the loop stages
   // them (GenParams::sobol_tile128), else unused
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
-    const T y = st.quantile(gen, d, j, k, l, sg.qv[li], sg.shv[li], xs);
+    const T y = st.template quantile<!STORE>(gen, d, j, k, l, sg.qv[li], sg.shv[li], xs);
     if (STORE) io.y[io.at(l, g)] = y;
     return y;
   }
