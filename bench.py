@@ -8,8 +8,9 @@ shifts; one step = one qmc_pnorm! pass over all samples.
 
   value      device time per step (CUDA events on the library's stream),
              problem resident in HBM, L2 flushed (256 MiB write) between steps
-  e2e        the same step through the C ABI from host buffers: upload of
-             Sigma/a/b/shifts, GPU factorisation, integration, read-back
+  e2e        the same step through the C ABI from host buffers (page-locked,
+             column-major): upload of Sigma/a/b/shifts, GPU factorisation,
+             integration, read-back
   roofline   the integration-loop kernel against the measured dense bf16
              tensor peak (contraction flops = samples * d (d - 1) per launch)
   cpu_baseline  the CPU checker (C restatement of the reference's Float64
@@ -480,9 +481,19 @@ def main():
     d = w.d
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
+    def pinned_f64(x):
+        # x as column-major FP64 in page-locked host memory: the layout of a
+        # column-major caller (the reference's), uploaded by DMA
+        x = np.asarray(x, dtype=np.float64)
+        h = torch.empty(x.shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T
+        h[...] = x
+        return h
+
+    Sig_h, a_h, b_h, sh_h = (pinned_f64(x) for x in (w.Sigma, w.a, w.b, w.shifts))
+
     def make(precision):
         opts = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0)
-        return D.QMCData(w.Sigma, w.a, w.b, opts, qmc_type="Richtmyer", shifts=w.shifts,
+        return D.QMCData(Sig_h, a_h, b_h, opts, qmc_type="Richtmyer", shifts=sh_h,
                          precision=precision, device=local)
 
     prof = L.DbgzProfile()
