@@ -109,6 +109,18 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def pinned_host(x, dtype=None):
+    """x as a column-major array in page-locked host memory: the layout of a
+    column-major (Julia) caller, taken by the API without a host copy and
+    uploaded by DMA."""
+    import torch
+    x = np.asarray(x, dtype=dtype)
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.uint64): torch.uint64}[x.dtype]
+    h = torch.empty(x.shape[::-1], dtype=tdt, pin_memory=True).numpy().T
+    h[...] = x
+    return h
+
+
 def workload(rank: int, world: int, quick: bool, d=None, points=None):
     from dbgenzpaper_b200 import workloads as W
     if quick:
@@ -260,8 +272,9 @@ def run_small(args):
     prof = L.DbgzProfile()
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device="cuda:0")
     opts = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0)
-    kw = dict(qmc_type=w.qmc_type, shifts=w.shifts) if w.qmc_type == "Richtmyer" else \
-        dict(qmc_type=w.qmc_type, ushifts=w.ushifts)
+    kw = dict(qmc_type=w.qmc_type, shifts=pinned_host(w.shifts, np.float64)) if w.qmc_type == "Richtmyer" else \
+        dict(qmc_type=w.qmc_type, ushifts=pinned_host(w.ushifts, np.uint64))
+    Sig_h, a_h, b_h = (pinned_host(x, np.float64) for x in (w.Sigma, w.a, w.b))
     modes = [("fp64", L.PREC_FP64)]
     if args.workload == "c2":
         modes += [("fp32_tf32", L.PREC_FP32_TF32), ("fp32_split_bf16", L.PREC_FP32_SPLIT_BF16),
@@ -282,7 +295,7 @@ def run_small(args):
         e2e = []
         for _ in range(args.steps):
             t = time.perf_counter()
-            Q2 = D.QMCData(w.Sigma, w.a, w.b, opts, precision=prec, **kw)
+            Q2 = D.QMCData(Sig_h, a_h, b_h, opts, precision=prec, **kw)
             P2, _, _ = D.qmc_pnorm(Q2, precision=prec)
             e2e.append(1e3 * (time.perf_counter() - t))
             Q2.close()
@@ -481,15 +494,7 @@ def main():
     d = w.d
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
-    def pinned_f64(x):
-        # x as column-major FP64 in page-locked host memory: the layout of a
-        # column-major caller (the reference's), uploaded by DMA
-        x = np.asarray(x, dtype=np.float64)
-        h = torch.empty(x.shape[::-1], dtype=torch.float64, pin_memory=True).numpy().T
-        h[...] = x
-        return h
-
-    Sig_h, a_h, b_h, sh_h = (pinned_f64(x) for x in (w.Sigma, w.a, w.b, w.shifts))
+    Sig_h, a_h, b_h, sh_h = (pinned_host(x, np.float64) for x in (w.Sigma, w.a, w.b, w.shifts))
 
     def make(precision):
         opts = D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0)
