@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   // layout: [staged entries x cap][colptr of block (CB+1)][ring].  The staged
   // entries are (slot offset, value) pairs, read by one load each, or -- in
   // the FP32 forward pass without stored state -- two arrays of offsets and
-  // values (measured at C5: pairs 947 ms, arrays 863 ms for that pass; pairs
+  // values (measured on the banded d = 10^4, bandwidth 64, 2^18 x 10 Sobol
+  // workload: pairs 947 ms, arrays 863 ms for that pass; pairs
   // faster for the FP64 pass, 1552 against 1588 ms, and the FP32 gradient,
   // 1744 against 2002 ms)
   constexpr bool kPairs = sizeof(T) == 8 || !Policy::kPlain;
