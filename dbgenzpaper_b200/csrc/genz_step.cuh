@@ -95,25 +95,28 @@ __device__ __forceinline__ uint32_t sobol_warp(const uint32_t *Vl, uint64_t idx)
 // b.  A step then reads three words (sobol_staged).
 //
 // sobol_stage_block: the 128 threads r of a tile together (all lanes of
-// their four warps), warp w filling dimensions 8w..8w+7 of a block of 32:
-// dimensions lb..lb+nv-1, tile base index base0, shift row ush (the shift of
-// dimension l at ush[l]).
+// their four warps), warp w filling entries 8w..8w+7 of a block of 32: entry
+// li < nv is dimension l0 + dir li when that lies in [0, lmax]; tile base
+// index base0, shift row ush (the shift of dimension l at ush[l]).
 __device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[16], const uint32_t *V, const uint64_t *ush,
-                                                  uint64_t base0, int64_t lb, int nv, int r) {
+                                                  uint64_t base0, int64_t l0, int dir, int64_t lmax, int nv,
+                                                  int r) {
   const uint32_t gw = (uint32_t)(base0 ^ (base0 >> 1));
   const int wid = r >> 5, ln = r & 31;
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     const int li = wid * 8 + q;
+    const int64_t l = l0 + dir * li;
+    const bool ok = li < nv && l >= 0 && l <= lmax;
     // x(base): lane k contributes V[k] when bit k of gray(base) is set
-    const uint32_t vk = li < nv ? __ldg(V + (lb + li) * 32 + ln) : 0u;
+    const uint32_t vk = ok ? __ldg(V + l * 32 + ln) : 0u;
     uint32_t t = ((gw >> ln) & 1u) ? vk : 0u;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t ^= __shfl_xor_sync(0xffffffffu, t, o);
     uint32_t v[7];
 #pragma unroll
     for (int e = 0; e < 7; ++e) v[e] = __shfl_sync(0xffffffffu, vk, e);
-    const uint32_t sh = (ln < 4 && li < nv) ? (uint32_t)__ldg(ush + lb + li) : 0u;
+    const uint32_t sh = (ln < 4 && ok) ? (uint32_t)__ldg(ush + l) : 0u;
     // lanes 0..3: bits 4..6 of gray(32 w) = 32 w ^ 16 w
     const uint32_t sel = ln < 4 ? (uint32_t)((ln << 1) ^ ln) : (uint32_t)(ln < 8 ? ln - 4 : ln - 8);
     uint32_t x;

@@ -128,9 +128,10 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
         if (tid < TS) {
           pl.stage(sm.sg, P.tgt, tid, l_base, nsb);
           if constexpr (Policy::kSobolTable)
-            if (P.gen.sobol_tile128)
+            if (pl.gen.sobol_tile128)
               dbgz::sobol_stage_block(sm.sob, P.gen.V, P.gen.ushift + k * (d - 1),
-                                      (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)), l_base, nsb, r);
+                                      (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)),
+                                      pl.sobol_l0(l_base), Policy::kSobolDir, d - 2, nsb, r);
         }
         __syncthreads();
         if (tid < TS) {
@@ -141,7 +142,7 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
             const int64_t l = l_base + li;
             uint32_t xs = 0u;
             if constexpr (Policy::kSobolTable)
-              if (P.gen.sobol_tile128) xs = sob_lane.at(sm.sob, li);
+              if (pl.gen.sobol_tile128) xs = sob_lane.at(sm.sob, li);
             T v = pl.emit(sm.sg, li, l, xs);
             sm.u.Ysub[li][r] = v;
             if (g0 < last_g0) Yw[l * TS + r] = v;

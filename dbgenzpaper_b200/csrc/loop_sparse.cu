@@ -118,16 +118,17 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
       if (r <= nb) scol[r] = (int)(P.colptr[i0 + 1 + r] - p0);
       pl.stage(sg, P.tgt, r, i0, nb);
       if constexpr (Policy::kSobolTable)
-        if (P.gen.sobol_tile128)
+        if (pl.gen.sobol_tile128)
           dbgz::sobol_stage_block(sob, P.gen.V, P.gen.ushift + k * (P.d - 1),
-                                  (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)), i0, nb, r);
+                                  (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)), pl.sobol_l0(i0),
+                                  Policy::kSobolDir, P.d - 2, nb, r);
       __syncthreads();
 #pragma unroll 1
       for (int li = 0; li < nb; ++li) {
         const int64_t i = i0 + li;
         uint32_t xs = 0u;
         if constexpr (Policy::kSobolTable)
-          if (P.gen.sobol_tile128) xs = sob_lane.at(sob, li);
+          if (pl.gen.sobol_tile128) xs = sob_lane.at(sob, li);
         const T y = pl.emit(sg, li, i, xs);
         yr[wslot * TS + r] = y;
         wslot = wslot + 1 == W ? 0 : wslot + 1;
@@ -275,7 +276,7 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
   // staged Sobol integers when every tile starts at a multiple of 128
-  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && !adj && (pa.sobol_first + pa.gen_base) % 128 == 0 &&
+  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && (pa.sobol_first + pa.gen_base) % 128 == 0 &&
                         (!pa.gen_base_dev || pa.m % 128 == 0);
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;

@@ -429,7 +429,8 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         if constexpr (Policy::kSobolTable)
           if (pl.gen.sobol_tile128)
             dbgz::sobol_stage_block(ms->sob[buf], pl.gen.V, pl.gen.ushift + pl.k * (dI - 1),
-                                    (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)), lb, nv, r);
+                                    (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)), pl.sobol_l0(lb),
+                                    Policy::kSobolDir, dI - 2, nv, r);
         pol::cp_async_commit();
       };
       for (int64_t ph = 0; ph < nphase; ++ph) {

@@ -128,6 +128,9 @@ struct Forward {
   // bandwidth 64 workload at 2^14 x 10 Sobol points:
   // the gradient call 125.1 ms without, 136.9 ms with them)
   static constexpr bool kSobolTable = GEN == DBGZ_QMC_SOBOL && !STORE;
+  // the QMC dimension of step li of a block: lbase + li
+  static constexpr int kSobolDir = 1;
+  __device__ __forceinline__ int64_t sobol_l0(int64_t lbase) const { return lbase; }
   Step st;
   dbgz::GenParams gen;
   int64_t j, k, g;  // point index in the pass, shift, global sample index
@@ -212,7 +215,11 @@ __device__ __forceinline__ float tf32_rn(float x) {
 template <typename T, int GEN>
 struct Adjoint {
   static constexpr bool kPlain = false;
-  static constexpr bool kSobolTable = false;
+  // takes staged Sobol integers (GenParams::sobol_tile128) where the loop
+  // stages them; the QMC dimension of step li of a block: d - 1 - lbase - li
+  static constexpr bool kSobolTable = GEN == DBGZ_QMC_SOBOL;
+  static constexpr int kSobolDir = -1;
+  __device__ __forceinline__ int64_t sobol_l0(int64_t lbase) const { return d - 1 - lbase; }
   dbgz::GenParams gen;
   int64_t j, k, g, d, tile;
   GradIO<T> io;
@@ -230,6 +237,7 @@ struct Adjoint {
                                              const GradIO<T> &io_) {
     gen = gp;
     gen.qmc_type = GEN;
+    if (!kSobolTable) gen.sobol_tile128 = 0;
     if (gp.gen_base_dev) gen.gen_base = *gp.gen_base_dev;
     d = d_;
     tile = tile_;
@@ -274,8 +282,11 @@ struct Adjoint {
     }
   }
 
-  // tent-transformed point w_t of y-index t (as StepFp*::quantile forms it)
-  __device__ __forceinline__ double point_w(const Staged<T> &sg, int li, int64_t t) const {
+  // tent-transformed point w_t of y-index t (as StepFp*::quantile forms it);
+  // Sobol: from the staged integer xs (already XORed with the shift) when
+  // `staged`, else generated here
+  __device__ __forceinline__ double point_w(const Staged<T> &sg, int li, int64_t t, uint32_t xs,
+                                            bool staged) const {
     double u;
     if (GEN == 0) {
       double x = __dmul_rn((double)(gen.gen_base + j + 1), sg.qv[li]);
@@ -291,8 +302,9 @@ struct Adjoint {
       const int L = gen.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
       const uint64_t xi =
-          (uint64_t)dbgz::sobol_warp(gen.V + t * 32, (uint64_t)(gen.sobol_first + gen.gen_base + j)) & mask;
-      const uint64_t sh = gen.ushift[k * (d - 1) + t] & mask;
+          (uint64_t)(staged ? xs : dbgz::sobol_warp(gen.V + t * 32, (uint64_t)(gen.sobol_first + gen.gen_base + j))) &
+          mask;
+      const uint64_t sh = staged ? 0ull : gen.ushift[k * (d - 1) + t] & mask;
       u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
     }
     return fabs(fma(u, 2.0, -1.0));
@@ -425,10 +437,10 @@ struct Adjoint {
     if (!io.sbar) return;
     io.sbar[io.at(t, g)] = sizeof(T) == 4 ? (T)tf32_rn((float)psb) : (T)psb;
   }
-  __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc) {
+  __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc, uint32_t xs) {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const double w = has_u ? point_w(sg, li, t) : 0.0;
+    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_tile128 != 0) : 0.0;
     if (sizeof(T) == 4) {
       float fa, fb, fu;
       const float sb = variable32(sg.tg[li], (float)w, has_u, (float)y, (float)s, (float)dc, true, fa, fb, fu);
@@ -445,10 +457,10 @@ struct Adjoint {
     store_gemm(t, has_u, y, p * sb);
     return (T)sb;
   }
-  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t = 0u) {
+  __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
     const int64_t t = d - 1 - l;
     const T y = t <= d - 2 ? io.y[io.at(t, g)] : T(0);
-    return emit_from(sg, li, l, y, io.s[io.at(t, g)], io.dc[io.at(t, g)]);
+    return emit_from(sg, li, l, y, io.s[io.at(t, g)], io.dc[io.at(t, g)], xs);
   }
   // chunked form: the stored state of the chunk's 8 steps (steps l0 .. l0+7,
   // n of them valid) is loaded before the first, so the loads overlap; in
@@ -481,11 +493,11 @@ struct Adjoint {
       }
     }
   }
-  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk, uint32_t) {
-    if (sizeof(T) != 4) return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk]);
+  __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk, uint32_t xs) {
+    if (sizeof(T) != 4) return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk], xs);
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const double w = has_u ? point_w(sg, li, t) : 0.0;
+    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_tile128 != 0) : 0.0;
     float fa, fb, fu;
     const float sb = variable32(sg.tg[li], (float)w, has_u, (float)pre_y[kk], (float)pre_s[kk],
                                 (float)pre_dc[kk], true, fa, fb, fu);
@@ -551,7 +563,7 @@ struct Adjoint {
     Staged<T> sg0;
     sg0.qv[0] = gen.q ? gen.q[0] : 0.0;
     sg0.shv[0] = shift_at<T>(gen, k * (d - 1));
-    const double w = point_w(sg0, 0, 0);
+    const double w = point_w(sg0, 0, 0, 0u, false);
     const T y = io.y[io.at(0, g)];
     double ga, gb, gu;
     variable(tgt[0], w, true, y, T(0), (T)io.dc1, false, ga, gb, gu);

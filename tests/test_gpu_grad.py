@@ -242,27 +242,35 @@ def _banded(n, seed):
     return S, lo, up, rng.random((n - 1, 4))
 
 
-def _banded_problem(D, S, lo, up, sh, band, m=512, context=None):
+def _banded_problem(D, S, lo, up, sh, band, m=512, context=None, sobol=False):
+    # sobol: Sobol points from index 2048 (a multiple of 128: the loops'
+    # staged integers), random shifts drawn from sh's values
+    kw = dict(qmc_type="Richtmyer", shifts=sh)
+    if sobol:
+        kw = dict(qmc_type="Sobol", ushifts=(sh * 2.0**63).astype(np.uint64), sobol_first=2048)
     Q = D.QMCDataSparse(S, lo, up, D.QMC_opts(m=m, n_reps=4, max_pts=m, max_abs_err=0.0),
-                        qmc_type="Richtmyer", shifts=sh, context=context)
+                        context=context, **kw)
     Q.truncate_band(band)
     return Q
 
 
-def _Pband(D, S, lo, up, sh, band):
-    Q = _banded_problem(D, S, lo, up, sh, band)
+def _Pband(D, S, lo, up, sh, band, m=512, sobol=False):
+    Q = _banded_problem(D, S, lo, up, sh, band, m=m, sobol=sobol)
     P = D.qmc_pnorm(Q, precision=L.PREC_FP64)[0]
     Q.close()
     return P
 
 
-def test_banded_gradient_matches_finite_differences(dbgz):
+@pytest.mark.parametrize("qmc,m", [("Richtmyer", 512), ("Sobol", 500)])
+def test_banded_gradient_matches_finite_differences(dbgz, qmc, m):
     # the banded path (classic factor, no pivoting) against central
-    # differences of the banded estimate in the original bounds
+    # differences of the banded estimate in the original bounds; Sobol: the
+    # adjoint takes the staged integers (partial last tile)
     D = dbgz
     n, band = 90, 6
+    sob = qmc == "Sobol"
     S, lo, up, sh = _banded(n, 91)
-    Q = _banded_problem(D, S, lo, up, sh, band)
+    Q = _banded_problem(D, S, lo, up, sh, band, m=m, sobol=sob)
     P, _, _, da, db, dU = D.qmc_pnorm_grad(Q, precision=L.PREC_FP64)
     assert dU is None
     assert abs(P - D.qmc_pnorm(Q, precision=L.PREC_FP64)[0]) <= 1e-14 * P
@@ -272,8 +280,8 @@ def test_banded_gradient_matches_finite_differences(dbgz):
     for i in rng.choice(n, 6, replace=False):
         e = np.zeros(n)
         e[i] = h
-        fdb = (_Pband(D, S, lo, up + e, sh, band) - _Pband(D, S, lo, up - e, sh, band)) / (2 * h)
-        fda = (_Pband(D, S, lo + e, up, sh, band) - _Pband(D, S, lo - e, up, sh, band)) / (2 * h)
+        fdb = (_Pband(D, S, lo, up + e, sh, band, m, sob) - _Pband(D, S, lo, up - e, sh, band, m, sob)) / (2 * h)
+        fda = (_Pband(D, S, lo + e, up, sh, band, m, sob) - _Pband(D, S, lo - e, up, sh, band, m, sob)) / (2 * h)
         assert abs(db[i] - fdb) <= 2e-6 * max(abs(fdb), abs(P)) + 1e-12, (i, db[i], fdb)
         assert abs(da[i] - fda) <= 2e-6 * max(abs(fda), abs(P)) + 1e-12, (i, da[i], fda)
 
