@@ -25,7 +25,11 @@
 //    without cancellation and Phi^-1 is taken of the smaller one; dc is the
 //    difference of two tails of the same side only when the interval lies
 //    in one tail, and then in FP64 (erfc) if the FP32 difference would
-//    cancel.  The weight product p stays FP64 (no underflow at d = 1000).
+//    cancel.  The weight product p stays FP64: FP32 would underflow where
+//    the FP64 product is still normal (a product of d factors of about
+//    1/2 leaves FP32's range at d ~ 150, FP64's at d ~ 1075); where P
+//    itself is below FP64's range (e.g. 1000 bounds at marginal
+//    probabilities 1e-3..1e-1) both give 0, as the reference does.
 //    u is clamped to [eps64, 1 - eps64] like the Float64 reference.
 #pragma once
 #include "normal32.cuh"

@@ -14,6 +14,7 @@
 // only the source of the first dimension's (c, dc) differs: it is computed
 // on the device into the array instead of on the host.
 #include "loop_simt_kernels.cuh"
+#include <cuda.h>
 #include <algorithm>
 #include <mutex>
 
@@ -35,13 +36,47 @@ static_assert(kMaxD * sizeof(TargetParams64) <= kTgtBytes, "target region too sm
 // host-side stand-in; the device address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
+// The array's device address belongs to a CUDA context (the module is loaded
+// per context), so the cache is keyed on the current context's unique id
+// (cuCtxGetId: a new context, also the primary context re-created after
+// cudaDeviceReset, gets a new id), not on the device ordinal.
 struct DeviceSlot {
+  unsigned long long ctx_id = 0;
+  bool used = false;
   unsigned char *ptr = nullptr;
   int per_sm = 0;
   int num_sms = 0;
 };
+constexpr int kSlots = 64;
 std::mutex g_mu;
-DeviceSlot g_slots[64];
+DeviceSlot g_slots[kSlots];
+int g_next_slot = 0;
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// The unique id of the calling thread's current context (0 on failure).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = (CtxGetCurrentFn)p;
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (CtxGetIdFn)p;
+    cudaGetLastError();
+  });
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // The FP64 step whose first-dimension (c, dc) is read from the array header.
 struct StepFp64Scratch : dbgz::StepFp64 {
@@ -68,11 +103,16 @@ __global__ void k_noalloc_setup(const double *U, int64_t d, const double *a, con
 }
 
 int setup_device(int dev, DeviceSlot &slot) {
+  // the context must be current (cudaGetDevice made the runtime's primary
+  // context current if the caller had none)
+  const unsigned long long id = current_context_id();
+  if (!id) return DBGZ_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (g_slots[dev].ptr) {
-    slot = g_slots[dev];
-    return DBGZ_OK;
-  }
+  for (int i = 0; i < kSlots; ++i)
+    if (g_slots[i].used && g_slots[i].ctx_id == id) {
+      slot = g_slots[i];
+      return DBGZ_OK;
+    }
   DeviceSlot s;
   void *p = nullptr;
   if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
@@ -89,7 +129,10 @@ int setup_device(int dev, DeviceSlot &slot) {
     cudaGetLastError();
     return DBGZ_ERR_CUDA;
   }
-  g_slots[dev] = s;
+  s.ctx_id = id;
+  s.used = true;
+  g_slots[g_next_slot] = s;  // round robin over the slots once all are taken
+  g_next_slot = (g_next_slot + 1) % kSlots;
   slot = s;
   return DBGZ_OK;
 }
@@ -103,11 +146,13 @@ extern "C" int dbgz_pnorm_pass_noalloc(int64_t d, const double *U, const double 
   if (!U || !a || !b || !q || !shifts || !qmc_reps || m < 1 || n_reps < 1 || n_base < 0)
     return DBGZ_ERR_INVALID_ARGUMENT;
   if (d < 2 || d > kMaxD) return DBGZ_ERR_DIMENSION;
-  const int64_t tps = (m + TS - 1) / TS;
+  // tiles per shift without overflow (m + TS - 1 could wrap), and the tile
+  // count checked before it is formed (tps * n_reps could wrap)
+  const int64_t tps = m / TS + (m % TS != 0);
+  if (n_reps > kMaxTiles || tps > kMaxTiles / n_reps) return DBGZ_ERR_DIMENSION;
   const int64_t n_tiles = tps * n_reps;
-  if (n_tiles > kMaxTiles) return DBGZ_ERR_DIMENSION;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     cudaGetLastError();
     return DBGZ_ERR_CUDA;
   }

@@ -5,8 +5,7 @@
  * This is the drop-in boundary for the reference's qmc_pnorm! path
  * (JakobPeterlin/DBGenzPaper, Julia).  Every entry point names the
  * reference function it replaces (file:line in that repository).  A Julia
- * caller binds these with ccall; any C caller can use
- * them directly.
+ * caller binds these with ccall; any C caller can use them directly.
  *
  * Conventions
  *   - Plain pointers and sizes only.  Matrices are column-major (Julia
@@ -260,9 +259,12 @@ int dbgz_pnorm_grad_sigma(dbgz_problem *p, int precision, double *result, double
  * Limits: 2 <= d <= 8192 and ceil(m/128) * n_reps <= 131072; larger sizes
  * return DBGZ_ERR_DIMENSION.  Large d runs on fewer CTAs (the workspace
  * share of one CTA grows with d), so this is slower than dbgz_pnorm.
- * The first call on a device looks up the array's device address with
- * that device current (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls share the one array and leave their
+ * The first call in a CUDA context (normally the primary context of each
+ * device) looks up the array's device address in that context
+ * (cudaGetSymbolAddress) and keeps it, keyed on the context's unique id,
+ * so a new context -- also the primary context re-created after
+ * cudaDeviceReset -- gets its own look-up; make the first call in each
+ * context before any stream capture.  All calls share the one array and leave their
  * intermediate data in it: calls whose work overlaps on the GPU (other
  * streams or host threads at the same time) race and corrupt each other's
  * results, so serialise them. */

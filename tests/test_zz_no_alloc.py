@@ -64,3 +64,8 @@ def test_noalloc_rejects_sizes_beyond_its_array(dbgz):
                                        None) == L.ERR_DIMENSION
     assert lib.dbgz_pnorm_pass_noalloc(10, None, fake, fake, fake, fake, 100, 2, 0, fake,
                                        None) == L.ERR_INVALID_ARGUMENT
+    # tile counts whose product (or m + 127) would wrap in 64 bits
+    assert lib.dbgz_pnorm_pass_noalloc(10, fake, fake, fake, fake, fake, 384, 6148914691236517206, 0,
+                                       fake, None) == L.ERR_DIMENSION
+    assert lib.dbgz_pnorm_pass_noalloc(10, fake, fake, fake, fake, fake, 2**63 - 1, 1, 0, fake,
+                                       None) == L.ERR_DIMENSION
