@@ -13,12 +13,12 @@ shifts; one step = one qmc_pnorm! pass over all samples.
              integration, read-back
   roofline   the integration-loop kernel against the measured dense bf16
              tensor peak (contraction flops = samples * d (d - 1) per launch)
-  cpu_baseline  the CPU checker (C restatement of the reference's Float64
-             loop, OpenMP on all host cores) on a bounded sample, projected
-             to the full step
+  cpu_baseline  one full step of the reference's Float64 loop restated
+             for speed on the CPU (oracle/genz_cpu_blas.c: BLAS-3
+             contraction, vectorised erf/erfinv, all host threads), measured
 
-``--impl reference`` times only the CPU restatement of the reference path
-(all host threads), on rank 0.
+``--impl reference`` times only that CPU restatement of the reference path
+(all host threads), on rank 0, in whole steps.
 """
 from __future__ import annotations
 
@@ -134,32 +134,58 @@ def workload(rank: int, world: int, quick: bool, d=None, points=None):
     return w
 
 
-def cpu_baseline(w, threads: int, target_s: float = 12.0):
-    """Time the CPU checker on a bounded sample of workload w; project to a full step."""
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_prepare(w):
+    """The CPU side of QMCData for workload w: the checker's cholesky_genz!
+    and truncation (the factor the timed CPU loop integrates over)."""
     from oracle import oracle as O
+    O.build()
     F = O.cholesky_genz(w.Sigma, w.a, w.b)
-    U = O.truncate_U(F["U"])
-    kw = dict(block_size_i=1024, block_size_i2=64, block_size_j=64, threads=threads)
-    # calibrate on a small sample, then size the timed sample to ~target_s
-    m0, r0 = 1024, 2
+    return O.truncate_U(F["U"]), F["a"], F["b"]
+
+
+def cpu_step(w, prep, threads: int, n_shifts=None):
+    """One qmc_loop! pass of the reference's Float64 path restated for speed on
+    the CPU (oracle/genz_cpu_blas.c: BLAS-3 contraction, vectorised erf and
+    erfinv, point tiles of 64 over all threads; the reference's x86 paper
+    blocks, block_size_i 2^9, block_size_i2 2^6, block_size_j 2^6) over all
+    w.m points of the first n_shifts shifts (all by default).  Returns
+    (seconds, per-shift means)."""
+    from oracle import oracle as O
+    U, a, b = prep
+    k = w.n_reps if n_shifts is None else n_shifts
     t = time.perf_counter()
-    O.qmc_pnorm(U, F["a"], F["b"], m=m0, n_reps=r0, shifts=w.shifts[:, :r0], **kw)
-    rate0 = m0 * r0 / (time.perf_counter() - t)
-    n_reps = min(w.n_reps, 4)
-    m = int(min(w.m, max(1024, rate0 * target_s / n_reps)))
-    t = time.perf_counter()
-    O.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=n_reps, shifts=w.shifts[:, :n_reps], **kw)
-    dt = time.perf_counter() - t
-    rate = m * n_reps / dt
+    reps = O.qmc_pass_blas(U, a, b, m=w.m, n_reps=k, shifts=w.shifts[:, :k], threads=threads)
+    return time.perf_counter() - t, reps
+
+
+def cpu_baseline(w, threads: int):
+    """The CPU restatement of the reference loop timed on one full step of
+    workload w (all points of all shifts), factorisation excluded like
+    `value`."""
+    from oracle import oracle as O
+    prep = cpu_prepare(w)
+    cpu_step(w, prep, threads, n_shifts=1)  # warm-up (page-in, thread pool)
+    dt, _ = cpu_step(w, prep, threads)
     return {
-        "value": 1e3 * w.samples / rate,
+        "value": 1e3 * dt,
         "unit": UNIT,
         "cores": threads,
         "kind": "port",
-        "sample": f"{m} points x {n_reps} shifts of the d={w.d} workload ({m * n_reps} samples, "
-                  f"{dt:.1f} s on {threads} threads, FP64, factorisation excluded); "
-                  f"projected to {w.samples} samples",
-        "samples_per_s": rate,
+        "sample": f"one full step: {w.m} points x {w.n_reps} shifts of the d={w.d} workload "
+                  f"({w.samples} samples), measured, factorisation excluded; C restatement of the "
+                  f"reference's Float64 qmc_loop! with its BLAS-3 contraction (oracle/genz_cpu_blas.c, "
+                  f"{O.cpu_isa()} build) on {threads} threads of a {cpu_model()}",
+        "samples_per_s": w.samples / dt,
     }
 
 
@@ -400,42 +426,53 @@ def run_c5(args):
 
 
 def run_reference(args):
+    """The reference arm: the reference's Float64 qmc_pnorm! pass restated on
+    the CPU (oracle/genz_cpu_blas.c; Julia is not installed on this image),
+    all host threads, rank 0 only.  A step is one full pass over the
+    workload's samples when --warmup + --steps such steps fit in about
+    three minutes, else a whole-shift sample of it (every point of the first
+    k shifts, k >= 2) scaled to the step's 16 shifts (the per-sample cost
+    does not depend on the shift); `sample` says which."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     from oracle import oracle as O
-    O.build()
-    w = workload(0, 1, args.quick)
-    F = O.cholesky_genz(w.Sigma, w.a, w.b)
-    U = O.truncate_U(F["U"])
-    kw = dict(block_size_i=1024, block_size_i2=64, block_size_j=64, threads=threads)
-    # bounded step: 2 shifts x m points, sized to ~1.5 s of CPU work
-    t = time.perf_counter()
-    O.qmc_pnorm(U, F["a"], F["b"], m=512, n_reps=2, shifts=w.shifts[:, :2], **kw)
-    rate0 = 1024 / (time.perf_counter() - t)
-    m = int(min(w.m, max(512, rate0 * 1.5 / 2)))
+    w = workload(0, 1, args.quick, args.d, args.points)
+    prep = cpu_prepare(w)
+    # size the step: one shift first, then the shifts per step
+    t1, _ = cpu_step(w, prep, threads, n_shifts=1)
+    per_step = t1 * w.n_reps
+    budget = 180.0
+    k = w.n_reps
+    if (args.steps + args.warmup) * per_step > budget:
+        k = max(2, min(w.n_reps, int(budget / ((args.steps + args.warmup) * t1))))
     for _ in range(args.warmup):
-        O.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=2, shifts=w.shifts[:, :2], **kw)
+        cpu_step(w, prep, threads, n_shifts=k)
     times = []
     for _ in range(args.steps):
-        t = time.perf_counter()
-        O.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=2, shifts=w.shifts[:, :2], **kw)
-        times.append(time.perf_counter() - t)
-    rate = 2 * m / statistics.mean(times)
-    val = 1e3 * w.samples / rate
+        dt, reps = cpu_step(w, prep, threads, n_shifts=k)
+        times.append(dt)
+    val = 1e3 * statistics.mean(times) * (w.n_reps / k)
+    if k == w.n_reps:
+        sample = (f"each step one full pass: {w.m} points x {w.n_reps} shifts of the d={w.d} workload "
+                  f"({w.samples} samples), measured")
+    else:
+        sample = (f"each step every point of {k} of the {w.n_reps} shifts ({w.m * k} samples), measured, "
+                  f"scaled by {w.n_reps}/{k} to the full step of {w.samples} samples")
+    sample += (f"; {threads} threads of a {cpu_model()}; C restatement of the reference's Float64 "
+               f"qmc_loop! (BLAS-3 contraction, vectorised erf/erfinv; oracle/genz_cpu_blas.c, "
+               f"{O.cpu_isa()} build; Julia is not installed on this image); factorisation excluded")
     line = {
         "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": val, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": w.name, "d": w.d, "points": w.m, "shifts": w.n_reps,
                    "samples": w.samples},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"each step {m} points x 2 shifts ({2 * m} samples) of the d={w.d} "
-                                   f"workload on {threads} threads, projected to {w.samples} samples "
-                                   "(C restatement of the reference's Float64 qmc_loop!; Julia is "
-                                   "not installed on this image)"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "samples_per_s": w.samples / (val * 1e-3)},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "P": float(np.mean(reps)),
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -202,3 +202,119 @@ def qmc_pnorm(U, a, b, *, m, n_reps, qmc_type=RICHTMYER, shifts=None, q=None, V=
                         C.byref(npts), _pd(reps))
     del keep
     return res.value, err.value, npts.value, reps
+
+
+# ---- the timed CPU baseline (oracle/genz_cpu_blas.c) ----------------------
+class CpuProblem(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("U", C.POINTER(C.c_double)),
+        ("a", C.POINTER(C.c_double)),
+        ("b", C.POINTER(C.c_double)),
+        ("qmc_type", C.c_int),
+        ("q", C.POINTER(C.c_double)),
+        ("shifts", C.POINTER(C.c_double)),
+        ("V", C.POINTER(C.c_uint32)),
+        ("sobol_first", C.c_int64),
+        ("ushifts", C.POINTER(C.c_uint64)),
+        ("n_bits", C.c_int64),
+    ]
+
+
+_cpu = None
+
+
+def cpu_isa() -> str:
+    """'avx512' when the host CPU has AVX-512 (F, DQ, BW, VL), else 'avx2'."""
+    try:
+        flags = open("/proc/cpuinfo").read()
+    except OSError:
+        return "avx2"
+    return "avx512" if all(f" {x}" in flags for x in ("avx512f", "avx512dq", "avx512bw", "avx512vl")) else "avx2"
+
+
+def openblas_path() -> str:
+    """numpy's bundled OpenBLAS (ILP64, symbols with the scipy_ prefix)."""
+    import glob
+    base = os.path.dirname(os.path.dirname(np.__file__))
+    cand = sorted(glob.glob(os.path.join(base, "numpy.libs", "libscipy_openblas64_*.so")))
+    if not cand:
+        raise RuntimeError("numpy's bundled OpenBLAS (libscipy_openblas64_*.so) not found")
+    return cand[0]
+
+
+def cpu_lib():
+    """The vectorised BLAS-3 CPU loop for this CPU, with dgemm bound."""
+    global _cpu
+    if _cpu is None:
+        path = os.path.join(_HERE, f"libgenz_cpu_{cpu_isa()}.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.cpu_blas_init.argtypes = [C.c_char_p]
+        L.cpu_qmc_pass.argtypes = [C.POINTER(CpuProblem), C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                   C.c_double, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_int,
+                                   C.POINTER(C.c_double)]
+        L.cpu_erfinv.argtypes = [C.c_int64, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        rc = L.cpu_blas_init(openblas_path().encode())
+        if rc != 0:
+            raise RuntimeError(f"cpu_blas_init failed ({rc})")
+        _cpu = L
+    return _cpu
+
+
+def cpu_erfinv(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    cpu_lib().cpu_erfinv(x.size, _pd(x), _pd(y))
+    return y
+
+
+def first_cdf(U, a, b):
+    """c_1, dc_1 of qmc_pnorm! (src/qmc.jl:800-809, erf form)."""
+    import math
+    c2 = math.sqrt(2.0)
+    aa = a[0] / (U[0, 0] * c2)
+    bb = b[0] / (U[0, 0] * c2)
+    return 0.5 * (1 + math.erf(aa)), 0.5 * (math.erf(bb) - math.erf(aa))
+
+
+def qmc_pass_blas(U, a, b, *, m, n_reps, qmc_type=RICHTMYER, shifts=None, q=None, V=None, sobol_first=0,
+                  ushifts=None, n_bits=32, block_size_i=512, block_size_i2=64, block_size_j=64,
+                  threads=0, n_pass_base=0):
+    """One qmc_loop! pass of the BLAS-3, vectorised CPU restatement (the timed
+    baseline); returns the per-shift means (first pass, n_pts0 = 0).  Default
+    blocks are the reference's x86/MKL paper settings (block_size_i 2^9,
+    block_size_i2 2^6, block_size_j 2^6: scripts/simulations/simulation_comparison.jl:33-34)."""
+    n = U.shape[0]
+    U = np.asfortranarray(U, dtype=np.float64)
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    keep = [U, a, b]
+    P = CpuProblem()
+    P.n = n
+    P.U, P.a, P.b = _pd(U), _pd(a), _pd(b)
+    P.qmc_type = qmc_type
+    P.n_bits = n_bits
+    if qmc_type == RICHTMYER:
+        q = sqrt_primes(n - 1) if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        sh = np.asfortranarray(shifts, dtype=np.float64)
+        assert sh.shape == (n - 1, n_reps)
+        keep += [q, sh]
+        P.q, P.shifts = _pd(q), _pd(sh)
+    else:
+        Vv = np.ascontiguousarray(V, dtype=np.uint32)
+        us = np.asfortranarray(ushifts, dtype=np.uint64)
+        assert us.shape == (n - 1, n_reps) and Vv.shape == (n - 1, 32)
+        keep += [Vv, us]
+        P.V = Vv.ctypes.data_as(C.POINTER(C.c_uint32))
+        P.ushifts = us.ctypes.data_as(C.POINTER(C.c_uint64))
+        P.sobol_first = sobol_first
+    c1, dc1 = first_cdf(U, a, b)
+    reps = np.zeros(n_reps, dtype=np.float64)
+    rc = cpu_lib().cpu_qmc_pass(C.byref(P), m, n_reps, 0, n_pass_base, c1, dc1, block_size_i,
+                                block_size_i2, block_size_j, threads, _pd(reps))
+    if rc != 0:
+        raise RuntimeError(f"cpu_qmc_pass failed ({rc})")
+    del keep
+    return reps

@@ -227,3 +227,54 @@ def test_pivot_margins_log(oracle):
     F2 = oracle.cholesky_genz(S, lo, up)
     assert np.array_equal(F1["U"], F2["U"]) and np.array_equal(F1["perm"], F2["perm"])
     assert np.all(F1["margins"][np.isfinite(F1["margins"])] >= 0.0)
+
+
+# ---- the timed CPU baseline (oracle/genz_cpu_blas.c) against the checker --
+@pytest.mark.parametrize("isa", ["avx2", "avx512"])
+def test_cpu_blas_pass_matches_checker(oracle, isa, monkeypatch):
+    """The BLAS-3, vectorised restatement of qmc_loop! that bench.py times
+    (src/qmc.jl:315-444) gives the checker's per-shift means to 1e-13
+    relative: both generators, partial last tiles, tile heights that are not
+    multiples of 8, several outer and inner dimension blocks."""
+    if isa == "avx512" and oracle.cpu_isa() != "avx512":
+        pytest.skip("no AVX-512 on this CPU")
+    monkeypatch.setattr(oracle, "_cpu", None)
+    monkeypatch.setattr(oracle, "cpu_isa", lambda: isa)
+    from oracle.oracle import sqrt_primes  # noqa: F401  (the checker is built)
+    rng = np.random.default_rng(77)
+    for d, m, bj, bi, bi2 in ((33, 500, 20, 16, 8), (150, 777, 100, 64, 32), (301, 300, 64, 128, 32)):
+        S = W.rand_spd(d, 1.0, rng)
+        lo, up = W.bounds_quarter(S)
+        F = oracle.cholesky_genz(S, lo, up)
+        U = oracle.truncate_U(F["U"])
+        sh = rng.random((d - 1, 3))
+        r_fast = oracle.qmc_pass_blas(U, F["a"], F["b"], m=m, n_reps=3, shifts=sh, block_size_j=bj,
+                                      block_size_i=bi, block_size_i2=bi2, threads=2)
+        r_chk = oracle.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=3, shifts=sh)[3]
+        np.testing.assert_allclose(r_fast, r_chk, rtol=1e-13, atol=0)
+        V = W.sobol_table(d - 1) if hasattr(W, "sobol_table") else None
+        if V is None:
+            import dbgenzpaper_b200 as D
+            V = D.sobol_dirnums(d - 1)
+        us = rng.integers(0, 2**63, size=(d - 1, 3), dtype=np.uint64)
+        first = 2 * m + 1
+        r_fast = oracle.qmc_pass_blas(U, F["a"], F["b"], m=m, n_reps=3, qmc_type=oracle.SOBOL, V=V,
+                                      ushifts=us, sobol_first=first, block_size_j=bj, block_size_i=bi,
+                                      block_size_i2=bi2, threads=2)
+        r_chk = oracle.qmc_pnorm(U, F["a"], F["b"], m=m, n_reps=3, qmc_type=oracle.SOBOL, V=V, ushifts=us,
+                                 sobol_first=first)[3]
+        np.testing.assert_allclose(r_fast, r_chk, rtol=1e-13, atol=0)
+
+
+def test_cpu_blas_erfinv(oracle):
+    """The vectorised erfinv of the CPU baseline against the checker's
+    Newton-refined one: relative error < 1e-13 where |x| >= 1e-3, absolute
+    < 1e-15 everywhere (the Halley step works on erfc(x) = 1 - |x|, so near
+    0 the error is absolute, about 1e-17)."""
+    x = np.concatenate([np.linspace(-1 + 4.4e-16, 1 - 4.4e-16, 20001), 1 - np.logspace(-15.6, -0.3, 500),
+                        -1 + np.logspace(-15.6, -0.3, 500), np.logspace(-12, -1, 200)])
+    y = oracle.cpu_erfinv(x)
+    yo = np.array([oracle.erfinv(v) for v in x])
+    big = np.abs(x) >= 1e-3
+    assert np.max(np.abs(y[big] - yo[big]) / np.abs(yo[big])) < 1e-13
+    assert np.max(np.abs(y - yo)) < 1e-15
