@@ -41,7 +41,8 @@ from . import _lib as L
 
 __all__ = [
     "QMCOpts", "QMC_opts", "QMCData", "QMCDataSparse", "QMCData_Distributions",
-    "qmc_pnorm", "qmc_pnorm_grad", "CholeskyGenz", "cholesky_genz", "cholesky_classic",
+    "qmc_pnorm", "qmc_pnorm_grad", "qmc_pnorm_logw", "log_mean_exp", "CholeskyGenz", "cholesky_genz",
+    "cholesky_classic", "cholesky_rowmax", "adapt_low_rank", "sobol_first_index",
     "get_sqrt_primes", "richtmyer_mat", "sobol_mat", "sobol_dirnums", "Context",
     "get_context", "DbgzError", "PRECISIONS", "qmc_pnorm_batch", "BatchPlan", "batch_autotune",
     "batch_tuning",
@@ -201,8 +202,7 @@ class QMCData:
             ush = np.asfortranarray(ush)
             if sobol_dirnums is not None:
                 V = np.ascontiguousarray(sobol_dirnums, dtype=np.uint32)
-            # SobolQMC skips skip0 = 2m - 1 points (src/qmc.jl:178)
-            first = (2 * opts.m - 1) + 1 if sobol_first is None else int(sobol_first)
+            first = sobol_first_index(opts.m) if sobol_first is None else int(sobol_first)
         self.shifts, self.ushifts, self.sobol_dirnums, self.sobol_first = sh, ush, V, first
         h = C.c_void_p()
         co = opts.to_c()
@@ -310,6 +310,39 @@ def qmc_pnorm(D, use_AppleBLAS=None, *, precision: Optional[int] = None, return_
     return out + (reps,) if return_reps else out
 
 
+def qmc_pnorm_logw(D, *, precision: Optional[int] = None):
+    """Per-sample log-weights of one pass (dbgz_pnorm_logw; no reference
+    counterpart) -> (logw, reps): logw[j, k] = log p of point j of shift k,
+    the sum of log dc over the sample's variables, finite where p underflows;
+    reps the pass's per-shift means of p.  The pass uses the points the next
+    qmc_pnorm pass would take and does not advance the generator."""
+    dist = isinstance(D, QMCData_Distributions)
+    base = D.D if dist else D
+    prec = base.resolved_precision() if precision is None else int(precision)
+    m, R = base.opts.m, base.opts.n_reps
+    logw = np.zeros((m, R), dtype=np.float64, order="F")
+    reps = np.zeros(R)
+    lib = L.lib()
+    if dist:
+        lib.dbgz_problem_set_cdf_form(base.handle, L.CDF_ERFC)
+    try:
+        st = lib.dbgz_pnorm_logw(base.handle, prec, L.ptr(logw), L.ptr(reps))
+    finally:
+        if dist:
+            lib.dbgz_problem_set_cdf_form(base.handle, int(base.cdf_form))
+    L.check(st, base.ctx.handle)
+    return logw, reps
+
+
+def log_mean_exp(logw, axis=0):
+    """log of the mean of exp(logw) along axis, without underflow: the log of
+    the per-shift estimate from per-sample log-weights."""
+    x = np.asarray(logw, dtype=np.float64)
+    mx = np.max(x, axis=axis, keepdims=True)
+    mx = np.where(np.isfinite(mx), mx, 0.0)
+    return np.squeeze(mx, axis=axis) + np.log(np.mean(np.exp(x - mx), axis=axis))
+
+
 def qmc_pnorm_grad(D, *, precision: Optional[int] = None, want_U: bool = True):
     """Estimate and exact gradient on the current point set (no counterpart
     in the reference): -> (P, err, n_pts, dP_da, dP_db, dP_dU).
@@ -395,7 +428,7 @@ def qmc_pnorm_batch(problems, opts: Optional[QMCOpts] = None, rng=None, qmc_type
         ush = np.concatenate([np.ravel(np.asarray(x, dtype=np.uint64), order="F") for x in ushifts])
         if sobol_dirnums is not None:
             V = np.ascontiguousarray(sobol_dirnums, dtype=np.uint32)
-        first = (2 * opts.m - 1) + 1 if sobol_first is None else int(sobol_first)
+        first = sobol_first_index(opts.m) if sobol_first is None else int(sobol_first)
     prec = (L.PREC_FP64 if opts.T == np.float64 else DEFAULT_FP32_PRECISION) if precision is None else int(precision)
     n = len(problems)
     P, err = np.zeros(n), np.zeros(n)
@@ -435,7 +468,7 @@ class BatchPlan:
         self.precision = ((L.PREC_FP64 if self.opts.T == np.float64 else DEFAULT_FP32_PRECISION)
                           if precision is None else int(precision))
         V = None if sobol_dirnums is None else np.ascontiguousarray(sobol_dirnums, dtype=np.uint32)
-        first = (2 * self.opts.m - 1) + 1 if sobol_first is None else int(sobol_first)
+        first = sobol_first_index(self.opts.m) if sobol_first is None else int(sobol_first)
         self._lib = L.lib()
         h = C.c_void_p()
         co = self.opts.to_c()
@@ -566,6 +599,41 @@ def cholesky_classic(M, a, b, block_size=2**7, block_size2=2**9, block_size3=2**
     return CholeskyGenz(Mf, np.arange(n), n, a, b, block_size, "none", sv)
 
 
+def cholesky_rowmax(M, a, b, block_size=2**7, block_size2=2**9, block_size3=2**10,
+                    block_size4=2**11, *, device=0) -> CholeskyGenz:
+    """cholesky_rowmax!(copy(M), copy(a), copy(b), ...) on the GPU
+    (src/cholesky.jl:244-432): diagonal pivoting; a and b come back scaled
+    but in the original order, as the reference leaves them."""
+    ctx = get_context(device)
+    Mf = np.array(M, dtype=np.float64, order="F", copy=True)
+    n = Mf.shape[0]
+    a, b = _f64(a).copy(), _f64(b).copy()
+    perm = np.zeros(n, dtype=np.int64)
+    sv = np.zeros(n)
+    rank = C.c_int64()
+    L.check(L.lib().dbgz_cholesky_rowmax(ctx.handle, n, L.ptr(Mf), L.ptr(a), L.ptr(b), block_size,
+                                         block_size2, block_size3, block_size4,
+                                         L.ptr(perm, C.c_int64), L.ptr(sv), C.byref(rank)), ctx.handle)
+    return CholeskyGenz(Mf, perm, rank.value, a, b, block_size, "row_max", sv)
+
+
+def adapt_low_rank(M, a, b, rank: int, perm, eps1: float, *, device=0):
+    """adapt_low_rank!(M, a, b, rank, perm, eps1) (src/cholesky.jl:24-123) on
+    copies -> (M, a, b, perm, k_js, k_0): perm holds 0-based indices, k_js the
+    blocks' 1-based end positions (as the reference returns them)."""
+    ctx = get_context(device)
+    Mf = np.array(M, dtype=np.float64, order="F", copy=True)
+    nr, n = Mf.shape
+    a, b = _f64(a).copy(), _f64(b).copy()
+    pm = np.array(perm, dtype=np.int64, copy=True)
+    k_js = np.zeros(max(int(rank), 1), dtype=np.int64)
+    k0 = C.c_int64()
+    L.check(L.lib().dbgz_adapt_low_rank(ctx.handle, nr, n, L.ptr(Mf), L.ptr(a), L.ptr(b), int(rank),
+                                        L.ptr(pm, C.c_int64), float(eps1), L.ptr(k_js, C.c_int64),
+                                        C.byref(k0)), ctx.handle)
+    return Mf, a, b, pm, k_js[:int(rank)], int(k0.value)
+
+
 def get_sqrt_primes(n: int) -> np.ndarray:
     q = np.zeros(n)
     L.check(L.lib().dbgz_sqrt_primes(n, L.ptr(q)))
@@ -578,6 +646,28 @@ def richtmyer_mat(m: int, q, n0: int = 0, *, device=0) -> np.ndarray:
     X = np.zeros((m, q.size), order="F")
     L.check(L.lib().dbgz_richtmyer_mat(ctx.handle, m, q.size, L.ptr(q), n0, L.ptr(X)), ctx.handle)
     return X
+
+
+def sobol_first_index(m: int, skip0: Optional[int] = None, exact: bool = False) -> int:
+    """Index of the first point SobolQMC draws, in the Gray-code order whose
+    index 0 is the all-zero point (the index the library's generators take).
+
+    SobolQMC starts from ``skip(SobolSeq(d), skip0)`` with skip0 = 2m - 1
+    (src/qmc_generators.jl:57-58).  Sobol.jl 1.5.0's ``skip(s, n)`` (exact =
+    false, the default) calls ``next!`` 2^floor(log2(n + 1)) times, and the
+    k-th ``next!`` of a fresh sequence returns Gray-code point k (the zero
+    point is never returned), so the first point sobol_mat! reads is
+    2^floor(log2(2m)) + 1: 2m + 1 when m is a power of two, 16385 for the
+    default m = 10^4.  ``exact=True`` restates ``skip(s, n, exact=true)``
+    (first point n + 1).  Sobol.jl itself is not part of the reference
+    repository; these semantics are its published ones, restated here."""
+    n = 2 * int(m) - 1 if skip0 is None else int(skip0)
+    if n < 0:
+        raise ValueError("skip0 must be non-negative")
+    if n == 0:
+        return 1
+    nskip = n if exact else 1 << ((n + 1).bit_length() - 1)
+    return nskip + 1
 
 
 def sobol_dirnums(dims: int) -> np.ndarray:

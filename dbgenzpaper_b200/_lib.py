@@ -92,6 +92,7 @@ SIGNATURES = {
     "dbgz_problem_truncate_band": (C.c_int, [_vp, C.c_int64]),
     "dbgz_problem_factor": (C.c_int, [_vp, _pd, _pi64, _pd, _pd, _pd, _pi64]),
     "dbgz_pnorm": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
+    "dbgz_pnorm_logw": (C.c_int, [_vp, C.c_int, _pd, _pd]),
     "dbgz_pnorm_graph": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
     "dbgz_pnorm_grad": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
     "dbgz_problem_sigma_adjoint": (C.c_int, [_vp, _pd, _pd, _pd, _pd]),
@@ -113,6 +114,10 @@ SIGNATURES = {
                                           C.c_int64, C.c_int64, _vp, _vp]),
     "dbgz_cholesky_genz": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,
                                      C.c_int64, C.c_int64, _pi64, _pd, _pi64]),
+    "dbgz_cholesky_rowmax": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64, C.c_int64,
+                                       C.c_int64, _pi64, _pd, _pi64]),
+    "dbgz_adapt_low_rank": (C.c_int, [_vp, C.c_int64, C.c_int64, _pd, _pd, _pd, C.c_int64, _pi64, C.c_double,
+                                      _pi64, _pi64]),
     "dbgz_cholesky_classic": (C.c_int, [_vp, C.c_int64, _pd, _pd, _pd, C.c_int64, C.c_int64,
                                         C.c_int64, C.c_int64, _pd]),
     "dbgz_sqrt_primes": (C.c_int, [C.c_int64, _pd]),

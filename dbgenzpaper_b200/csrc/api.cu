@@ -632,4 +632,66 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
   return DBGZ_OK;
 }
 
+int dbgz_pnorm_logw(dbgz_problem *p, int precision, double *logw, double *qmc_reps) {
+  if (!p || !logw) return DBGZ_ERR_INVALID_ARGUMENT;
+  dbgz_ctx *ctx = p->ctx;
+  if (precision < DBGZ_PREC_FP64 || precision > DBGZ_PREC_FP32_SIMT)
+    return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "pnorm_logw: bad precision %d", precision);
+  cudaSetDevice(ctx->device);
+  const dbgz_opts &o = p->opts;
+  const int64_t n_reps = o.n_reps, m = o.m;
+  DBGZ_TRY(dbgz_first_dim_cdf(p));
+  if (precision != DBGZ_PREC_FP64 && !p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
+  const int64_t tps = (m + 127) / 128;
+  const int64_t n_tiles = tps * n_reps;
+  DBGZ_TRY(dbgz_ensure(ctx, p->partials, sizeof(double) * n_tiles));
+  DBGZ_TRY(dbgz_ensure(ctx, p->reps, sizeof(double) * n_reps));
+  DevBuf lw;  // one double per sample, [tile * 128 + row]; back to the pool at the end
+  struct Release {
+    DevBuf &b;
+    ~Release() { dbgz_release(b); }
+  } release_lw{lw};
+  DBGZ_TRY(dbgz_ensure(ctx, lw, sizeof(double) * (size_t)n_tiles * 128));
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(p->reps.p, 0, sizeof(double) * n_reps, ctx->stream));
+  DBGZ_CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+  PassArgs pa{};
+  pa.kind = kLoopLogWeight;
+  pa.d = p->d;
+  pa.m = m;
+  pa.n_reps = n_reps;
+  pa.sobol_first = p->sobol_first;
+  pa.n_bits = (int)o.n_bits;
+  pa.qmc_type = p->qmc_type;
+  pa.cdf_form = p->cdf_form;
+  pa.c1 = p->c1;
+  pa.dc1 = p->dc1;
+  pa.gen_base = p->gen_base;
+  pa.grad.N = n_tiles * 128;
+  pa.grad.p = (double *)lw.p;
+  pa.grad.dc1 = p->dc1;
+  const bool sparse = p->structure == DBGZ_STRUCTURE_SPARSE;
+  const bool tensor = !sparse && (precision == DBGZ_PREC_FP32_TF32 || precision == DBGZ_PREC_FP32_SPLIT_BF16);
+  if (sparse)
+    DBGZ_TRY(dbgz_loop_sparse(p, pa, precision, (double *)p->partials.p, n_tiles));
+  else if (tensor)
+    DBGZ_TRY(dbgz_loop_umma(p, pa, precision, (double *)p->partials.p, n_tiles));
+  else
+    DBGZ_TRY(dbgz_loop_simt(p, pa, precision, (double *)p->partials.p, n_tiles));
+  DBGZ_TRY(dbgz_finalize_pass(p, (const double *)p->partials.p, tps, 0, m, (double *)p->reps.p));
+  // the shift-major tile order gives point j of shift k at k * tps * 128 + j
+  DBGZ_CUDA_TRY(ctx, cudaMemcpy2DAsync(logw, sizeof(double) * (size_t)m, lw.p, sizeof(double) * (size_t)tps * 128,
+                                       sizeof(double) * (size_t)m, (size_t)n_reps, cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+  std::vector<double> reps(n_reps);
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(reps.data(), p->reps.p, sizeof(double) * n_reps, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+  int dev_status = 0;
+  DBGZ_CUDA_TRY(ctx, cudaMemcpyAsync(&dev_status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  DBGZ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (dev_status != 0)
+    return dbgz_fail(ctx, DBGZ_ERR_TIMEOUT, "pnorm_logw: a bounded wait in the tensor-core loop gave up");
+  if (qmc_reps) std::memcpy(qmc_reps, reps.data(), sizeof(double) * n_reps);
+  return DBGZ_OK;
+}
+
 }  // extern "C"

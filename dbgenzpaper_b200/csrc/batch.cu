@@ -422,7 +422,7 @@ int plan_setup(dbgz_batch_plan *P, const dbgz_opts &o, const uint32_t *dirnums, 
     S.gen.n_bits = P->n_bits;
     S.gen.gen_base = 0;
     S.gen.sobol_first = P->sobol_first;
-    S.gen.sobol_tile128 = P->qmc_type == DBGZ_QMC_SOBOL && P->sobol_first % 128 == 0;  // tiles start at multiples of 128
+    S.gen.sobol_staged = P->qmc_type == DBGZ_QMC_SOBOL;
     S.gen.q = P->dq;
     S.gen.shift64 = P->dsh64 + B.offs;
     S.gen.shift32 = P->dsh32 + B.offs;

@@ -90,6 +90,106 @@ k_genz_block_smem(double *M, int64_t n, double *a, double *b, double *dvec, doub
   cholk::genz_block_smem(M, n, a, b, dvec, svec, perm, i0, i1, ii1, eps0_ptr, rank, genz_sh);
 }
 
+// One bs1 block of cholesky_rowmax! (src/cholesky.jl:290-357), one CTA: the
+// pivot is the largest remaining diagonal of the panel (first on ties, NaN
+// never chosen unless it is the current row's own), the rank test m_ii > 0
+// comes before the swap, a and b are not swapped.  The same operations in
+// the same order as the checker's restatement.
+__global__ void __launch_bounds__(kStepThreads)
+k_rowmax_block(double *M, int64_t n, double *dvec, int64_t *perm, int64_t i0, int64_t i1, int64_t ii1,
+               int64_t *rank) {
+  __shared__ double red_v[32];
+  __shared__ int64_t red_i[32];
+  __shared__ int64_t sh_im;
+  __shared__ double sh_mii;
+  __shared__ int sh_stop;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (rank[0] < n) return;
+  for (int64_t k = i0 + tid; k <= ii1; k += blockDim.x) dvec[k] = 0.0;
+  __syncthreads();
+  // larger wins; equal values keep the smaller index; NaN (INT64_MAX index) never wins
+  auto better = [](double v2, int64_t i2, double v, int64_t i) {
+    if (i2 == INT64_MAX) return false;
+    if (i == INT64_MAX) return true;
+    return v2 > v || (v2 == v && i2 < i);
+  };
+  for (int64_t i = i0; i <= i1; ++i) {
+    double bv = 0.0;
+    int64_t bi = INT64_MAX;
+    for (int64_t k = i + tid; k <= ii1; k += blockDim.x) {
+      const double v = dm_sub(M[k * n + k], dvec[k]);
+      if (v == v && better(v, k, bv, bi)) { bv = v; bi = k; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double v2 = __shfl_down_sync(0xffffffffu, bv, off);
+      const int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
+      if (lane + off < 32 && better(v2, i2, bv, bi)) { bv = v2; bi = i2; }
+    }
+    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double v = red_v[0];
+      int64_t im = red_i[0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+        if (better(red_v[w], red_i[w], v, im)) { v = red_v[w]; im = red_i[w]; }
+      const double m_own = dm_sub(M[i * n + i], dvec[i]);
+      if (m_own != m_own || im == INT64_MAX) im = i;  // the scan starts from row i's own value
+      double m_ii = dm_sub(M[im * n + im], dvec[im]);
+      int stop = 0;
+      if (m_ii > 0) {
+        m_ii = dm_sqrt(m_ii);
+      } else {
+        rank[0] = i;  // 0-based i == the reference's i - 1
+        stop = 1;
+      }
+      if (!stop && im != i) {
+        const int64_t tp = perm[i]; perm[i] = perm[im]; perm[im] = tp;
+        const double t = dvec[im]; dvec[im] = dvec[i]; dvec[i] = t;
+      }
+      sh_im = im;
+      sh_mii = m_ii;
+      sh_stop = stop;
+    }
+    __syncthreads();
+    if (sh_stop) return;
+    const int64_t im = sh_im;
+    if (im != i) {  // rows over columns i0..n, then full columns
+      for (int64_t k = i0 + tid; k < n; k += blockDim.x) {
+        const double t = M[k * n + i];
+        M[k * n + i] = M[k * n + im];
+        M[k * n + im] = t;
+      }
+      __syncthreads();
+      for (int64_t k = tid; k < n; k += blockDim.x) {
+        const double t = M[i * n + k];
+        M[i * n + k] = M[im * n + k];
+        M[im * n + k] = t;
+      }
+      __syncthreads();
+    }
+    const double m_ii = sh_mii;
+    if (tid == 0) M[i * n + i] = m_ii;
+    if (i == i0) {
+      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
+        const double m_ij = dm_div(M[j * n + i], m_ii);
+        M[j * n + i] = m_ij;
+        M[i * n + j] = m_ij;
+        dvec[j] = dm_add(dvec[j], dm_mul(m_ij, m_ij));
+      }
+    } else if (i < ii1) {
+      for (int64_t j = i + 1 + tid; j <= ii1; j += blockDim.x) {
+        double acc = 0.0;
+        for (int64_t l = i0; l <= i - 1; ++l) acc = dm_fma(M[l * n + j], M[i * n + l], acc);
+        const double m_ij = dm_div(dm_sub(M[i * n + j], acc), m_ii);
+        M[j * n + i] = m_ij;
+        M[i * n + j] = m_ij;
+        dvec[j] = dm_add(dvec[j], dm_mul(m_ij, m_ij));
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // C[j,k] -= sum_{l=p0..p1} A(l,j) B(l,k) over [c0, c1]^2, one tile per CTA.
 constexpr int kTile = cholk::kTile;
 __global__ void __launch_bounds__(256)
@@ -362,6 +462,68 @@ int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b
     cudaError_t e = cudaMemcpyAsync(rank_host, rank, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "cholesky_genz: %s", cudaGetErrorString(e));
+  }
+  cudaStreamSynchronize(st);
+  dbgz_release(work);
+  return rc;
+}
+
+// cholesky_rowmax! (src/cholesky.jl:244-432) on the device: the Genz
+// driver's block structure with the diagonal-pivoting block step.
+int dbgz_chol_rowmax_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b, int64_t bs1, int64_t bs2,
+                         int64_t bs3, int64_t bs4, int64_t *perm, double *scale, int64_t *rank_host) {
+  if (bs1 < 1 || bs2 < 1 || bs3 < 1 || bs4 < 1)
+    return dbgz_fail(ctx, DBGZ_ERR_INVALID_ARGUMENT, "block sizes must be positive");
+  DevBuf work;
+  DBGZ_TRY(dbgz_ensure(ctx, work, sizeof(double) * (n + 1) + sizeof(int64_t) * 2));
+  double *dvec = (double *)work.p;
+  int64_t *rank = (int64_t *)(dvec + n + 1);
+  cudaStream_t st = ctx->stream;
+  cudaMemsetAsync(dvec, 0, sizeof(double) * n, st);
+  int rc = scale_correlation(ctx, M, n, a, b, scale, 1);
+  if (rc) {
+    dbgz_release(work);
+    return rc;
+  }
+  {
+    std::vector<int64_t> id(n);
+    for (int64_t i = 0; i < n; ++i) id[i] = i;
+    cudaMemcpyAsync(perm, id.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st);
+    int64_t rn = n;
+    cudaMemcpyAsync(rank, &rn, sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+  }
+  for (int64_t iv0 = 0; iv0 < n && rc == DBGZ_OK; iv0 += bs4) {
+    int64_t iv1 = std::min(n - 1, iv0 + bs4 - 1);
+    for (int64_t iii0 = iv0; iii0 <= iv1 && rc == DBGZ_OK; iii0 += bs3) {
+      int64_t iii1 = std::min(iv1, iii0 + bs3 - 1);
+      for (int64_t ii0 = iii0; ii0 <= iii1 && rc == DBGZ_OK; ii0 += bs2) {
+        int64_t ii1 = std::min(iii1, ii0 + bs2 - 1);
+        for (int64_t i0 = ii0; i0 <= ii1 && rc == DBGZ_OK; i0 += bs1) {
+          int64_t i1 = std::min(ii1, i0 + bs1 - 1);
+          k_rowmax_block<<<1, kStepThreads, 0, st>>>(M, n, dvec, perm, i0, i1, ii1, rank);
+          dbgz_count_launch(ctx);
+          if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1);
+        }
+        if (ii1 < iii1 && rc == DBGZ_OK) {
+          rc = launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1);
+          if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0);
+        }
+      }
+      if (iii1 < iv1 && rc == DBGZ_OK) {
+        rc = launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1);
+        if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0);
+      }
+    }
+    if (iv1 < n - 1 && rc == DBGZ_OK) {
+      rc = launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1);
+      if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0);
+    }
+  }
+  if (rc == DBGZ_OK) {
+    cudaError_t e = cudaMemcpyAsync(rank_host, rank, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "cholesky_rowmax: %s", cudaGetErrorString(e));
   }
   cudaStreamSynchronize(st);
   dbgz_release(work);

@@ -15,16 +15,18 @@
 //   dP/dSigma_ij = G_ij / (s_i s_j)                                  (i != j)
 //   dP/dSigma_ii = (G_ii - sum_j G_ij R_ij - (abar'' a'' + bbar'' b'')/2) / s_i^2
 // where abar''_t = dP/da_{pi t} * s_{pi t} is the gradient with respect to
-// the scaled bound.  Dense FP64 linear algebra (TRMM, two TRSMs, one GEMM)
-// is cuBLAS on the context's stream; the rest are small kernels here.
-#include <cublas_v2.h>
-
+// the scaled bound.  The dense FP64 linear algebra runs in this library's own
+// kernels (dense64.cuh) on the context's stream:
+//   M = Phi(U Ubar')            one GEMM over k >= max(i, j), lower triangle
+//                               written with the halved diagonal;
+//   V = U^-1                    triangular inverse;
+//   S = (V M) V'                two GEMMs over the triangles' nonzero blocks;
+//   R = U'U                     one GEMM over k <= min(i, j).
 #include <cmath>
 #include <vector>
 
+#include "dense64.cuh"
 #include "internal.cuh"
-
-int dbgz_get_cublas(dbgz_ctx *ctx, cublasHandle_t *out);  // grad.cu
 
 namespace {
 
@@ -35,15 +37,6 @@ __global__ void k_adj_prepare(const double *U, const double *Ubar, int64_t d, do
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < d; i += (int64_t)gridDim.x * blockDim.x) {
     Uc[j * d + i] = i <= j ? U[j * d + i] : 0.0;
     T1[j * d + i] = i >= j ? Ubar[i * d + j] : 0.0;  // T1[i, j] = Ubar[j, i]
-  }
-}
-
-// M <- Phi(M): lower triangle, diagonal halved, upper triangle zero
-__global__ void k_adj_phi(double *M, int64_t d) {
-  const int64_t j = blockIdx.y;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < d; i += (int64_t)gridDim.x * blockDim.x) {
-    double &v = M[j * d + i];
-    v = i > j ? v : (i == j ? 0.5 * v : 0.0);
   }
 }
 
@@ -95,36 +88,52 @@ int dbgz_sigma_adjoint_dev(dbgz_problem *p, const double *dU, const double *da, 
   const size_t nn = (size_t)d * d;
   cudaStream_t st = ctx->stream;
   DevBuf w;
-  DBGZ_TRY(dbgz_ensure(ctx, w, 8 * (4 * nn + (size_t)d) + 4096));
-  double *Uc = (double *)w.p, *T1 = Uc + nn, *M = T1 + nn, *R = M + nn, *r = R + nn;
+  DBGZ_TRY(dbgz_ensure(ctx, w, 8 * (6 * nn + (size_t)d) + 4096));
+  double *Uc = (double *)w.p, *T1 = Uc + nn, *M = T1 + nn, *R = M + nn, *V = R + nn, *X = V + nn, *r = X + nn;
   int rc = DBGZ_OK;
   do {
-    cublasHandle_t h;
-    if ((rc = dbgz_get_cublas(ctx, &h))) break;
     const dim3 g2((unsigned)((d + 255) / 256), (unsigned)d);
     k_adj_prepare<<<g2, 256, 0, st>>>((const double *)p->U.p, dU, d, Uc, T1);
     dbgz_count_launch(ctx);
-    const double one = 1.0, zero = 0.0;
-    const int n = (int)d;
-    cublasStatus_t cs;
-    // M = U Ubar'
-    cs = cublasDtrmm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n, &one, Uc,
-                     n, T1, n, M, n);
-    if (cs == CUBLAS_STATUS_SUCCESS) {
-      k_adj_phi<<<g2, 256, 0, st>>>(M, d);
-      dbgz_count_launch(ctx);
-      // S = U^-1 Phi(M) U^-T, in place
-      cs = cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n, &one,
-                       Uc, n, M, n);
+    int nl = 0;
+    // M's tiles strictly above the diagonal are not written by the first GEMM
+    cudaError_t ce = cudaMemsetAsync(M, 0, 8 * nn, st);
+    dense64::GemmArgs g;
+    // M = Phi(Uc T1): Uc[i,k] = 0 for k < i, T1[k,j] = 0 for k < j
+    g.m = g.n = g.k = d;
+    g.A = Uc; g.lda = d; g.B = T1; g.ldb = d; g.C = M; g.ldc = d;
+    g.kmin_row = g.kmin_col = 1;
+    g.out = dense64::kOutLowerPhi;
+    if (ce == cudaSuccess) ce = dense64::gemm64<false, false>(g, st, &nl);
+    // V = U^-1
+    if (ce == cudaSuccess) ce = dense64::trinv64(Uc, d, V, st, &nl);
+    // X = V M: V[i,k] = 0 for k < i, M[k,j] = 0 for k < j
+    if (ce == cudaSuccess) {
+      g = dense64::GemmArgs{};
+      g.m = g.n = g.k = d;
+      g.A = V; g.lda = d; g.B = M; g.ldb = d; g.C = X; g.ldc = d;
+      g.kmin_row = g.kmin_col = 1;
+      ce = dense64::gemm64<false, false>(g, st, &nl);
     }
-    if (cs == CUBLAS_STATUS_SUCCESS)
-      cs = cublasDtrsm(h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, n, n, &one,
-                       Uc, n, M, n);
-    // R = U' U, the permuted correlation matrix
-    if (cs == CUBLAS_STATUS_SUCCESS)
-      cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, Uc, n, Uc, n, &zero, R, n);
-    if (cs != CUBLAS_STATUS_SUCCESS) {
-      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "sigma_adjoint: cuBLAS failed (%d)", (int)cs);
+    // S = X V' (into M): V'[k,j] = V[j,k] = 0 for k < j
+    if (ce == cudaSuccess) {
+      g = dense64::GemmArgs{};
+      g.m = g.n = g.k = d;
+      g.A = X; g.lda = d; g.B = V; g.ldb = d; g.C = M; g.ldc = d;
+      g.kmin_col = 1;
+      ce = dense64::gemm64<false, true>(g, st, &nl);
+    }
+    // R = Uc' Uc, the permuted correlation matrix: Uc[k,i] = 0 for k > i
+    if (ce == cudaSuccess) {
+      g = dense64::GemmArgs{};
+      g.m = g.n = g.k = d;
+      g.A = Uc; g.lda = d; g.B = Uc; g.ldb = d; g.C = R; g.ldc = d;
+      g.kmax_row = g.kmax_col = 1;
+      ce = dense64::gemm64<true, false>(g, st, &nl);
+    }
+    for (int i = 0; i < nl; ++i) dbgz_count_launch(ctx);
+    if (ce != cudaSuccess) {
+      rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "sigma_adjoint: dense kernel launch failed (%s)", cudaGetErrorString(ce));
       break;
     }
     k_adj_rowsum<<<(unsigned)((d + 127) / 128), 128, 0, st>>>(M, R, d, r);

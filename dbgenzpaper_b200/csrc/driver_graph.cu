@@ -108,9 +108,6 @@ std::vector<uint64_t> signature(const dbgz_problem *p, int precision, const Pass
                           &p->partials, &p->reps, &p->drv_state, &p->q,          &p->shifts,      &p->shifts32,
                           &p->V,      &p->ushifts, &p->tgt32,     &p->tgt64,      &p->csc_colptr,  &p->csc_row,
                           &p->csc_val64, &p->csc_val32};
-  // Sobol points from the staged per-block tables only from a 128-aligned
-  // first index
-  s.push_back((uint64_t)((pa.sobol_first + pa.gen_base) % 128 == 0));
   for (const DevBuf *b : bufs) {
     addp(b->p);
     s.push_back((uint64_t)b->bytes);

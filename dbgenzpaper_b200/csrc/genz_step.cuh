@@ -52,14 +52,13 @@ struct GenParams {
   const uint32_t *V;     // Sobol direction numbers (d-1) x 32
   const uint64_t *ushift;// (d-1) x n_reps
   const int64_t *gen_base_dev;  // when set, gen_base is read from here (device-driven passes)
-  // Sobol, nonzero when every tile starts at a multiple of 128 (the pass's
-  // first index sobol_first + gen_base is one): the integer of index
-  // base + r (r < 128) is x(base) ^ XOR_{k<7} [bit k of gray(r)] V[k], since
-  // gray(base + r) = gray(base) ^ gray(r) and the integer is linear in the
-  // Gray code's bits.  Loops that stage x(base) and V[0..6] per block pass the
-  // integer in, already XORed with the shift's low 32 bits (n_bits <= 32:
-  // the shift enters only there); zero: sobol_warp and the shift per step
-  int sobol_tile128;
+  // Sobol, nonzero when the loop stages the integers of each block of
+  // dimensions per tile (sobol_stage_block) and passes the point's integer,
+  // already XORed with the shift's low 32 bits (n_bits <= 32: the shift
+  // enters only there), into the step; zero: sobol_warp and the shift per
+  // step.  Any first index: a tile's 128 points need the integers of 5
+  // multiples of 32 and the terms of a 5-bit Gray code (SobolLane).
+  int sobol_staged;
 };
 
 // Gray-code Sobol integer of point index idx in dimension l, computed by
@@ -87,65 +86,86 @@ __device__ __forceinline__ uint32_t sobol_warp(const uint32_t *Vl, uint64_t idx)
   return x ^ t;
 }
 
-// Staged Sobol integers for 128-sample tiles that start at a multiple of 128
-// (GenParams::sobol_tile128).  Since gray(B + i) = gray(B) ^ gray(i) when B is
-// a multiple of 2^k and i < 2^k, and the integer is linear in the Gray code's
-// bits, the integer of index base + 32 w + i (warp w of the tile, lane i) is
-//   x(base + 32 w) ^ x(gray(i) & 3) ^ x(gray(i) & 28),
-// with gray(32 w) = 32 w ^ 16 w bringing V[4..6] into the first term.  Per
-// dimension li of a block, tab[li][0..15] holds: [w] = x(base + 32 w) ^ the
-// tile's shift (low 32 bits: n_bits <= 32, so the shift enters only there),
-// [4 + a] = V[0], V[1] XORed by the bits of a, [8 + b] = V[2..4] by the bits of
-// b.  A step then reads three words (sobol_staged).
+// Staged Sobol integers of a 128-point tile with first index T (any T).
+// Write T = B + o with B a multiple of 32 and o < 32; the point of tile row
+// r < 128 has index B + 32 q + k with q = (o + r) >> 5 (0..4) and
+// k = (o + r) & 31.  Since gray(N + k) = gray(N) ^ gray(k) for N a multiple
+// of 32 and k < 32, and the integer is linear in the Gray code's bits, that
+// integer is
+//   x(B + 32 q) ^ x(gray(k) & 3) ^ x(gray(k) & 28).
+// The five bases follow from x(B) by the recurrence over consecutive
+// multiples of 32, x(32 (c + 1)) = x(32 c) ^ V[4] ^ V[5 + ctz(c + 1)]
+// (of the 32 Gray-code steps between them, V[0..3] enter an even number of
+// times, V[4] once, and the last step flips bit 5 + ctz(c + 1), which does
+// not enter the 32-bit integer when it is 32 or more).  Per dimension li of a
+// block, tab[li][0..16] holds: [q] = x(B + 32 q) ^ the tile's shift (low 32
+// bits), [5 + a] = V[0], V[1] XORed by the bits of a, [9 + b] = V[2..4] by
+// the bits of b.  A step then reads three words (SobolLane::at).
 //
 // sobol_stage_block: the 128 threads r of a tile together (all lanes of
 // their four warps), warp w filling entries 8w..8w+7 of a block of 32: entry
-// li < nv is dimension l0 + dir li when that lies in [0, lmax]; tile base
+// li < nv is dimension l0 + dir li when that lies in [0, lmax]; tile first
 // index base0, shift row ush (the shift of dimension l at ush[l]).
-__device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[16], const uint32_t *V, const uint64_t *ush,
-                                                  uint64_t base0, int64_t l0, int dir, int64_t lmax, int nv,
-                                                  int r) {
-  const uint32_t gw = (uint32_t)(base0 ^ (base0 >> 1));
+constexpr int kSobolRow = 17;  // words per staged dimension
+__device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[kSobolRow], const uint32_t *V,
+                                                  const uint64_t *ush, uint64_t base0, int64_t l0, int dir,
+                                                  int64_t lmax, int nv, int r) {
+  const uint64_t B = base0 & ~31ull;
+  const uint32_t gB = (uint32_t)(B ^ (B >> 1));
   const int wid = r >> 5, ln = r & 31;
+  // lanes 1..4: bit 5 + ctz(c + ln) of the recurrence (c = B / 32)
+  const int zb = (ln >= 1 && ln <= 4) ? 5 + __ffsll((long long)((B >> 5) + (uint64_t)ln)) - 1 : 32;
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     const int li = wid * 8 + q;
     const int64_t l = l0 + dir * li;
     const bool ok = li < nv && l >= 0 && l <= lmax;
-    // x(base): lane k contributes V[k] when bit k of gray(base) is set
+    // x(B): lane k contributes V[k] when bit k of gray(B) is set
     const uint32_t vk = ok ? __ldg(V + l * 32 + ln) : 0u;
-    uint32_t t = ((gw >> ln) & 1u) ? vk : 0u;
+    uint32_t t = ((gB >> ln) & 1u) ? vk : 0u;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) t ^= __shfl_xor_sync(0xffffffffu, t, o);
-    uint32_t v[7];
+    uint32_t v[5];
 #pragma unroll
-    for (int e = 0; e < 7; ++e) v[e] = __shfl_sync(0xffffffffu, vk, e);
-    const uint32_t sh = (ln < 4 && ok) ? (uint32_t)__ldg(ush + l) : 0u;
-    // lanes 0..3: bits 4..6 of gray(32 w) = 32 w ^ 16 w
-    const uint32_t sel = ln < 4 ? (uint32_t)((ln << 1) ^ ln) : (uint32_t)(ln < 8 ? ln - 4 : ln - 8);
+    for (int e = 0; e < 5; ++e) v[e] = __shfl_sync(0xffffffffu, vk, e);
+    // x(B + 32 ln) = x(B) ^ XOR_{s = 1..ln} (V[4] ^ V[5 + ctz(c + s)]), lanes 0..4
+    const uint32_t vz = __shfl_sync(0xffffffffu, vk, zb & 31);
+    uint32_t term = (ln >= 1 && ln <= 4) ? v[4] ^ (zb < 32 ? vz : 0u) : 0u;
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, term, o);
+      if (ln >= o) term ^= u;
+    }
+    const uint32_t sh = (ln < 5 && ok) ? (uint32_t)__ldg(ush + l) : 0u;
     uint32_t x;
-    if (ln < 4)
-      x = t ^ ((sel & 1u) ? v[4] : 0u) ^ ((sel & 2u) ? v[5] : 0u) ^ ((sel & 4u) ? v[6] : 0u) ^ sh;
-    else if (ln < 8)
-      x = ((sel & 1u) ? v[0] : 0u) ^ ((sel & 2u) ? v[1] : 0u);
-    else
-      x = ((sel & 1u) ? v[2] : 0u) ^ ((sel & 2u) ? v[3] : 0u) ^ ((sel & 4u) ? v[4] : 0u);
-    if (ln < 16) tab[li][ln] = x;
+    if (ln < 5) {
+      x = t ^ term ^ sh;
+    } else if (ln < 9) {
+      const int a = ln - 5;
+      x = ((a & 1) ? v[0] : 0u) ^ ((a & 2) ? v[1] : 0u);
+    } else {
+      const int b = ln - 9;
+      x = ((b & 1) ? v[2] : 0u) ^ ((b & 2) ? v[3] : 0u) ^ ((b & 4) ? v[4] : 0u);
+    }
+    if (ln < 17) tab[li][ln] = x;
   }
 }
 
-// The shifted integer of tile row r in block dimension li (sobol_stage_block).
+// The shifted integer of tile row r in block dimension li, for the tile
+// whose first point index is base0 (sobol_stage_block).
 struct SobolLane {
-  uint32_t w, a, b;  // warp, gray(lane) & 3, gray(lane) >> 2
-  __device__ __forceinline__ explicit SobolLane(int r) {
-    const uint32_t g = (uint32_t)((r & 31) ^ ((r & 31) >> 1));
-    w = (uint32_t)(r >> 5);
+  uint32_t q, a, b;  // base slot, gray(k) & 3, gray(k) >> 2
+  __device__ __forceinline__ SobolLane(int r, uint64_t base0) {
+    const uint32_t s = (uint32_t)(base0 & 31u) + (uint32_t)r;  // o + r < 160
+    const uint32_t k = s & 31u;
+    const uint32_t g = k ^ (k >> 1);
+    q = s >> 5;
     a = g & 3u;
     b = g >> 2;
   }
-  __device__ __forceinline__ uint32_t at(const uint32_t (*tab)[16], int li) const {
+  __device__ __forceinline__ uint32_t at(const uint32_t (*tab)[kSobolRow], int li) const {
     const uint32_t *t = tab[li];
-    return t[w] ^ t[4 + a] ^ t[8 + b];
+    return t[q] ^ t[5 + a] ^ t[9 + b];
   }
 };
 
@@ -198,9 +218,9 @@ struct StepFp64 {
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
-      const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
+      const uint32_t xw = g.sobol_staged ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
       uint64_t xi = (uint64_t)xw & mask;
-      uint64_t sh = g.sobol_tile128 ? 0ull : g.ushift[k * (d - 1) + l] & mask;
+      uint64_t sh = g.sobol_staged ? 0ull : g.ushift[k * (d - 1) + l] & mask;
       u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
     }
     u = fabs(fma(u, 2.0, -1.0));
@@ -265,15 +285,15 @@ struct StepFp32 {
       // n_bits <= 32: the shifted integer has at most 32 bits
       const int L = g.n_bits;
       const uint32_t mask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
-      const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
-      const uint32_t sh = g.sobol_tile128 ? 0u : (uint32_t)g.ushift[k * (d - 1) + l];
+      const uint32_t xw = g.sobol_staged ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
+      const uint32_t sh = g.sobol_staged ? 0u : (uint32_t)g.ushift[k * (d - 1) + l];
       sobol_tent_f32((xw ^ sh) & mask, L, w, w1);
     } else {
       const int L = g.n_bits;
       const uint64_t mask = (L >= 64) ? ~0ull : ((1ull << L) - 1);
-      const uint32_t xw = g.sobol_tile128 ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
+      const uint32_t xw = g.sobol_staged ? x0 : sobol_warp(g.V + l * 32, (uint64_t)(g.sobol_first + g.gen_base + j));
       const uint64_t xi = (uint64_t)xw & mask;
-      const uint64_t sh = g.sobol_tile128 ? 0ull : g.ushift[k * (d - 1) + l] & mask;
+      const uint64_t sh = g.sobol_staged ? 0ull : g.ushift[k * (d - 1) + l] & mask;
       const double u = (double)((xi ^ sh) & mask) * ldexp(1.0, -L);
       w = (float)fabs(fma(u, 2.0, -1.0));
       w1 = (float)(2.0 * fmin(u, 1.0 - u));

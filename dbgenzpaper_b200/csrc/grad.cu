@@ -7,13 +7,14 @@
 // factor (policies.cuh).  Per-variable terms (dP/da_t, dP/db_t, dP/dU_tt)
 // come out as per-(tile, warp) partial sums reduced here in a fixed order;
 // the off-diagonal dP/dU[l, t] = mean over samples of y_l * (p sbar_t) is one
-// plain GEMM of the two stored arrays (cuBLAS: FP64 DGEMM for the FP64 path,
-// TF32 tensor-core GEMM with FP32 accumulation for the FP32 paths).
-#include <cublas_v2.h>
-
+// GEMM of the two stored arrays over the strict upper triangle l < t (FP64:
+// dense64.cuh on CUDA cores, split over samples with the split sums added in
+// a fixed order; FP32 paths: tcgen05 TF32 with FP32 accumulation, du_gemm.cu).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
+#include "dense64.cuh"
 #include "internal.cuh"
 
 namespace {
@@ -69,32 +70,8 @@ __global__ void k_grad_assemble(const void *gemm, int esz, const double *sums, c
   }
 }
 
-struct CublasHandle {
-  cublasHandle_t h = nullptr;
-  int device = -1;
-  ~CublasHandle() {
-    if (h) cublasDestroy(h);
-  }
-};
-thread_local CublasHandle g_cublas;
-
 }  // namespace
 
-// The calling thread's cuBLAS handle for the context's device, bound to the
-// context's stream.
-int dbgz_get_cublas(dbgz_ctx *ctx, cublasHandle_t *out) {
-  if (!g_cublas.h || g_cublas.device != ctx->device) {
-    if (g_cublas.h) cublasDestroy(g_cublas.h);
-    g_cublas.h = nullptr;
-    if (cublasCreate(&g_cublas.h) != CUBLAS_STATUS_SUCCESS)
-      return dbgz_fail(ctx, DBGZ_ERR_CUDA, "cublasCreate failed");
-    g_cublas.device = ctx->device;
-  }
-  if (cublasSetStream(g_cublas.h, ctx->stream) != CUBLAS_STATUS_SUCCESS)
-    return dbgz_fail(ctx, DBGZ_ERR_CUDA, "cublasSetStream failed");
-  *out = g_cublas.h;
-  return DBGZ_OK;
-}
 
 extern "C" int dbgz_first_dim_cdf(dbgz_problem *p);  // api.cu
 
@@ -218,14 +195,33 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
     if (want_U) {
       const int nc = (int)((t1 - t0) * 128);
       if (precision == DBGZ_PREC_FP64) {
-        cublasHandle_t h;
-        DBGZ_TRY(dbgz_get_cublas(ctx, &h));
-        const double one = 1.0, beta = t0 > 0 ? 1.0 : 0.0;
-        const cublasStatus_t cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)d, (int)d, nc, &one,
-                                              (const double *)ga.y, (int)N, (const double *)ga.sbar, (int)N, &beta,
-                                              (double *)dU, (int)d);
-        if (cs != CUBLAS_STATUS_SUCCESS)
-          return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: cuBLAS GEMM failed (%d)", (int)cs);
+        // dU[l, t] (+)= sum_n Y[n, l] SB[n, t] for l < t, Y and SB the stored
+        // rows as N x d column-major matrices
+        dense64::GemmArgs g;
+        g.m = g.n = d;
+        g.k = nc;
+        g.A = (const double *)ga.y;
+        g.lda = N;
+        g.B = (const double *)ga.sbar;
+        g.ldb = N;
+        g.C = (double *)dU;
+        g.ldc = d;
+        g.out = dense64::kOutStrictUpper;
+        g.accumulate = t0 > 0;
+        // split over samples: about four CTAs per SM, at least 1024 samples each
+        const int64_t nt = (d + dense64::BM - 1) / dense64::BM;
+        const int64_t tiles = nt * (nt + 1) / 2;
+        int64_t sp = (4 * (int64_t)ctx->num_sms + tiles - 1) / tiles;
+        sp = std::max<int64_t>(1, std::min<int64_t>(sp, std::min<int64_t>(64, nc / 1024)));
+        g.splits = (int)sp;
+        DBGZ_TRY(dbgz_ensure(ctx, du_work, std::max<size_t>(8, dense64::gemm64_partial_bytes(g))));
+        g.partial = (double *)du_work.p;
+        int nl = 0;
+        const cudaError_t ce = dense64::gemm64<true, false>(g, ctx->stream, &nl);
+        for (int i = 0; i < nl; ++i) dbgz_count_launch(ctx);
+        if (ce != cudaSuccess)
+          return dbgz_fail(ctx, DBGZ_ERR_CUDA, "pnorm_grad: FP64 factor-gradient GEMM launch failed (%s)",
+                           cudaGetErrorString(ce));
       } else {
         // the strict upper triangle only, on tcgen05 (du_gemm.cu)
         DBGZ_TRY(dbgz_du_gemm_tf32(ctx, d, (const float *)ga.y, (const float *)ga.sbar, nc, (float *)dU, t0 > 0,

@@ -126,6 +126,8 @@ struct dbgz_problem {
 int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b, int64_t bs1,
                        int64_t bs2, int64_t bs3, int64_t bs4, int64_t *perm, double *scale,
                        int64_t *rank_host);
+int dbgz_chol_rowmax_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b, int64_t bs1, int64_t bs2,
+                         int64_t bs3, int64_t bs4, int64_t *perm, double *scale, int64_t *rank_host);
 int dbgz_chol_classic_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b,
                           int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4, double *scale);
 int dbgz_truncate_dev(dbgz_ctx *ctx, int64_t n, double *U, double eps_T);
@@ -142,7 +144,10 @@ int dbgz_sobol_dev(dbgz_ctx *ctx, int64_t m, int64_t dims, const uint32_t *V, in
 
 // ---- integration loop (loop_simt.cu) ---------------------------------------
 // Which sequential step the loops run (policies.cuh).
-enum LoopKind { kLoopForward = 0, kLoopForwardStore = 1, kLoopAdjoint = 2 };
+// kLoopLogWeight: a forward pass that also writes each sample's log-weight
+// log p = log dc_0 + ... + log dc_{d-1} to pa.grad.p (one double per sample,
+// [tile * 128 + row]), finite where p itself underflows
+enum LoopKind { kLoopForward = 0, kLoopForwardStore = 1, kLoopAdjoint = 2, kLoopLogWeight = 3 };
 
 // Forward state kept for the adjoint and the adjoint's outputs (device
 // arrays; element type float or double per precision).

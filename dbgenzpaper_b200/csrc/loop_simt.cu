@@ -45,9 +45,8 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.gen_base = pa.gen_base;
   P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
-  // staged Sobol integers when every tile starts at a multiple of 128
-  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && pa.kind != kLoopAdjoint &&
-                        (pa.sobol_first + pa.gen_base) % 128 == 0 && (!pa.gen_base_dev || pa.m % 128 == 0);
+  // staged Sobol integers (not in the adjoint pass)
+  P.gen.sobol_staged = pa.qmc_type == DBGZ_QMC_SOBOL && pa.kind != kLoopAdjoint;
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
   P.gen.shift32 = (const float *)p->shifts32.p;
@@ -99,6 +98,9 @@ int launch_kind(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   switch (pa.kind) {
     case kLoopForwardStore: return launch_simt<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
     case kLoopAdjoint: return launch_simt<T, pol::Adjoint<T, GEN>>(p, pa, partials, n_tiles);
+    case kLoopLogWeight:
+      return launch_simt<T, pol::Forward<T, GEN, false, typename pol::StepOf<T>::type, true>>(p, pa, partials,
+                                                                                            n_tiles);
     default: return launch_simt<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
   }
 }

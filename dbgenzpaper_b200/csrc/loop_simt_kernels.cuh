@@ -51,7 +51,7 @@ struct SimtSmem {
   } u;
   T Ublk[SB][SB + 1];         // coefficients of the sub-block (and of the cross block)
   pol::Staged<T> sg;
-  uint32_t sob[SB][16];       // Sobol integers of the sub-block (dbgz::sobol_stage_block)
+  uint32_t sob[SB][dbgz::kSobolRow];  // Sobol integers of the sub-block (dbgz::sobol_stage_block)
   double red[NT / 32];
 };
 
@@ -69,7 +69,8 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
     const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
     Policy pl;
     if (tid < TS) pl.tile_begin(P.gen, d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, P.cdf_form, P.io);
-    const dbgz::SobolLane sob_lane(r);
+    // this row's terms of the staged Sobol integers of the tile
+    const dbgz::SobolLane sob_lane(r, tid < TS ? (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)) : 0u);
 
     for (int64_t g0 = 0; g0 < nY; g0 += G) {
       const int ng = (int)(nY - g0 < (int64_t)G ? nY - g0 : (int64_t)G);
@@ -128,7 +129,7 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
         if (tid < TS) {
           pl.stage(sm.sg, P.tgt, tid, l_base, nsb);
           if constexpr (Policy::kSobolTable)
-            if (pl.gen.sobol_tile128)
+            if (pl.gen.sobol_staged)
               dbgz::sobol_stage_block(sm.sob, P.gen.V, P.gen.ushift + k * (d - 1),
                                       (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)),
                                       pl.sobol_l0(l_base), Policy::kSobolDir, d - 2, nsb, r);
@@ -142,7 +143,7 @@ __device__ __forceinline__ void simt_tile(const SimtParams<T> &P, SimtSmem<T> &s
             const int64_t l = l_base + li;
             uint32_t xs = 0u;
             if constexpr (Policy::kSobolTable)
-              if (pl.gen.sobol_tile128) xs = sob_lane.at(sm.sob, li);
+              if (pl.gen.sobol_staged) xs = sob_lane.at(sm.sob, li);
             T v = pl.emit(sm.sg, li, l, xs);
             sm.u.Ysub[li][r] = v;
             if (g0 < last_g0) Yw[l * TS + r] = v;

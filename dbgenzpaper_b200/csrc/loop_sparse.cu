@@ -84,10 +84,9 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
   int *scol = reinterpret_cast<int *>(smem_raw + ((sizeof(SlotVal<T>) * P.max_block_nnz + 15) & ~size_t(15)));
   T *ring = reinterpret_cast<T *>(scol + CB + 4);
   __shared__ pol::Staged<T> sg;
-  __shared__ uint32_t sob[Policy::kSobolTable ? CB : 1][16];  // Sobol integers of the block (dbgz::sobol_stage_block)
+  __shared__ uint32_t sob[Policy::kSobolTable ? CB : 1][dbgz::kSobolRow];  // Sobol integers of the block (dbgz::sobol_stage_block)
   __shared__ double red[TS / 32];
   const int r = threadIdx.x;
-  const dbgz::SobolLane sob_lane(r);
   const int W = P.W;
   T *yr = P.ring_in_smem ? ring : P.yglob + (int64_t)blockIdx.x * P.W * TS;
 
@@ -96,6 +95,8 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
     const int64_t j = (tile - k * P.tiles_per_shift) * TS + r;
     Policy pl;
     pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
+    // this row's terms of the staged Sobol integers of the tile
+    const dbgz::SobolLane sob_lane(r, (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)));
     int wslot = 0;  // ring slot of y-index i (i mod W)
     for (int64_t i0 = 0; i0 < P.nY; i0 += CB) {
       const int nb = (int)(P.nY - i0 < CB ? P.nY - i0 : CB);
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
       if (r <= nb) scol[r] = (int)(P.colptr[i0 + 1 + r] - p0);
       pl.stage(sg, P.tgt, r, i0, nb);
       if constexpr (Policy::kSobolTable)
-        if (pl.gen.sobol_tile128)
+        if (pl.gen.sobol_staged)
           dbgz::sobol_stage_block(sob, P.gen.V, P.gen.ushift + k * (P.d - 1),
                                   (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)), pl.sobol_l0(i0),
                                   Policy::kSobolDir, P.d - 2, nb, r);
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
         const int64_t i = i0 + li;
         uint32_t xs = 0u;
         if constexpr (Policy::kSobolTable)
-          if (pl.gen.sobol_tile128) xs = sob_lane.at(sob, li);
+          if (pl.gen.sobol_staged) xs = sob_lane.at(sob, li);
         const T y = pl.emit(sg, li, i, xs);
         yr[wslot * TS + r] = y;
         wslot = wslot + 1 == W ? 0 : wslot + 1;
@@ -275,9 +276,8 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.gen.gen_base = pa.gen_base;
   P.gen.gen_base_dev = pa.gen_base_dev;
   P.gen.sobol_first = pa.sobol_first;
-  // staged Sobol integers when every tile starts at a multiple of 128
-  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && (pa.sobol_first + pa.gen_base) % 128 == 0 &&
-                        (!pa.gen_base_dev || pa.m % 128 == 0);
+  // staged Sobol integers
+  P.gen.sobol_staged = pa.qmc_type == DBGZ_QMC_SOBOL;
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
   P.gen.shift32 = (const float *)p->shifts32.p;
@@ -335,6 +335,9 @@ static int launch_sparse_kind(dbgz_problem *p, const PassArgs &pa, double *parti
   switch (pa.kind) {
     case kLoopForwardStore: return launch_sparse<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
     case kLoopAdjoint: return launch_sparse<T, pol::Adjoint<T, GEN>>(p, pa, partials, n_tiles);
+    case kLoopLogWeight:
+      return launch_sparse<T, pol::Forward<T, GEN, false, typename pol::StepOf<T>::type, true>>(p, pa, partials,
+                                                                                              n_tiles);
     default: return launch_sparse<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
   }
 }

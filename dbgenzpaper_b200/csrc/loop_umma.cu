@@ -118,7 +118,7 @@ struct Smem {
   static __host__ __device__ int bbytes(int P) { return bpart(P) * Fmt<MODE>::NPART; }
   static __host__ __device__ int off_b(int) { return 2 * ABYTES; }
   static __host__ __device__ int off_misc(int P) { return 2 * ABYTES + 2 * bbytes(P); }
-  static constexpr int MISC = 15360;  // two CTAs per SM: 2 x (total + 1 KB) <= 228 KB
+  static constexpr int MISC = 15872;  // two CTAs per SM: 2 x (total + 1 KB) <= 228 KB
   static __host__ __device__ int total(int P) { return off_misc(P) + MISC + 1024; }
 };
 
@@ -134,7 +134,7 @@ struct Misc {
   int abort;
   // Sobol integers of the block's dimensions (dbgz::sobol_stage_block); last,
   // so that kernels that do not stage them are launched without it
-  uint32_t sob[2][BK][16];
+  uint32_t sob[2][BK][dbgz::kSobolRow];
 };
 static_assert(sizeof(Misc) <= Smem<DBGZ_PREC_FP32_TF32>::MISC, "shared scalars exceed their budget");
 // dynamic shared memory of a launch: the Sobol staging only where it is used
@@ -400,7 +400,6 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
     uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
     const bool need_ws = !BATCH && nphase1 > 1;
     uint32_t blk = 0;  // blocks run by this CTA (selects the staging buffer)
-    const dbgz::SobolLane sob_lane(r);  // this row's terms of the staged Sobol integers
     for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles; it += gridDim.x) {
       const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
       const int64_t tile = BATCH ? (int64_t)P.item_tile[it] : it;
@@ -418,6 +417,8 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         pl.tile_begin(pb->gen, dI, tile, tpsI, r, pb->first[0], pb->first[1], pb->first[2], 0, P.io);
       else
         pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
+      // this row's terms of the staged Sobol integers of the tile
+      const dbgz::SobolLane sob_lane(r, (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)));
       // asynchronous staging of one block into buffer `buf` (one commit group)
       auto stage_block = [&](int buf, int64_t lb, int nv) {
         for (int e = r; e < BK * BK; e += TS) {
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         }
         pl.stage_async(ms->sg[buf], tgtI, r, lb, nv);
         if constexpr (Policy::kSobolTable)
-          if (pl.gen.sobol_tile128)
+          if (pl.gen.sobol_staged)
             dbgz::sobol_stage_block(ms->sob[buf], pl.gen.V, pl.gen.ushift + pl.k * (dI - 1),
                                     (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)), pl.sobol_l0(lb),
                                     Policy::kSobolDir, dI - 2, nv, r);
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                   const int64_t l = lbase + li;
                   uint32_t xs = 0u;
                   if constexpr (Policy::kSobolTable)
-                    if (pl.gen.sobol_tile128) xs = sob_lane.at(ms->sob[cur], li);
+                    if (pl.gen.sobol_staged) xs = sob_lane.at(ms->sob[cur], li);
                   y = pl.emit_k(sgc, li, l, k, xs);
                   const float4 *urow = reinterpret_cast<const float4 *>(&ublk[li][8 * ch]);
                   const float4 u0 = urow[0], u1 = urow[1];
@@ -650,6 +651,7 @@ auto pick_kind(const PassArgs &pa) -> decltype(&k_genz_umma<MODE, pol::Forward<f
   switch (pa.kind) {
     case kLoopForwardStore: return k_genz_umma<MODE, pol::Forward<float, GEN, true>>;
     case kLoopAdjoint: return k_genz_umma<MODE, pol::Adjoint<float, GEN>>;
+    case kLoopLogWeight: return k_genz_umma<MODE, pol::Forward<float, GEN, false, dbgz::StepFp32, true>>;
     default: return k_genz_umma<MODE, pol::Forward<float, GEN, false>>;
   }
 }
@@ -721,10 +723,8 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   P.gen.n_bits = pa.n_bits;
   P.gen.gen_base = pa.gen_base;
   P.gen.gen_base_dev = pa.gen_base_dev;
-  // Sobol points from the 128-index table when every tile starts at a
-  // multiple of 128 (also in device-driven passes: m a multiple of 128)
-  P.gen.sobol_tile128 = pa.qmc_type == DBGZ_QMC_SOBOL && !adj && (pa.sobol_first + pa.gen_base) % 128 == 0 &&
-                        (!pa.gen_base_dev || pa.m % 128 == 0);
+  // Sobol points from the per-block staged integers (forward passes)
+  P.gen.sobol_staged = pa.qmc_type == DBGZ_QMC_SOBOL && !adj;
   P.gen.sobol_first = pa.sobol_first;
   P.gen.q = (const double *)p->q.p;
   P.gen.shift64 = (const double *)p->shifts.p;
@@ -861,8 +861,7 @@ int setup_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A, UmmaBatchPlan *B) {
     D.gen.shift32 = A.dsh32 ? A.dsh32 + A.offs[k] : nullptr;
     D.gen.V = A.dV;
     D.gen.ushift = A.dush ? A.dush + A.offs[k] : nullptr;
-    // every tile starts at a multiple of 128 when the first index does
-    D.gen.sobol_tile128 = A.qmc_type == DBGZ_QMC_SOBOL && A.sobol_first % 128 == 0;
+    D.gen.sobol_staged = A.qmc_type == DBGZ_QMC_SOBOL;
     D.U32 = A.dU32 + A.off2[k];
     D.tgt = A.dt32 + A.off1[k];
     D.first = A.dfirst + 3 * k;

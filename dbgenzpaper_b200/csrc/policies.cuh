@@ -120,10 +120,12 @@ struct StepOf<float> {
 };
 
 // ---------------------------------------------------------------- forward ---
-template <typename T, int GEN, bool STORE, typename Step = typename StepOf<T>::type>
+// LOGW: also sum log dc over the sample's variables and write the sum (the
+// sample's log-weight) to io.p at the tile's end (kLoopLogWeight)
+template <typename T, int GEN, bool STORE, typename Step = typename StepOf<T>::type, bool LOGW = false>
 struct Forward {
   static constexpr bool kPlain = !STORE;  // a forward pass that keeps no state
-  // takes staged Sobol integers (GenParams::sobol_tile128); not in the pass
+  // takes staged Sobol integers (GenParams::sobol_staged); not in the pass
   // that keeps the state for the adjoint (measured on the banded d = 10^4,
   // bandwidth 64 workload at 2^14 x 10 Sobol points:
   // the gradient call 125.1 ms without, 136.9 ms with them)
@@ -132,6 +134,7 @@ struct Forward {
   static constexpr int kSobolDir = 1;
   __device__ __forceinline__ int64_t sobol_l0(int64_t lbase) const { return lbase; }
   Step st;
+  double lw;  // LOGW: log of the weight so far
   dbgz::GenParams gen;
   int64_t j, k, g;  // point index in the pass, shift, global sample index
   int64_t d;
@@ -143,7 +146,7 @@ struct Forward {
                                              double up1, int cdf_form_, const GradIO<T> &io_) {
     gen = gp;
     gen.qmc_type = GEN;
-    if (!kSobolTable) gen.sobol_tile128 = 0;  // points from sobol_warp whatever the launch says
+    if (!kSobolTable) gen.sobol_staged = 0;  // points from sobol_warp whatever the launch says
     if (gp.gen_base_dev) gen.gen_base = *gp.gen_base_dev;
     d = d_;
     k = tile / tiles_per_shift;
@@ -152,6 +155,7 @@ struct Forward {
     cdf_form = cdf_form_;
     io = io_;
     st.init(c1, dc1, up1);
+    if (LOGW) lw = log(dc1);
   }
   // cooperative: r in [0, 128)
   __device__ __forceinline__ void stage(Staged<T> &sg, const typename TgtT<T>::type *tgt, int r,
@@ -176,7 +180,7 @@ struct Forward {
     }
   }
   // xs: the Sobol integer of this point in dimension l when the loop stages
-  // them (GenParams::sobol_tile128), else unused
+  // them (GenParams::sobol_staged), else unused
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
     const T y = st.template quantile<!STORE>(gen, d, j, k, l, sg.qv[li], sg.shv[li], xs);
     if (STORE) io.y[io.at(l, g)] = y;
@@ -191,6 +195,7 @@ struct Forward {
   __device__ __forceinline__ void consume(const Staged<T> &sg, T s, int li, int64_t l) {
     const auto tg = sg.tg[li];
     st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
+    if (LOGW) lw += log((double)st.dc);
     if (STORE) {
       io.s[io.at(l + 1, g)] = s;
       io.dc[io.at(l + 1, g)] = (T)st.dc;
@@ -199,6 +204,7 @@ struct Forward {
   // value of this sample added to the tile's sum of p
   __device__ __forceinline__ double tile_value(bool valid) {
     if (STORE) io.p[g] = valid ? st.p : 0.0;
+    if (LOGW) io.p[g] = valid ? lw : -INFINITY;
     return valid ? st.p : 0.0;
   }
   __device__ __forceinline__ void tile_end(const typename TgtT<T>::type *, int, int, int64_t, bool) {}
@@ -215,7 +221,7 @@ __device__ __forceinline__ float tf32_rn(float x) {
 template <typename T, int GEN>
 struct Adjoint {
   static constexpr bool kPlain = false;
-  // takes staged Sobol integers (GenParams::sobol_tile128) where the loop
+  // takes staged Sobol integers (GenParams::sobol_staged) where the loop
   // stages them; the QMC dimension of step li of a block: d - 1 - lbase - li
   static constexpr bool kSobolTable = GEN == DBGZ_QMC_SOBOL;
   static constexpr int kSobolDir = -1;
@@ -237,7 +243,7 @@ struct Adjoint {
                                              const GradIO<T> &io_) {
     gen = gp;
     gen.qmc_type = GEN;
-    if (!kSobolTable) gen.sobol_tile128 = 0;
+    if (!kSobolTable) gen.sobol_staged = 0;
     if (gp.gen_base_dev) gen.gen_base = *gp.gen_base_dev;
     d = d_;
     tile = tile_;
@@ -440,7 +446,7 @@ struct Adjoint {
   __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc, uint32_t xs) {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_tile128 != 0) : 0.0;
+    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_staged != 0) : 0.0;
     if (sizeof(T) == 4) {
       float fa, fb, fu;
       const float sb = variable32(sg.tg[li], (float)w, has_u, (float)y, (float)s, (float)dc, true, fa, fb, fu);
@@ -497,7 +503,7 @@ struct Adjoint {
     if (sizeof(T) != 4) return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk], xs);
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_tile128 != 0) : 0.0;
+    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_staged != 0) : 0.0;
     float fa, fb, fu;
     const float sb = variable32(sg.tg[li], (float)w, has_u, (float)pre_y[kk], (float)pre_s[kk],
                                 (float)pre_dc[kk], true, fa, fb, fu);

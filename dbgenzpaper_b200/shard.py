@@ -29,7 +29,10 @@ def shift_block(rank: int, world: int, n_reps_total: int) -> tuple[int, int]:
 def combine(reps: np.ndarray) -> tuple[float, float]:
     """Mean over shifts and 3*SEM, exactly as qmc_pnorm! forms them."""
     n = reps.size
-    result = float(np.sum(reps) / n)
+    total = 0.0
+    for v in reps:  # in shift order, as sum(D.qmc_reps) over a short vector
+        total += float(v)
+    result = total / n
     acc = 0.0
     for v in reps:
         acc += (v - result) ** 2 / n

@@ -150,9 +150,12 @@ int dbgz_get_profile(const dbgz_ctx *ctx, dbgz_profile *out);
  *              (src/qmc_generators.jl:63); sobol_dirnums is (d-1) x 32
  *              direction numbers v_k of each dimension as 32-bit integers
  *              (row per dimension), or NULL for the library's own table
- *              (dbgz_sobol_dirnums); sobol_first is the index of the first
- *              point of the first pass (skip0 + 1 when the caller skipped
- *              skip0 points as SobolQMC does with skip0 = 2m-1).
+ *              (dbgz_sobol_dirnums); sobol_first is the Gray-code index
+ *              (0 = the all-zero point) of the first point of the first
+ *              pass: the number of next! calls the caller's SobolSeq has
+ *              made, plus one.  SobolQMC's skip(SobolSeq(d), 2m-1) makes
+ *              2^floor(log2(2m)) of them (Sobol.jl's skip with exact =
+ *              false), so its first point is 2^floor(log2(2m)) + 1.
  * The problem keeps its own generator position: like the reference's
  * QMCData, a second dbgz_pnorm on the same problem continues from the
  * points the previous call ended on (src/qmc.jl:836). */
@@ -190,6 +193,19 @@ int dbgz_problem_factor(const dbgz_problem *p, double *U, int64_t *perm, double 
  * (length n_reps, may be NULL) receives the per-shift running means. */
 int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err,
                int64_t *n_pts, double *qmc_reps);
+
+/* Per-sample log-weights of one pass (no reference counterpart: a view of
+ * the estimator of qmc_loop!, src/qmc.jl:315-444, whose weight is
+ * p = dc_1 dc_2 ... dc_d, src/qmc.jl:405-429).  Runs one pass of m points x
+ * n_reps shifts at the problem's current generator position -- the points
+ * the next dbgz_pnorm pass would take; the position does not advance -- and
+ * writes log p of every sample, the sum of log dc over its variables in
+ * FP64, to logw (m x n_reps, column-major: point j of shift k at
+ * logw[k * m + j]).  The log-weights stay finite where p underflows to 0
+ * (for example 1000 bounds at marginal probabilities 1e-3..1e-1), so the
+ * estimate can be compared between precisions in log space.  qmc_reps
+ * (n_reps, may be NULL) receives the pass's per-shift means of p. */
+int dbgz_pnorm_logw(dbgz_problem *p, int precision, double *logw, double *qmc_reps);
 
 /* dbgz_pnorm with the adaptive loop driven on the device: one CUDA graph
  * launch per call runs every pass -- a conditional while node whose body is
@@ -344,6 +360,33 @@ int dbgz_cholesky_genz(dbgz_ctx *ctx, int64_t d, double *M, double *a, double *b
 int dbgz_cholesky_classic(dbgz_ctx *ctx, int64_t d, double *M, double *a, double *b,
                           int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
                           double *scale_vec);
+
+/* cholesky_rowmax!(M, a, b, bs1, bs2, bs3, bs4) (src/cholesky.jl:244-432):
+ * Cholesky with diagonal pivoting (the largest remaining diagonal of the
+ * bs2 panel, first on ties) on the GPU, with cholesky_genz!'s block
+ * structure and arithmetic contract.  Host arrays in/out as in
+ * dbgz_cholesky_genz: M (d x d, correlation-scaled then factored in place,
+ * upper triangle = U), a and b scaled by 1/sqrt(Sigma_ii) but not permuted
+ * (as the reference leaves them), perm (0-based), scale_vec, and rank: the
+ * first row whose remaining diagonal is not positive (d when none).  Not
+ * called by qmc_pnorm!. */
+int dbgz_cholesky_rowmax(dbgz_ctx *ctx, int64_t d, double *M, double *a, double *b, int64_t bs1,
+                         int64_t bs2, int64_t bs3, int64_t bs4, int64_t *perm, double *scale_vec,
+                         int64_t *rank);
+
+/* adapt_low_rank!(M, a, b, rank, perm, eps1) (src/cholesky.jl:24-123):
+ * for a factor of rank r (M: nr x n, column-major; columns r+1..n hold the
+ * dependent variables' coefficients in rows 1..r), every dependent column
+ * with no entry above eps1 in rows 1..r moves to the end; every other is
+ * scaled by its last such entry (its level i_j; a and b are scaled with it
+ * and swapped when that entry is negative) and placed at the end of the
+ * block of level i_j.  Host arrays, updated in place: M, a, b, perm
+ * (0-based indices).  k_js (length rank) receives the blocks' 1-based end
+ * positions and *k_0 the number of columns moved to the end.  The levels are
+ * found on the device and the columns written to their final places by one
+ * gather; the values are the reference's. */
+int dbgz_adapt_low_rank(dbgz_ctx *ctx, int64_t nr, int64_t n, double *M, double *a, double *b,
+                        int64_t rank, int64_t *perm, double eps1, int64_t *k_js, int64_t *k_0);
 /* get_sqrt_primes!(q) (src/qmc_generators.jl:300-310), host only. */
 int dbgz_sqrt_primes(int64_t n, double *q);
 /* richtmyer_mat!(X, q, n0) (src/qmc_generators.jl:314-325): X is m x n

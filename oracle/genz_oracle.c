@@ -266,6 +266,162 @@ void orc_cholesky_genz_margins(int64_t n, double *M, double *a, double *b,
 }
 
 /* src/cholesky.jl:144-242 (no pivoting; only the upper triangle is used) */
+/* ------------------------------------------------------------------ */
+/* Cholesky with diagonal pivoting: src/cholesky.jl:244-432            */
+/* ------------------------------------------------------------------ */
+void orc_cholesky_rowmax(int64_t n, double *M, double *a, double *b,
+                         int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
+                         int64_t *perm, double *scale_vec, int64_t *rank_out) {
+  scale_to_correlation(n, M, a, b, scale_vec, 1); /* :252-271 (a, b scaled, not permuted later) */
+  for (int64_t i = 0; i < n; ++i) perm[i] = i;
+  int64_t rank = n;
+  double *d_vec = (double *)calloc((size_t)n + 1, sizeof(double));
+#define D1(k) d_vec[(k) - 1]
+  for (int64_t iv0 = 1; iv0 <= n; iv0 += bs4) {
+    int64_t iv1 = imin(n, iv0 + bs4 - 1);
+    for (int64_t iii0 = iv0; iii0 <= iv1; iii0 += bs3) {
+      int64_t iii1 = imin(iv1, iii0 + bs3 - 1);
+      for (int64_t ii0 = iii0; ii0 <= iii1; ii0 += bs2) {
+        int64_t ii1 = imin(iii1, ii0 + bs2 - 1);
+        for (int64_t i0 = ii0; i0 <= ii1; i0 += bs1) {
+          int64_t i1 = imin(ii1, i0 + bs1 - 1);
+          for (int64_t k = i0; k <= ii1; ++k) D1(k) = 0.0;
+          for (int64_t i = i0; i <= i1; ++i) {
+            /* largest remaining diagonal of the panel, first on ties (:294-305) */
+            int64_t i_m = i;
+            double m_ii = M1(i, i) - D1(i);
+            for (int64_t k = i; k <= ii1; ++k) {
+              double m_kk = M1(k, k) - D1(k);
+              if (m_kk > m_ii) { m_ii = m_kk; i_m = k; }
+            }
+            if (m_ii > 0) { /* :309-314: the rank test comes before the swap */
+              m_ii = sqrt(m_ii);
+            } else {
+              rank = i - 1;
+              break;
+            }
+            if (i_m != i) { /* :316-326 (a and b are not swapped) */
+              int64_t tp = perm[i - 1]; perm[i - 1] = perm[i_m - 1]; perm[i_m - 1] = tp;
+              double t = D1(i_m); D1(i_m) = D1(i); D1(i) = t;
+              for (int64_t k = i0; k <= n; ++k) { t = M1(i, k); M1(i, k) = M1(i_m, k); M1(i_m, k) = t; }
+              for (int64_t k = 1; k <= n; ++k) { t = M1(k, i); M1(k, i) = M1(k, i_m); M1(k, i_m) = t; }
+            }
+            M1(i, i) = m_ii;
+            if (i == i0) { /* :332-338 */
+              for (int64_t j = i + 1; j <= ii1; ++j) {
+                double m_ij = M1(i, j) / m_ii;
+                M1(i, j) = m_ij;
+                M1(j, i) = m_ij;
+                D1(j) = D1(j) + m_ij * m_ij;
+              }
+            } else if (i < ii1) { /* :339-353 */
+              for (int64_t j = i + 1; j <= ii1; ++j) {
+                double acc = 0.0;
+                for (int64_t l = i0; l <= i - 1; ++l) acc = fma(M1(j, l), M1(l, i), acc);
+                M1(j, i) = M1(j, i) - acc;
+              }
+              for (int64_t j = i + 1; j <= ii1; ++j) {
+                double m_ij = M1(j, i);
+                m_ij = m_ij / m_ii;
+                M1(i, j) = m_ij;
+                M1(j, i) = m_ij;
+                D1(j) = D1(j) + m_ij * m_ij;
+              }
+            }
+          }
+          if (rank < n) break;
+          if (i1 < ii1) { /* :361-365 */
+            for (int64_t k = i1 + 1; k <= ii1; ++k)
+              for (int64_t j = i1 + 1; j <= ii1; ++j) {
+                double acc = 0.0;
+                for (int64_t l = i0; l <= i1; ++l) acc = fma(M1(j, l), M1(l, k), acc);
+                M1(j, k) = M1(j, k) - acc;
+              }
+          }
+        }
+        if (rank < n) break;
+        if (ii1 < iii1) { /* :372-379 */
+          trsm_upper_t(n, M, ii0, ii1, ii1 + 1, iii1);
+          syrk_full(n, M, ii0, ii1, ii1 + 1, iii1);
+        }
+      }
+      if (rank < n) break;
+      if (iii1 < iv1) { /* :385-392 */
+        trsm_upper_t(n, M, iii0, iii1, iii1 + 1, iv1);
+        syrk_full(n, M, iii0, iii1, iii1 + 1, iv1);
+      }
+    }
+    if (rank < n) break;
+    if (iv1 < n) { /* :398-405 */
+      trsm_upper_t(n, M, iv0, iv1, iv1 + 1, n);
+      syrk_full(n, M, iv0, iv1, iv1 + 1, n);
+    }
+  }
+#undef D1
+  free(d_vec);
+  *rank_out = rank;
+}
+
+/* ------------------------------------------------------------------ */
+/* adapt_low_rank!: src/cholesky.jl:24-123                             */
+/* ------------------------------------------------------------------ */
+void orc_adapt_low_rank(int64_t nr, int64_t n, double *M, double *a, double *b, int64_t rank, int64_t *perm,
+                        double eps1, int64_t *k_js, int64_t *k_0_out) {
+  /* M is nr x n (column-major); k_js (length rank) receives the 1-based
+   * block ends; perm holds 0-based indices and is permuted in place */
+#define MC(i, j) M[((j) - 1) * nr + ((i) - 1)]
+  double *tmp = (double *)malloc(sizeof(double) * (size_t)(nr > 0 ? nr : 1));
+  for (int64_t i = 1; i <= rank; ++i) k_js[i - 1] = i;
+  int64_t k_0 = 0, j = rank + 1, n_active = n;
+  while (j <= n_active) {
+    /* level: last row i <= rank with |M[i, j]| > eps1 (:41) */
+    int64_t i_j = 0;
+    for (int64_t i = rank; i >= 1; --i)
+      if (fabs(MC(i, j)) > eps1) { i_j = i; break; }
+    if (i_j == 0) { /* :44-61: to the end, not advancing j */
+      if (j != n_active) {
+        for (int64_t r = 1; r <= nr; ++r) { double t = MC(r, n_active); MC(r, n_active) = MC(r, j); MC(r, j) = t; }
+        double t = a[j - 1]; a[j - 1] = a[n_active - 1]; a[n_active - 1] = t;
+        t = b[j - 1]; b[j - 1] = b[n_active - 1]; b[n_active - 1] = t;
+        int64_t tp = perm[j - 1]; perm[j - 1] = perm[n_active - 1]; perm[n_active - 1] = tp;
+      }
+      k_0 += 1;
+      n_active -= 1;
+      continue;
+    }
+    /* :64-80: scale by the pivot, swap the bounds if it is negative */
+    double m_ij = MC(i_j, j);
+    int is_neg = m_ij < 0.0;
+    double inv_m = 1.0 / m_ij;
+    for (int64_t k = 1; k <= i_j; ++k) MC(k, j) *= inv_m;
+    a[j - 1] *= inv_m;
+    b[j - 1] *= inv_m;
+    if (is_neg) { double t = a[j - 1]; a[j - 1] = b[j - 1]; b[j - 1] = t; }
+    /* :85-111: insert at the end of block i_j */
+    int64_t pos = k_js[i_j - 1] + 1;
+    if (j != pos) {
+      for (int64_t r = 1; r <= nr; ++r) tmp[r - 1] = MC(r, j);
+      double va = a[j - 1], vb = b[j - 1];
+      int64_t vp = perm[j - 1];
+      for (int64_t c = j; c >= pos + 1; --c) {
+        for (int64_t r = 1; r <= nr; ++r) MC(r, c) = MC(r, c - 1);
+        a[c - 1] = a[c - 2];
+        b[c - 1] = b[c - 2];
+        perm[c - 1] = perm[c - 2];
+      }
+      for (int64_t r = 1; r <= nr; ++r) MC(r, pos) = tmp[r - 1];
+      a[pos - 1] = va;
+      b[pos - 1] = vb;
+      perm[pos - 1] = vp;
+    }
+    for (int64_t k = i_j; k <= rank; ++k) k_js[k - 1] += 1; /* :115-118 */
+    j += 1;
+  }
+#undef MC
+  free(tmp);
+  *k_0_out = k_0;
+}
+
 void orc_cholesky_classic(int64_t n, double *M, double *a, double *b,
                           int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
                           double *scale_vec) {
@@ -372,6 +528,7 @@ void orc_sobol_points(int64_t dims, const uint32_t *V, int64_t first, int64_t m,
 /* ------------------------------------------------------------------ */
 typedef struct tile_buf {
   double *Y, *S, *c, *dc, *p;
+  double *lw; /* per-sample sum of log dc (the log of p), when P->logw is set */
 } tile_buf;
 
 static inline double clamp9(double v) { return fmax(fmin(v, 9.0), -9.0); }
@@ -439,6 +596,7 @@ static void cdf_update(const orc_problem *P, double a_i, double b_i, double inv_
     tb->c[t] = cv;
     tb->dc[t] = dv;
     tb->p[t] *= dv;
+    if (tb->lw) tb->lw[t] += log(dv);
   }
 }
 
@@ -452,6 +610,7 @@ static double dense_tile(const orc_problem *P, const orc_opts *o, int64_t bi, in
 #define Y1(t, i) tb->Y[((i) - 1) * len + (t)]
 #define S1(t, c) tb->S[((c) - 1) * len + (t)]
   for (int64_t t = 0; t < len; ++t) { tb->c[t] = c_1; tb->dc[t] = dc_1; tb->p[t] = dc_1; }
+  if (tb->lw) for (int64_t t = 0; t < len; ++t) tb->lw[t] = log(dc_1);
   memset(tb->S, 0, sizeof(double) * (size_t)(len * bi));
   for (int64_t ii1 = 1; ii1 <= n - 1; ii1 += bi) {
     int64_t ii2 = imin(ii1 + bi - 1, n - 1);
@@ -509,6 +668,7 @@ static double sparse_tile(const orc_problem *P, const orc_opts *o, const csc *C,
   const int64_t n = P->n;
   const double c2 = sqrt(2.0);
   for (int64_t t = 0; t < len; ++t) { tb->c[t] = c_1; tb->dc[t] = dc_1; tb->p[t] = dc_1; }
+  if (tb->lw) for (int64_t t = 0; t < len; ++t) tb->lw[t] = log(dc_1);
   for (int64_t i = 1; i <= n - 1; ++i) {
     rand_points(P, o, n_pass_base, j1, len, i, k, tb);
     double *Yi = tb->Y + (i - 1) * len;
@@ -557,6 +717,7 @@ static void qmc_loop(const orc_problem *P, const orc_opts *o, const csc *C, int 
       tb.c = (double *)malloc(sizeof(double) * (size_t)bj);
       tb.dc = (double *)malloc(sizeof(double) * (size_t)bj);
       tb.p = (double *)malloc(sizeof(double) * (size_t)bj);
+      tb.lw = P->logw ? (double *)malloc(sizeof(double) * (size_t)bj) : NULL;
 #pragma omp for schedule(dynamic, 1)
       for (int64_t tt = 0; tt < n_tiles; ++tt) {
         int64_t j1 = 1 + tt * bj;
@@ -565,8 +726,9 @@ static void qmc_loop(const orc_problem *P, const orc_opts *o, const csc *C, int 
         tile_sums[tt] = P->sparse
             ? sparse_tile(P, o, C, n_pass_base, j1, len, k, c_1, dc_1, &tb)
             : dense_tile(P, o, bi, bi2, n_pass_base, j1, len, k, c_1, dc_1, &tb);
+        if (P->logw) memcpy(P->logw + (k - 1) * m + (j1 - 1), tb.lw, sizeof(double) * (size_t)len);
       }
-      free(tb.Y); free(tb.S); free(tb.c); free(tb.dc); free(tb.p);
+      free(tb.Y); free(tb.S); free(tb.c); free(tb.dc); free(tb.p); free(tb.lw);
     }
     double total = 0.0;
     for (int64_t tt = 0; tt < n_tiles; ++tt) total += tile_sums[tt];

@@ -59,6 +59,15 @@ void orc_cholesky_genz(int64_t n, double *M, double *a, double *b,
 void orc_cholesky_genz_margins(int64_t n, double *M, double *a, double *b,
                                int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
                                int64_t *perm, double *scale_vec, int64_t *rank, double *margins);
+/* src/cholesky.jl:244-432 (diagonal pivoting; a, b scaled, not permuted) */
+void orc_cholesky_rowmax(int64_t n, double *M, double *a, double *b,
+                         int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
+                         int64_t *perm, double *scale_vec, int64_t *rank);
+/* src/cholesky.jl:24-123.  M is nr x n; perm 0-based, permuted in place;
+ * k_js (length rank) receives the 1-based block ends, *k_0 the number of
+ * zero-level columns moved to the end. */
+void orc_adapt_low_rank(int64_t nr, int64_t n, double *M, double *a, double *b, int64_t rank, int64_t *perm,
+                        double eps1, int64_t *k_js, int64_t *k_0);
 /* src/cholesky.jl:144-242 */
 void orc_cholesky_classic(int64_t n, double *M, double *a, double *b,
                           int64_t bs1, int64_t bs2, int64_t bs3, int64_t bs4,
@@ -89,6 +98,9 @@ typedef struct orc_problem {
   int sparse;             /* 1: QMCDataSparse loop over strict-upper CSC */
   int64_t gen_base0;      /* generator position of the first pass (0 for a
                              fresh QMCData; next_points! advances it by m) */
+  double *logw;           /* optional (NULL: unused), m x n_reps: each sample's
+                             log p = sum of log dc over its variables, of the
+                             last pass (a diagnostic; no reference counterpart) */
 } orc_problem;
 
 /* src/qmc.jl:783-850 (+ the loops :315-444, :485-608, :618-718).

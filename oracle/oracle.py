@@ -54,6 +54,7 @@ class OrcProblem(C.Structure):
         ("cdf_form", C.c_int),
         ("sparse", C.c_int),
         ("gen_base0", C.c_int64),
+        ("logw", C.POINTER(C.c_double)),
     ]
 
 
@@ -79,6 +80,8 @@ def lib():
         L.orc_cholesky_genz.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pi64, pd, pi64]
         L.orc_cholesky_genz_margins.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pi64, pd, pi64, pd]
         L.orc_cholesky_classic.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pd]
+        L.orc_cholesky_rowmax.argtypes = [i64, pd, pd, pd, i64, i64, i64, i64, pi64, pd, pi64]
+        L.orc_adapt_low_rank.argtypes = [i64, i64, pd, pd, pd, i64, pi64, d, pi64, pi64]
         L.orc_truncate_U.argtypes = [i64, pd, d]
         L.orc_sqrt_primes.argtypes = [i64, pd]
         L.orc_richtmyer_mat.argtypes = [i64, i64, pd, i64, pd]
@@ -135,6 +138,35 @@ def cholesky_classic(Sigma, a, b, bs1=128, bs2=512, bs3=1024, bs4=2048):
     return dict(U=M, perm=np.arange(n), rank=n, a=a, b=b, scale_vec=scale)
 
 
+def cholesky_rowmax(Sigma, a, b, bs1=128, bs2=512, bs3=1024, bs4=2048):
+    """cholesky_rowmax!(copy(Σ), copy(a), copy(b), bs1, ...) -> dict (src/cholesky.jl:244-432)."""
+    n = Sigma.shape[0]
+    M = np.array(Sigma, dtype=np.float64, order="F", copy=True)
+    a = np.array(a, dtype=np.float64, copy=True)
+    b = np.array(b, dtype=np.float64, copy=True)
+    perm = np.zeros(n, dtype=np.int64)
+    scale = np.zeros(n, dtype=np.float64)
+    rank = C.c_int64(0)
+    lib().orc_cholesky_rowmax(n, _pd(M), _pd(a), _pd(b), bs1, bs2, bs3, bs4,
+                              perm.ctypes.data_as(C.POINTER(C.c_int64)), _pd(scale), C.byref(rank))
+    return dict(U=M, perm=perm, rank=rank.value, a=a, b=b, scale_vec=scale)
+
+
+def adapt_low_rank(M, a, b, rank, perm, eps1):
+    """adapt_low_rank!(M, a, b, rank, perm, eps1) on copies -> (M, a, b, perm, k_js, k_0)
+    (src/cholesky.jl:24-123); perm 0-based, k_js 1-based block ends."""
+    M = np.array(M, dtype=np.float64, order="F", copy=True)
+    a = np.array(a, dtype=np.float64, copy=True)
+    b = np.array(b, dtype=np.float64, copy=True)
+    perm = np.array(perm, dtype=np.int64, copy=True)
+    k_js = np.zeros(max(rank, 1), dtype=np.int64)
+    k0 = C.c_int64(0)
+    lib().orc_adapt_low_rank(M.shape[0], M.shape[1], _pd(M), _pd(a), _pd(b), rank,
+                             perm.ctypes.data_as(C.POINTER(C.c_int64)), float(eps1),
+                             k_js.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(k0))
+    return M, a, b, perm, k_js[:rank], k0.value
+
+
 def truncate_U(U, eps_T=np.finfo(np.float64).eps):
     U = np.array(U, dtype=np.float64, order="F", copy=True)
     lib().orc_truncate_U(U.shape[0], _pd(U), float(eps_T))
@@ -166,8 +198,10 @@ def sobol_points(V, first, m):
 def qmc_pnorm(U, a, b, *, m, n_reps, qmc_type=RICHTMYER, shifts=None, q=None, V=None,
               sobol_first=0, ushifts=None, cdf_form=CDF_ERF, sparse=False,
               block_size_i=64, block_size_i2=32, block_size_j=64, n_bits=32,
-              max_pts=None, max_abs_err=1e-6, threads=0, gen_base0=0):
-    """qmc_pnorm! on a prepared problem (U, permuted/scaled a, b) -> (P, err, n_pts, reps)."""
+              max_pts=None, max_abs_err=1e-6, threads=0, gen_base0=0, logw=None):
+    """qmc_pnorm! on a prepared problem (U, permuted/scaled a, b) -> (P, err, n_pts, reps).
+    logw: an (m, n_reps) float64 Fortran-ordered array that receives each
+    sample's log-weight (sum of log dc) of the last pass."""
     n = U.shape[0]
     U = np.asfortranarray(U, dtype=np.float64)
     a = np.ascontiguousarray(a, dtype=np.float64)
@@ -180,6 +214,9 @@ def qmc_pnorm(U, a, b, *, m, n_reps, qmc_type=RICHTMYER, shifts=None, q=None, V=
     P.cdf_form = cdf_form
     P.sparse = 1 if sparse else 0
     P.gen_base0 = int(gen_base0)
+    if logw is not None:
+        assert logw.shape == (m, n_reps) and logw.dtype == np.float64 and logw.flags.f_contiguous
+        P.logw = _pd(logw)
     if qmc_type == RICHTMYER:
         q = sqrt_primes(n - 1) if q is None else np.ascontiguousarray(q, dtype=np.float64)
         sh = np.asfortranarray(shifts, dtype=np.float64)

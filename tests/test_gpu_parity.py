@@ -314,14 +314,15 @@ def test_pnorm_tensor_core_phases(D, n, m, n_reps, prec):
 
 @pytest.mark.parametrize("prec", [L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
 @pytest.mark.parametrize("n,m,first", [(200, 1024, 2048), (600, 1024, 128 * 37), (300, 1000, 2048),
-                                       (300, 1024, 2048 + 37)])
+                                       (300, 1024, 2048 + 37), (300, 1000, None), (200, 1500, None)])
 def test_pnorm_tensor_core_sobol_points(D, n, m, first, prec):
-    # Sobol points in the tensor-core loop: from the per-block tables when a
-    # pass starts at a multiple of 128 (first and m aligned), per step
-    # otherwise (the third case switches after its first pass); three passes
-    # against the FP64 loop and the FP32 SIMT loop on the same points.  Other
-    # points would move P by about the QMC error, which the test requires to
-    # be far above its tolerance.
+    # Sobol points in the tensor-core loop, from the per-block staged
+    # integers at any first index: tiles at multiples of 128, at other
+    # offsets, offsets that change from pass to pass (m not a multiple of 32),
+    # and the default first index of SobolQMC (2^floor(log2(2m)) + 1); three
+    # passes against the FP64 loop and the FP32 SIMT loop on the same points.
+    # Other points would move P by about the QMC error, which the test
+    # requires to be far above its tolerance.
     S = _spd(n, n + 11)
     lo, up = W.bounds_quarter(S)
     R = 3
@@ -345,16 +346,17 @@ def test_pnorm_tensor_core_sobol_points(D, n, m, first, prec):
 
 
 @pytest.mark.parametrize("sparse", [False, True])
-@pytest.mark.parametrize("m,first", [(1000, 2048), (1024, 128 * 19), (1000, 2085)])
+@pytest.mark.parametrize("m,first", [(1000, 2048), (1024, 128 * 19), (1000, 2085), (1000, None), (1500, None),
+                                     (1024, None)])
 def test_sobol_staged_points_fp64_vs_checker(D, oracle, sparse, m, first):
-    # the FP64 loops (dense SIMT, banded) against the checker on Sobol points:
-    # staged per-block integers when a pass starts at a multiple of 128 (the
-    # first pass of the first case, with a partial last tile, and every pass
-    # of the second), per step otherwise
+    # the FP64 loops (dense SIMT, banded) against the checker on Sobol points
+    # from the per-block staged integers at any first index (partial last
+    # tiles, offsets that change between passes, the default first index
+    # 2^floor(log2(2m)) + 1 of SobolQMC for m a power of two and not)
     n, R = 160, 3
     S = _spd(n, 5 + m)
     lo, up = W.bounds_quarter(S)
-    us = np.random.default_rng(m + first).integers(0, 2**64, size=(n - 1, R), dtype=np.uint64)
+    us = np.random.default_rng(m + (first or 0)).integers(0, 2**64, size=(n - 1, R), dtype=np.uint64)
     opts = D.QMC_opts(m=m, n_reps=R, max_pts=2 * m, max_abs_err=0.0)
     cls = D.QMCDataSparse if sparse else D.QMCData
     Q = cls(S, lo, up, opts, qmc_type="Sobol", ushifts=us, sobol_first=first)

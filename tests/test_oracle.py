@@ -278,3 +278,84 @@ def test_cpu_blas_erfinv(oracle):
     big = np.abs(x) >= 1e-3
     assert np.max(np.abs(y[big] - yo[big]) / np.abs(yo[big])) < 1e-13
     assert np.max(np.abs(y - yo)) < 1e-15
+
+
+# ---- cholesky_rowmax! and adapt_low_rank! (src/cholesky.jl:24-123, 244-432)
+def test_adapt_low_rank_reference_testset(oracle):
+    """test/runtests.jl:61-89: a rank-20 factor with 10 dependent columns,
+    column 25 (1-based) all zero: one zero-level column, moved to the end."""
+    rng = np.random.default_rng(61)
+    n, rank = 30, 20
+    M = np.zeros((n, n))
+    M[np.arange(rank), np.arange(rank)] = 1.0
+    M[:rank, rank:] = rng.random((rank, n - rank))
+    M[:, 24] = 0.0
+    a, b = np.zeros(n), np.ones(n)
+    M2, a2, b2, perm, k_js, k_0 = oracle.adapt_low_rank(M, a, b, rank, np.arange(n), 1e-10)
+    assert k_0 == 1
+    assert perm[-1] == 24
+    assert np.all(M2[:, -1] == 0.0)
+    assert len(k_js) == rank
+    # every column is where its level puts it, scaled so its last entry is 1
+    assert sorted(perm.tolist()) == list(range(n))
+    assert k_js[-1] == n - k_0
+
+
+def test_adapt_low_rank_levels_and_signs(oracle):
+    """Columns of every level, negative pivots (bounds swapped), several
+    zero columns: the block structure k_js, the scaling and the order."""
+    rng = np.random.default_rng(62)
+    n, rank = 40, 12
+    M = np.zeros((n, n))
+    M[np.arange(rank), np.arange(rank)] = 1.0
+    lev = rng.integers(0, rank + 1, size=n - rank)  # 0: a zero column
+    for c, l in zip(range(rank, n), lev):
+        if l:
+            M[:l, c] = rng.standard_normal(l)
+            M[l - 1, c] = rng.choice([-1.0, 1.0]) * (0.5 + rng.random())
+    a, b = -rng.random(n), rng.random(n)
+    M2, a2, b2, perm, k_js, k_0 = oracle.adapt_low_rank(M, a, b, rank, np.arange(n), 1e-12)
+    assert k_0 == int(np.sum(lev == 0))
+    for t in range(n - k_0):
+        c = perm[t]
+        if c >= rank:
+            l = lev[c - rank]
+            m = M[l - 1, c]
+            assert np.array_equal(M2[:l, t], M[:l, c] * (1.0 / m))
+            lo, hi = a[c] * (1.0 / m), b[c] * (1.0 / m)
+            assert (a2[t], b2[t]) == ((hi, lo) if m < 0 else (lo, hi))
+    # blocks: level-i constraints sit right after base column i-1 and its earlier ones
+    starts = [0] + list(k_js[:-1])
+    for i in range(rank):
+        assert perm[starts[i]] == i
+        for t in range(starts[i] + 1, k_js[i]):
+            assert lev[perm[t] - rank] == i + 1
+
+
+@pytest.mark.parametrize("n,rank_true,bs", [(60, 60, (8, 16, 32, 64)), (100, 37, (16, 32, 64, 128)),
+                                            (300, 300, (64, 128, 256, 512))])
+def test_cholesky_rowmax_reconstruction(oracle, n, rank_true, bs):
+    """Diagonal pivoting: the permuted correlation matrix is U'U to 1e-10
+    (the bound of test/runtests.jl:15-36) on the leading rank block, the
+    pivots take the largest remaining diagonal, and a rank-deficient matrix
+    stops at its rank."""
+    rng = np.random.default_rng(n + rank_true)
+    A = rng.standard_normal((n, rank_true))
+    S = A @ A.T + (0.0 if rank_true < n else 0.5) * np.eye(n)
+    a, b = -np.ones(n), np.ones(n)
+    F = oracle.cholesky_rowmax(S, a, b, *bs)
+    d = np.sqrt(np.diag(S))
+    R = S / np.outer(d, d)
+    p = F["perm"]
+    r = F["rank"]
+    # the rank test is m_ii > 0 (src/cholesky.jl:309-314), not against a
+    # tolerance: past the true rank the pivots are rounding residue (about
+    # 1e-8 after the square root) until one is not positive
+    assert (r == n) if rank_true == n else (rank_true <= r < n)
+    if rank_true < n:
+        assert np.all(np.diag(F["U"])[rank_true:r] < 1e-6)
+    r = rank_true
+    U = np.triu(F["U"])[:r, :r]
+    assert np.max(np.abs(R[np.ix_(p[:r], p[:r])] - U.T @ U)) < 1e-10
+    # a and b are scaled in place but not permuted (src/cholesky.jl:265-266)
+    np.testing.assert_array_equal(F["a"], a / d)
