@@ -44,6 +44,13 @@ MIXED = "fp32_split_bf16"   # mixed-precision mode of the headline number
 # DRAM bytes of one 2^21-sample launch of the split-BF16 loop at d=1000 (ncu capture of a
 # 131,072-sample launch: 0.239 GB read + 0.347 GB written, scaled by the sample count)
 TRAFFIC_PER_LAUNCH = 16 * (238.68e6 + 347.43e6)
+# warp instructions of one split-BF16 loop launch at d = 1000 per sample (ncu
+# smsp__inst_executed.sum of a 131,072-sample launch: 8.717e8), and its
+# XU (special-function) pipe share; the issue roofline below scales it to the
+# timed launch
+INST_PER_SAMPLE = 8.717e8 / 131072
+XU_PIPE_PCT = 15.3
+ISSUE_PROFILE = "profiles/genz_umma_splitbf16_d1000_8192pts_full.md"
 
 
 def _peaks():
@@ -189,7 +196,7 @@ def cpu_baseline(w, threads: int):
     }
 
 
-def run_c4(args):
+def run_c4(args, emit=True):
     """The batch configuration: 4096 problems, d ~ U{16..256}, Sobol 2^14 x 8
     each.  The loops' engine per dimension is chosen by the library's
     autotuner (once, untimed, reported); each mode runs as a batch plan (one
@@ -272,11 +279,13 @@ def run_c4(args):
         "max_abs_err_fp32_simt_vs_fp64": float(np.max(np.abs(P32 - P64))),
         "sample_dims_per_s_fp32": samples * float(dims.mean() - 1) / (out["fp32_split_bf16"]["loop_ms"] * 1e-3),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    if emit:
+        print(json.dumps(line), flush=True)
+        return 0
+    return line
 
 
-def run_small(args):
+def run_small(args, emit=True):
     """The d = 10 (c1: Richtmyer 10^4 x 10, FP64, reordering on) and d = 500
     (c2: Sobol 2^16 x 12; FP64, FP32+TF32 and split-BF16) configurations:
     per mode the pass on the device (CUDA events on the library's stream)
@@ -365,11 +374,13 @@ def run_small(args):
             Qa.close()
             ad[drv] = {"ms": statistics.median(ts), "n_pts": r[2], "P": r[0]}
         line["adaptive_100_passes"] = ad
-    print(json.dumps(line), flush=True)
-    return 0
+    if emit:
+        print(json.dumps(line), flush=True)
+        return 0
+    return line
 
 
-def run_c5(args):
+def run_c5(args, emit=True):
     """The banded configuration: d = 10^4 AR(1) (rho = 0.9), factor truncated to
     64 super-diagonals, a = -inf, Sobol 2^18 x 10; P (FP32 and FP64 banded
     loops) and P with dP/da, dP/db (FP32 adjoint, chunked over samples).
@@ -408,6 +419,14 @@ def run_c5(args):
     (P32, e32, _), out["fp32_ms"] = timed(lambda: D.qmc_pnorm(Q, precision=L.PREC_FP32_SIMT), args.steps)
     (P64, e64, _), out["fp64_ms"] = timed(lambda: D.qmc_pnorm(Q, precision=L.PREC_FP64), max(1, args.steps // 2))
     g, out["fp32_grad_ms"] = timed(lambda: D.qmc_pnorm_grad(Q, precision=L.PREC_FP32_SIMT), max(1, args.steps // 2))
+    lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+    # stored forward state of the gradient call: dimension checkpoints every
+    # 256 dimensions (the band's last values and the recursion state) and one
+    # segment's recomputed rows, against y, s, dc of every sample-variable
+    out["grad_state"] = {"checkpoint_every_dims": 256, "bytes": int(prof.grad_state_bytes),
+                         "sample_chunks": int(prof.grad_chunks),
+                         "full_state_bytes": int(w.m * w.n_reps * 3 * 4 * w.d)}
+    out["grad_state"]["fraction_of_full"] = out["grad_state"]["bytes"] / out["grad_state"]["full_state_bytes"]
     Q.close()
     samples = float(w.m * w.n_reps)
     line = {
@@ -421,8 +440,32 @@ def run_c5(args):
         "dP_db_norm": float(np.linalg.norm(g[4])), "P_grad_call": g[0],
         "sample_dims_per_s_fp32": samples * (w.d - 1) / (out["fp32_ms"] * 1e-3),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    if emit:
+        print(json.dumps(line), flush=True)
+        return 0
+    return line
+
+
+def other_configs(args):
+    """The other benchmark configurations measured in the same run (their own
+    lines come from `--workload c1|c2|c4|c5`): d = 10 (FP64, with the CPU
+    checker on the full workload), d = 500 (FP64 and the mixed modes), the
+    4096-problem batch and the banded d = 10^4 problem, with fewer timed steps
+    than their own lines.  Each record is that configuration's line."""
+    import copy
+    out = {}
+    for wl, steps, warm in (("c1", 5, 2), ("c2", 5, 2), ("c4", 2, 1), ("c5", 2, 1)):
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup = wl, steps, warm
+        t = time.perf_counter()
+        try:
+            rec = {"c1": run_small, "c2": run_small, "c4": run_c4, "c5": run_c5}[wl](a, emit=False)
+        except Exception as e:  # report, do not lose the headline line
+            rec = {"error": f"{type(e).__name__}: {e}"}
+        if isinstance(rec, dict):
+            rec["wall_s"] = time.perf_counter() - t
+        out[wl] = rec
+    return out
 
 
 def run_reference(args):
@@ -487,6 +530,8 @@ def main():
     ap.add_argument("--precision", default=MIXED)
     ap.add_argument("--quick", action="store_true", help="small d=200 case for smoke runs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="headline line only (without the d = 10, d = 500, batch and banded records)")
     ap.add_argument("--d", type=int, default=None, help="dimension (default: 1000)")
     ap.add_argument("--points", type=int, default=None, help="points per shift (default: 2^17)")
     ap.add_argument("--only", action="store_true",
@@ -657,6 +702,23 @@ def main():
         Pm = D.qmc_pnorm(Qq, precision=D.PRECISIONS[name])[0]
         acc[name] = {"P": Pm, "abs_err": abs(Pm - acc["P_fp64"]), "rel_err": abs(Pm - acc["P_fp64"]) / acc["P_fp64"]}
     Qq.close()
+    # accuracy at the workload's own bounds, where P underflows: per-sample
+    # log-weights of the same points (dbgz_pnorm_logw), log P from their
+    # log-mean-exp, against FP64 with the erfc form of the CDF (the erf form
+    # rounds the deep lower tails to 0 and gives P = 0 exactly)
+    Qc = D.QMCData(Sig_h, a_h, b_h, D.QMC_opts(m=w.m, n_reps=w.n_reps, max_pts=w.m, max_abs_err=0.0),
+                   qmc_type="Richtmyer", shifts=sh_h, cdf_form=L.CDF_ERFC, device=local)
+    lw64 = D.qmc_pnorm_logw(Qc, precision=L.PREC_FP64)[0]
+    lP64 = float(D.log_mean_exp(lw64.ravel()))
+    own = {"workload": w.name, "reference": "FP64, erfc form of the CDF", "log10_P_fp64": lP64 / math.log(10)}
+    for name in ("fp32_split_bf16", "fp32_tf32", "fp32_simt"):
+        lwm = D.qmc_pnorm_logw(Qc, precision=D.PRECISIONS[name])[0]
+        dlog = float(D.log_mean_exp(lwm.ravel())) - lP64
+        dshift = np.abs(D.log_mean_exp(lwm) - D.log_mean_exp(lw64))
+        own[name] = {"log_P_minus_log_P_fp64": dlog, "rel_err_P": math.expm1(abs(dlog)),
+                     "max_abs_dlog_per_shift": float(np.max(dshift))}
+    Qc.close()
+    del lw64
     # gradient accuracy on the same model: mixed vs FP64 adjoint, and dP/dB
     # against central differences (h = 1e-4) of FP64 estimates on common points
     Qf, sq = make_fm(wq)
@@ -733,6 +795,17 @@ def main():
             "qmc_3sem": err_mix,
             "other_modes": other,
             "grad": grad,
+            "accuracy": {
+                "criterion": "|P - P_fp64| <= 1e-5",
+                "headline_workload": {"P": P_mix, "P_fp64": P64, "abs_err": abs(P_mix - P64),
+                                      "note": "P underflows to 0 in FP64 at these bounds (erf form: dc = 0 "
+                                              "exactly in the deep lower tail), so its absolute error is "
+                                              "trivially 0; see own_bounds_log_space and quarter_bounds"},
+                "quarter_bounds": {"workload": acc["workload"], "P_fp64": acc["P_fp64"],
+                                   **{k: {"abs_err": v["abs_err"], "rel_err": v["rel_err"]}
+                                      for k, v in acc.items() if isinstance(v, dict) and "abs_err" in v}},
+                "own_bounds_log_space": own,
+            },
             "accuracy_quarter_bounds": acc,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH if w.samples == 2**21 else None,
@@ -742,6 +815,20 @@ def main():
                          "kernel": f"integration loop ({args.precision})",
                          "flops_per_launch": flops, "launch_ms": loop_ms,
                          "peak_source": f"{peak_kind} bf16_tflops (burst)"},
+            # the binding resource of the loop: instruction issue (one warp
+            # instruction per cycle per SM sub-partition, 4 x 148 at the sampled
+            # SM clock), not the tensor pipe
+            "roofline_issue": {
+                "bound": "issue", "achieved": INST_PER_SAMPLE * w.samples / (loop_ms * 1e-3),
+                "peak": 4 * 148 * (clocks.get("sm_mhz") or 1965.0) * 1e6, "unit": "warp inst/s",
+                "frac": INST_PER_SAMPLE * w.samples / (loop_ms * 1e-3) /
+                        (4 * 148 * (clocks.get("sm_mhz") or 1965.0) * 1e6),
+                "inst_per_launch": INST_PER_SAMPLE * w.samples,
+                "inst_per_sample_dim": INST_PER_SAMPLE / (d - 1),
+                "xu_pipe_pct_of_peak": XU_PIPE_PCT,
+                "source": "instruction count from the ncu capture in " + ISSUE_PROFILE +
+                          " scaled by the sample count; time from this run's CUDA events",
+                "applies_to": "fp32_split_bf16" if args.precision == "fp32_split_bf16" else "stale: other precision"},
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "host_timed_parts": e2e_parts},
             "gpu_launches": int(n_kern),
@@ -749,6 +836,8 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w, os.cpu_count() or 1)
+        if world == 1 and not args.quick and not args.no_other_configs:
+            line["other_configs"] = other_configs(args)
         print(json.dumps(line), flush=True)
     del Q
     if dist:

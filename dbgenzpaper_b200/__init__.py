@@ -80,6 +80,12 @@ class Context:
         (larger sample counts run in chunks of tiles)."""
         L.check(self._lib.dbgz_set_state_budget(self.handle, int(nbytes)), self.handle)
 
+    def set_grad_checkpoints(self, segment: int) -> None:
+        """Banded gradients: a checkpoint every `segment` dimensions, each
+        segment recomputed from its checkpoint before the adjoint sweeps it
+        (default 256; 0 stores the whole forward state).  Same results."""
+        L.check(self._lib.dbgz_set_grad_checkpoints(self.handle, int(segment)), self.handle)
+
     def close(self):
         if self.handle:
             if self._lib.dbgz_destroy(self.handle) == L.OK:

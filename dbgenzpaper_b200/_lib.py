@@ -56,6 +56,8 @@ class DbgzProfile(C.Structure):
         ("prepare_ms", C.c_double),
         ("prepare_launches", C.c_int64),
         ("sigma_adjoint_ms", C.c_double),
+        ("grad_state_bytes", C.c_int64),
+        ("grad_chunks", C.c_int64),
     ]
 
 
@@ -93,6 +95,7 @@ SIGNATURES = {
     "dbgz_problem_factor": (C.c_int, [_vp, _pd, _pi64, _pd, _pd, _pd, _pi64]),
     "dbgz_pnorm": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
     "dbgz_pnorm_logw": (C.c_int, [_vp, C.c_int, _pd, _pd]),
+    "dbgz_set_grad_checkpoints": (C.c_int, [_vp, C.c_int64]),
     "dbgz_pnorm_graph": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd]),
     "dbgz_pnorm_grad": (C.c_int, [_vp, C.c_int, _pd, _pd, _pi64, _pd, _pd, _pd]),
     "dbgz_problem_sigma_adjoint": (C.c_int, [_vp, _pd, _pd, _pd, _pd]),

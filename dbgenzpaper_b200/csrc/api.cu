@@ -175,6 +175,12 @@ int dbgz_set_state_budget(dbgz_ctx *ctx, uint64_t bytes) {
   return DBGZ_OK;
 }
 
+int dbgz_set_grad_checkpoints(dbgz_ctx *ctx, int64_t segment) {
+  if (!ctx || segment < 0) return DBGZ_ERR_INVALID_ARGUMENT;
+  ctx->grad_ckpt_seg = segment;
+  return DBGZ_OK;
+}
+
 int dbgz_release_cached(dbgz_ctx *ctx, uint64_t *freed_bytes) {
   if (!ctx) return DBGZ_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
@@ -352,6 +358,8 @@ int dbgz_prepare(dbgz_ctx *ctx, int64_t d, const double *Sigma, const double *a,
   p->structure = structure;
   p->cdf_form = cdf_form;
   p->sobol_first = sobol_first;
+  p->lower_inf = true;
+  for (int64_t i = 0; i < d; ++i) p->lower_inf = p->lower_inf && std::isinf(a[i]) && a[i] < 0;
   int rc = DBGZ_OK;
   const size_t nn = (size_t)d * d;
   const int64_t launches0 = ctx->launch_count;
@@ -576,6 +584,8 @@ int dbgz_pnorm(dbgz_problem *p, int precision, double *result, double *err, int6
   dbgz_profile pr{};
   pr.prepare_ms = ctx->prof.prepare_ms;
   pr.prepare_launches = ctx->prof.prepare_launches;
+  pr.grad_state_bytes = ctx->prof.grad_state_bytes;
+  pr.grad_chunks = ctx->prof.grad_chunks;
   const int64_t launches0 = ctx->launch_count;
   if (prof) cudaEventRecord(ctx->ev[0], ctx->stream);
   while (true) {

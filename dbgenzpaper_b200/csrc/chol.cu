@@ -193,7 +193,10 @@ k_rowmax_block(double *M, int64_t n, double *dvec, int64_t *perm, int64_t i0, in
 // C[j,k] -= sum_{l=p0..p1} A(l,j) B(l,k) over [c0, c1]^2, one tile per CTA.
 constexpr int kTile = cholk::kTile;
 __global__ void __launch_bounds__(256)
-k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, int a_row) {
+k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, int a_row,
+               const int64_t *rank) {
+  // after a rank failure the reference stops (src/cholesky.jl:575-576, 586-587, ...): no update
+  if (rank && rank[0] < n) return;
   cholk::schur_tile_dev(M, n, p0, p1, c0, c1, a_row, c0 + blockIdx.x * (int64_t)kTile,
                         c0 + blockIdx.y * (int64_t)kTile);
 }
@@ -213,7 +216,8 @@ k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t
 constexpr int kTrsmWarps = 8, kTrsmSlots = 8, kTrsmPass = 32 * kTrsmSlots, kTrsmLc = 32;
 constexpr int kTrsmLd = kTrsmPass + 1;  // padded row of the staged chunk
 __global__ void __launch_bounds__(32 * kTrsmWarps)
-k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1) {
+k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, const int64_t *rank) {
+  if (rank && rank[0] < n) return;  // after a rank failure: no update
   extern __shared__ double Us[];  // [kTrsmLc][kTrsmLd]: Us[lc * kTrsmLd + rr] = U[l0 + lc, q0 + rr]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t c = c0 + (int64_t)blockIdx.x * kTrsmWarps + warp;
@@ -351,18 +355,18 @@ __global__ void k_to_f32(const double *src, float *dst, int64_t nn) {
 }
 
 int launch_schur(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0,
-                 int64_t c1, int a_row) {
+                 int64_t c1, int a_row, const int64_t *rank = nullptr) {
   if (c1 < c0 || p1 < p0) return DBGZ_OK;
   int64_t nt = (c1 - c0 + kTile) / kTile;
   dim3 grid((unsigned)nt, (unsigned)nt);
-  k_schur_update<<<grid, 256, 0, ctx->stream>>>(M, n, p0, p1, c0, c1, a_row);
+  k_schur_update<<<grid, 256, 0, ctx->stream>>>(M, n, p0, p1, c0, c1, a_row, rank);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   return DBGZ_OK;
 }
 
 int launch_trsm(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0,
-                int64_t c1) {
+                int64_t c1, const int64_t *rank = nullptr) {
   if (c1 < c0) return DBGZ_OK;
   const int64_t nc = c1 - c0 + 1;
   const size_t smem = sizeof(double) * kTrsmLc * kTrsmLd;
@@ -373,7 +377,7 @@ int launch_trsm(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int
     if (ctx->device >= 0 && ctx->device < 64) attr_set[ctx->device] = true;
   }
   k_trsm_ut<<<(unsigned)((nc + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps, smem, ctx->stream>>>(M, n, p0, p1,
-                                                                                                    c0, c1);
+                                                                                                    c0, c1, rank);
   dbgz_count_launch(ctx);
   DBGZ_CUDA_TRY(ctx, cudaGetLastError());
   return DBGZ_OK;
@@ -438,21 +442,21 @@ int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b
             k_genz_block<<<1, kStepThreads, 0, st>>>(M, n, a, b, dvec, svec, ovec, perm, i0, i1, ii1, eps0, rank);
           }
           dbgz_count_launch(ctx);
-          if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1);
+          if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1, rank);
         }
         if (ii1 < iii1 && rc == DBGZ_OK) {
-          rc = launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1);
-          if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0);
+          rc = launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1, rank);
+          if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0, rank);
         }
       }
       if (iii1 < iv1 && rc == DBGZ_OK) {
-        rc = launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1);
-        if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0);
+        rc = launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1, rank);
+        if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0, rank);
       }
     }
     if (iv1 < n - 1 && rc == DBGZ_OK) {
-      rc = launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1);
-      if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0);
+      rc = launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, rank);
+      if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0, rank);
     }
   }
   // Blocks after a rank failure return immediately (they read rank < n),
@@ -503,21 +507,21 @@ int dbgz_chol_rowmax_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double 
           int64_t i1 = std::min(ii1, i0 + bs1 - 1);
           k_rowmax_block<<<1, kStepThreads, 0, st>>>(M, n, dvec, perm, i0, i1, ii1, rank);
           dbgz_count_launch(ctx);
-          if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1);
+          if (i1 < ii1) rc = launch_schur(ctx, M, n, i0, i1, i1 + 1, ii1, 1, rank);
         }
         if (ii1 < iii1 && rc == DBGZ_OK) {
-          rc = launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1);
-          if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0);
+          rc = launch_trsm(ctx, M, n, ii0, ii1, ii1 + 1, iii1, rank);
+          if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, ii0, ii1, ii1 + 1, iii1, 0, rank);
         }
       }
       if (iii1 < iv1 && rc == DBGZ_OK) {
-        rc = launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1);
-        if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0);
+        rc = launch_trsm(ctx, M, n, iii0, iii1, iii1 + 1, iv1, rank);
+        if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iii0, iii1, iii1 + 1, iv1, 0, rank);
       }
     }
     if (iv1 < n - 1 && rc == DBGZ_OK) {
-      rc = launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1);
-      if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0);
+      rc = launch_trsm(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, rank);
+      if (rc == DBGZ_OK) rc = launch_schur(ctx, M, n, iv0, iv1, iv1 + 1, n - 1, 0, rank);
     }
   }
   if (rc == DBGZ_OK) {

@@ -40,13 +40,25 @@ __global__ void k_adj_prepare(const double *U, const double *Ubar, int64_t d, do
   }
 }
 
-// r_i = sum_j G_ij R_ij with G = (S + S')/2, one thread per row, ascending j
-__global__ void k_adj_rowsum(const double *S, const double *R, int64_t d, double *r) {
+// r_i = sum_j G_ij R_ij with G = (S + S')/2 and R = U'U symmetric:
+// r = (row sums + column sums of S o R) / 2.  Row sums: one thread per row,
+// ascending j (coalesced over i); column sums: one warp per column
+// (contiguous), a fixed lane order and shuffle tree.
+__global__ void k_adj_rowsum(const double *S, const double *R, int64_t d, double *rs) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= d) return;
   double acc = 0.0;
-  for (int64_t j = 0; j < d; ++j) acc += 0.5 * (S[j * d + i] + S[i * d + j]) * R[j * d + i];
-  r[i] = acc;
+  for (int64_t j = 0; j < d; ++j) acc = fma(S[j * d + i], R[j * d + i], acc);
+  rs[i] = acc;
+}
+__global__ void k_adj_colsum(const double *S, const double *R, int64_t d, const double *rs, double *r) {
+  const int64_t i = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= d) return;
+  double acc = 0.0;
+  for (int64_t j = lane; j < d; j += 32) acc = fma(S[i * d + j], R[i * d + j], acc);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) r[i] = 0.5 * (rs[i] + acc);
 }
 
 // out[pi i, pi j] from the permuted-coordinate G, scaling and bound terms
@@ -88,8 +100,9 @@ int dbgz_sigma_adjoint_dev(dbgz_problem *p, const double *dU, const double *da, 
   const size_t nn = (size_t)d * d;
   cudaStream_t st = ctx->stream;
   DevBuf w;
-  DBGZ_TRY(dbgz_ensure(ctx, w, 8 * (6 * nn + (size_t)d) + 4096));
-  double *Uc = (double *)w.p, *T1 = Uc + nn, *M = T1 + nn, *R = M + nn, *V = R + nn, *X = V + nn, *r = X + nn;
+  DBGZ_TRY(dbgz_ensure(ctx, w, 8 * (6 * nn + 2 * (size_t)d) + 4096));
+  double *Uc = (double *)w.p, *T1 = Uc + nn, *M = T1 + nn, *R = M + nn, *V = R + nn, *X = V + nn, *r = X + nn,
+         *rs = r + d;
   int rc = DBGZ_OK;
   do {
     const dim3 g2((unsigned)((d + 255) / 256), (unsigned)d);
@@ -136,7 +149,9 @@ int dbgz_sigma_adjoint_dev(dbgz_problem *p, const double *dU, const double *da, 
       rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "sigma_adjoint: dense kernel launch failed (%s)", cudaGetErrorString(ce));
       break;
     }
-    k_adj_rowsum<<<(unsigned)((d + 127) / 128), 128, 0, st>>>(M, R, d, r);
+    k_adj_rowsum<<<(unsigned)((d + 127) / 128), 128, 0, st>>>(M, R, d, rs);
+    dbgz_count_launch(ctx);
+    k_adj_colsum<<<(unsigned)((d + 7) / 8), 256, 0, st>>>(M, R, d, rs, r);
     dbgz_count_launch(ctx);
     // T1 is free now: the result in original order
     k_adj_scatter<<<g2, 256, 0, st>>>(M, r, (const int64_t *)p->perm.p, (const double *)p->scale.p,

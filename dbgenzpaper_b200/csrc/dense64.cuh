@@ -232,17 +232,70 @@ __global__ void k_trinv64(const double *U, int64_t d, double *X) {
   for (int64_t i = c + 1 + threadIdx.x; i < d; i += blockDim.x) X[c * d + i] = 0.0;
 }
 
+// The same back substitution with the next column of U loaded into
+// registers while the current one is applied, and one barrier per step:
+// every thread forms x_r = rhs_r / U_rr itself (the same operation on the
+// same operands), so the step's only exchange is the right-hand side in
+// shared memory.  Thread t owns rows t + 128 q, q < Q (d <= 128 Q).
+template <int Q>
+__global__ void __launch_bounds__(128) k_trinv64_pf(const double *U, int64_t d, double *X) {
+  extern __shared__ double rhs[];
+  const int64_t c = blockIdx.x;
+  const int tid = threadIdx.x;
+  for (int64_t i = tid; i < d; i += 128) rhs[i] = i == c ? 1.0 : 0.0;
+  double ucur[Q], unext[Q];
+  double dcur = U[c * d + c], dnext = 1.0;
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int64_t i = tid + 128 * q;
+    ucur[q] = i < c ? U[c * d + i] : 0.0;
+  }
+  __syncthreads();
+  for (int64_t r = c; r >= 0; --r) {
+    if (r > 0) {
+      const double *un = U + (r - 1) * d;
+      dnext = un[r - 1];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int64_t i = tid + 128 * q;
+        unext[q] = i < r - 1 ? un[i] : 0.0;
+      }
+    }
+    const double xr = rhs[r] / dcur;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int64_t i = tid + 128 * q;
+      if (i < r) rhs[i] = fma(-ucur[q], xr, rhs[i]);
+    }
+    if (tid == 0) X[c * d + r] = xr;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) ucur[q] = unext[q];
+    dcur = dnext;
+  }
+  for (int64_t i = c + 1 + tid; i < d; i += 128) X[c * d + i] = 0.0;
+}
+
 inline size_t trinv64_smem(int64_t d) { return sizeof(double) * (size_t)d; }
 
-inline cudaError_t trinv64(const double *U, int64_t d, double *X, cudaStream_t st, int *launches = nullptr) {
+template <typename K>
+inline cudaError_t trinv64_launch(K kern, const double *U, int64_t d, double *X, cudaStream_t st) {
   const size_t smem = trinv64_smem(d);
   if (smem > 48 * 1024) {
-    const cudaError_t e = cudaFuncSetAttribute(k_trinv64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  k_trinv64<<<(unsigned)d, 128, smem, st>>>(U, d, X);
-  if (launches) ++*launches;
+  kern<<<(unsigned)d, 128, smem, st>>>(U, d, X);
   return cudaGetLastError();
+}
+
+inline cudaError_t trinv64(const double *U, int64_t d, double *X, cudaStream_t st, int *launches = nullptr) {
+  if (launches) ++*launches;
+  if (d <= 128 * 2) return trinv64_launch(k_trinv64_pf<2>, U, d, X, st);
+  if (d <= 128 * 4) return trinv64_launch(k_trinv64_pf<4>, U, d, X, st);
+  if (d <= 128 * 8) return trinv64_launch(k_trinv64_pf<8>, U, d, X, st);
+  if (d <= 128 * 16) return trinv64_launch(k_trinv64_pf<16>, U, d, X, st);
+  return trinv64_launch(k_trinv64, U, d, X, st);
 }
 
 }  // namespace

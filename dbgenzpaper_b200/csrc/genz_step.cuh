@@ -229,6 +229,19 @@ struct StepFp64 {
     double v = fma(2.0, u, -1.0);
     return kSqrt2 * erfinv(v);
   }
+  __device__ __forceinline__ void set_form(int) {}
+  // the state between two steps, as four doubles (checkpoints)
+  __device__ __forceinline__ void pack(double (&v)[4]) const {
+    v[0] = c;
+    v[1] = dc;
+    v[2] = p;
+    v[3] = 0.0;
+  }
+  __device__ __forceinline__ void unpack(const double (&v)[4]) {
+    c = v[0];
+    dc = v[1];
+    p = v[2];
+  }
   __device__ __forceinline__ void cdf(double s, double a, double b, double inv_u, int erfc_form) {
     double cv = (a - s) * inv_u;
     double dv = (b - s) * inv_u;
@@ -239,6 +252,36 @@ struct StepFp64 {
       dv = 0.5 * (1.0 + erf(dv)) - cv;
     } else {
       double c_val = 0.5 * erfc(-cv);
+      dv = 0.5 * erfc(-dv) - c_val;
+      cv = c_val;
+    }
+    c = cv;
+    dc = dv;
+    p *= dv;
+  }
+};
+
+// The FP64 step of a problem whose lower bounds are all -inf (P(X <= b)):
+// the lower argument is always clamped to -9, so its CDF value is one
+// constant, evaluated once per sample by the same function from the same
+// argument (hidden from constant folding) -- the same bits as the general
+// step, one erf (or erfc) per step fewer.
+struct StepFp64LowerInf : StepFp64 {
+  double cinf;  // the lower bound's CDF value in the pass's form (set_form)
+  __device__ __forceinline__ void set_form(int erfc_form) {
+    double m9 = -9.0;
+    asm volatile("" : "+d"(m9));
+    cinf = erfc_form ? 0.5 * erfc(-m9) : 0.5 * (1.0 + erf(m9));
+  }
+  __device__ __forceinline__ void cdf(double s, double /*a*/, double b, double inv_u, int erfc_form) {
+    double dv = (b - s) * inv_u;
+    dv = fmax(fmin(dv, 9.0), -9.0);
+    double cv;
+    if (!erfc_form) {
+      cv = cinf;
+      dv = 0.5 * (1.0 + erf(dv)) - cv;
+    } else {
+      const double c_val = cinf;
       dv = 0.5 * erfc(-dv) - c_val;
       cv = c_val;
     }
@@ -307,6 +350,21 @@ struct StepFp32 {
     const float y = phi_inv_lower_f32(fmaxf(arg, kEps));
     return lower ? y : -y;
   }
+  __device__ __forceinline__ void set_form(int) {}
+  // the state between two steps, as four doubles (checkpoints; the floats
+  // are exact in double)
+  __device__ __forceinline__ void pack(double (&v)[4]) const {
+    v[0] = lo;
+    v[1] = up;
+    v[2] = dc;
+    v[3] = p;
+  }
+  __device__ __forceinline__ void unpack(const double (&v)[4]) {
+    lo = (float)v[0];
+    up = (float)v[1];
+    dc = (float)v[2];
+    p = v[3];
+  }
   __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
     float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
     float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
@@ -325,6 +383,54 @@ struct StepFp32 {
     dc = d;
     p *= (double)d;
   }
+};
+
+// The FP32 step of a problem whose lower bounds are all -inf: the lower tail
+// argument is always -9, its tail mass one constant computed once per sample
+// by the same function from the same argument -- the same bits as StepFp32,
+// one tail mass per step fewer.
+struct StepFp32LowerInf : StepFp32 {
+  float ea9;
+  __device__ __forceinline__ void init(double c1, double dc1, double up1) {
+    StepFp32::init(c1, dc1, up1);
+    float nine = 9.0f;
+    asm volatile("" : "+f"(nine));
+    ea9 = tail_mass_f32(nine);
+  }
+  __device__ __forceinline__ void cdf(float s, float /*a*/, float b, float inv_u, int /*erfc_form*/) {
+    const float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
+    const float ea = ea9;
+    const float eb = tail_mass_f32(fabsf(xb));
+    // alpha = -9 < 0: the interval is in the lower tail or straddles 0
+    const bool lo_t = xb <= 0.0f;
+    float d = lo_t ? eb - ea : (1.0f - ea) - eb;
+    const bool need64 = lo_t && ea > 0.5f * eb;
+    if (need64) d = same_tail_mass64(-xb, 9.0f);
+    lo = ea;
+    up = lo_t ? 1.0f - eb : eb;
+    dc = d;
+    p *= (double)d;
+  }
+};
+
+// Step types of a working type, general and for all-lower-bounds -inf.
+template <typename T, bool kLowerInf>
+struct StepSel;
+template <>
+struct StepSel<double, false> {
+  using type = StepFp64;
+};
+template <>
+struct StepSel<double, true> {
+  using type = StepFp64LowerInf;
+};
+template <>
+struct StepSel<float, false> {
+  using type = StepFp32;
+};
+template <>
+struct StepSel<float, true> {
+  using type = StepFp32LowerInf;
 };
 
 }  // namespace dbgz

@@ -97,17 +97,52 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   DBGZ_TRY(dbgz_first_dim_cdf(p));
   if (precision != DBGZ_PREC_FP64 && !p->U32.p && !sparse) DBGZ_TRY(dbgz_make_U32(p));
   if (!p->Ub.p) DBGZ_TRY(dbgz_make_Ub(p));
+  // Banded problems with dimension checkpoints (ctx->grad_ckpt_seg > 0): the
+  // forward pass keeps, every `seg` y-indices, each sample's ring of the last
+  // W values and its recursion state (a checkpoint), and the adjoint then
+  // runs segment by segment from the last: the segment's y, s, dc recomputed
+  // from its checkpoint into a buffer of seg + 2 rows, the adjoint steps of
+  // the segment's variables on it, the adjoint's own ring and state carried
+  // to the next segment.  The same kernels and arithmetic as storing
+  // everything: the same bits, with the stored state of K = ceil((d-1)/seg)
+  // checkpoints instead of d rows.
+  const int64_t seg = sparse ? ctx->grad_ckpt_seg : 0;
+  const int64_t nY = d - 1, K = seg > 0 ? (nY + seg - 1) / seg : 0;
+  const bool ckpt = seg > 0 && K >= 1;
+  int64_t Wf = 0, Wb = 0;  // ring sizes of the forward and adjoint banded loops
+  if (ckpt) {
+    PassArgs sa{};
+    sa.d = d;
+    sa.m = m;
+    sa.n_reps = n_reps;
+    sa.qmc_type = p->qmc_type;
+    sa.n_bits = (int)o.n_bits;
+    sa.setup_only = true;
+    sa.kind = kLoopAdjoint;  // builds both CSCs
+    DBGZ_TRY(dbgz_loop_sparse(p, sa, precision, nullptr, 1));
+    Wf = p->bandwidth + 1;
+    Wb = p->bandwidth_b + 1;
+  }
+  const int64_t ck_rows = seg + 2;  // rows of a segment's recomputed state
   // samples per chunk: as many whole tiles as the context's state budget
   // allows (forward-store, adjoint, reduction and the dU GEMM run per chunk;
   // the GEMM accumulates across chunks)
-  const size_t tile_bytes = 128 * ((sparse ? 3 : 4) * esz * (size_t)d + 8) + 3 * 4 * 8 * (size_t)d;
+  const size_t state_per_sample =
+      ckpt ? (size_t)(K - 1) * (Wf * esz + 32) + (Wb * esz + 32) + 3 * ck_rows * esz
+           : (sparse ? 3 : 4) * esz * (size_t)d;
+  const size_t tile_bytes = 128 * (state_per_sample + 8) + 3 * 4 * 8 * (size_t)d;
   const int64_t chunk =
       std::max<int64_t>(1, std::min<int64_t>(n_tiles, (int64_t)(ctx->state_budget / tile_bytes)));
   const int64_t N = chunk * 128;
-  // one allocation: y, s, dc (+ p sbar on the dense path), p, 3 partial arrays, sums, dU
-  const size_t arr = esz * (size_t)d * N;
+  ctx->prof.grad_state_bytes = (int64_t)(state_per_sample * (size_t)N);
+  ctx->prof.grad_chunks = (n_tiles + chunk - 1) / chunk;
+  // one allocation: y, s, dc (+ p sbar on the dense path; a segment's rows
+  // with checkpoints), checkpoints, p, 3 partial arrays, sums, dU
+  const size_t arr = esz * (size_t)(ckpt ? ck_rows : d) * N;
+  const size_t ck_bytes = ckpt ? (size_t)(K - 1) * ((size_t)Wf * esz + 32) * N + ((size_t)Wb * esz + 32) * N : 0;
   const size_t part = sizeof(double) * (size_t)chunk * 4 * d;
-  const size_t total = (sparse ? 3 : 4) * arr + 8 * (size_t)N + 3 * part + 3 * 8 * (size_t)d * (kRedChunks + 1) +
+  const size_t total = (sparse ? 3 : 4) * arr + ck_bytes + 8 * 256 + 8 * (size_t)N + 3 * part +
+                       3 * 8 * (size_t)d * (kRedChunks + 1) +
                        (sparse ? 0 : esz * (size_t)d * d + 8 * (size_t)d * d) + 2 * 8 * (size_t)d +
                        8 * (size_t)n_tiles + 16384;
   DBGZ_TRY(dbgz_ensure(ctx, p->grad_buf, total));
@@ -123,6 +158,12 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   ga.s = take(arr);
   ga.dc = take(arr);
   ga.sbar = sparse ? nullptr : take(arr);
+  // checkpoints: slots 0..K-2 (forward: ring [Wf][N], state [4][N]) and the
+  // adjoint's carry (ring [Wb][N], state [4][N])
+  char *ck_ring = ckpt ? take((size_t)(K > 1 ? K - 1 : 1) * Wf * esz * N) : nullptr;
+  double *ck_state = ckpt ? (double *)take((size_t)(K > 1 ? K - 1 : 1) * 32 * N) : nullptr;
+  char *cr_ring = ckpt ? take((size_t)Wb * esz * N) : nullptr;
+  double *cr_state = ckpt ? (double *)take((size_t)32 * N) : nullptr;
   ga.p = (double *)take(8 * (size_t)N);
   ga.ga = (double *)take(part);
   ga.gb = (double *)take(part);
@@ -172,6 +213,13 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
     if (tensor) return dbgz_loop_umma(p, pa, precision, tiles, t1);
     return dbgz_loop_simt(p, pa, precision, tiles, t1);
   };
+  // a pass of the banded loop with the segment fields of pa as they stand
+  auto sparse_run = [&](int kind, int64_t t0, int64_t t1) -> int {
+    pa.kind = kind;
+    pa.tile0 = t0;
+    double *tiles = kind == kLoopAdjoint ? adj_tiles : (double *)p->partials.p;
+    return dbgz_loop_sparse(p, pa, precision, kind == kLoopForwardStore ? adj_tiles : tiles, t1);
+  };
   const bool want_U = dP_dU || dP_dSigma;
   DevBuf du_work;  // split partial tiles of the FP32 dU GEMM (back to the pool at the end, stream-ordered)
   struct Release {
@@ -180,9 +228,57 @@ static int grad_impl(dbgz_problem *p, int precision, double *result, double *err
   } release_du{du_work};
   for (int64_t t0 = 0; t0 < n_tiles; t0 += chunk) {
     const int64_t t1 = std::min(n_tiles, t0 + chunk);
-    // forward keeping the state, then the adjoint on the anti-transposed factor
-    DBGZ_TRY(run(kLoopForwardStore, t0, t1));
-    DBGZ_TRY(run(kLoopAdjoint, t0, t1));
+    if (!ckpt) {
+      // forward keeping the state, then the adjoint on the anti-transposed factor
+      DBGZ_TRY(run(kLoopForwardStore, t0, t1));
+      DBGZ_TRY(run(kLoopAdjoint, t0, t1));
+    } else {
+      // forward with checkpoints (and the tile sums of the estimate)
+      pa.store_p = 1;
+      pa.ck_save = 1;
+      pa.ck_ring = ck_ring;
+      pa.ck_state = ck_state;
+      pa.ck_seg = seg;
+      pa.ck_N = N;
+      DBGZ_TRY(run(kLoopForward, t0, t1));
+      pa.store_p = 0;
+      pa.ck_save = 0;
+      for (int64_t sg = K - 1; sg >= 0; --sg) {
+        // recompute the segment: steps [seg sg, seg (sg + 1)] (one past the
+        // segment: s and dc of its last variable come from the next step)
+        pa.i_begin = seg * sg;
+        pa.i_end = std::min(seg * (sg + 1) + 1, nY);
+        pa.ck_load = sg > 0;
+        pa.ck_in_ring = ck_ring + (size_t)(sg > 0 ? sg - 1 : 0) * Wf * esz * N;
+        pa.ck_in_state = ck_state + (size_t)(sg > 0 ? sg - 1 : 0) * 4 * N;
+        pa.io_row0 = seg * sg;
+        pa.io_rows = ck_rows;
+        pa.tile_finish = 0;
+        pa.kind = kLoopForwardStore;
+        pa.tile0 = t0;
+        DBGZ_TRY(sparse_run(kLoopForwardStore, t0, t1));
+        // the adjoint steps of variables seg sg + 1 .. min(seg (sg + 1), d - 1)
+        pa.i_begin = nY - std::min(seg * (sg + 1), nY);
+        pa.i_end = nY - seg * sg;
+        pa.ck_load = sg < K - 1;
+        pa.ck_in_ring = cr_ring;
+        pa.ck_in_state = cr_state;
+        pa.ck_save = sg > 0 ? 2 : 0;
+        pa.ck_ring = cr_ring;
+        pa.ck_state = cr_state;
+        pa.tile_finish = sg == 0;
+        DBGZ_TRY(sparse_run(kLoopAdjoint, t0, t1));
+        pa.ck_save = 0;
+        pa.ck_ring = ck_ring;
+        pa.ck_state = ck_state;
+      }
+      pa.i_begin = 0;
+      pa.i_end = -1;
+      pa.ck_load = 0;
+      pa.io_row0 = 0;
+      pa.io_rows = 0;
+      pa.tile_finish = 1;
+    }
     const int64_t rows = (t1 - t0) * 4, per = (rows + kRedChunks - 1) / kRedChunks;
     const int64_t n_chunks = (rows + per - 1) / per;
     k_reduce_rows<<<dim3((unsigned)((d + 127) / 128), (unsigned)n_chunks), 128, 0, ctx->stream>>>(

@@ -65,6 +65,9 @@ struct dbgz_ctx {
   size_t pool_bytes = 0;
   int64_t live_problems = 0;  // problems created on this context and not yet freed
   size_t state_budget = size_t(48) << 30;  // bytes of stored forward state a gradient call may hold
+  // banded gradients: dimensions per checkpoint segment (0: store the whole
+  // forward state instead)
+  int64_t grad_ckpt_seg = 256;
   BatchTuning batch_tune[4][2];            // [precision][qmc_type]
 };
 
@@ -120,6 +123,9 @@ struct dbgz_problem {
   DevBuf yws, partials, reps;
   double c1 = 0, dc1 = 0;
   bool c1_ready = false;
+  // every lower bound is -inf: the forward loops take the one-sided step
+  // (dbgz::StepFp64LowerInf / StepFp32LowerInf, the same bits)
+  bool lower_inf = false;
 };
 
 // ---- factorisation (chol.cu) -------------------------------------------
@@ -173,6 +179,22 @@ struct PassArgs {
   int64_t tile0 = 0;  // run tiles [tile0, n_tiles) only (sample chunks of the adjoint)
   const int64_t *gen_base_dev = nullptr;  // device copy of gen_base (device-driven passes)
   bool setup_only = false;  // make the launch's buffers and operands, launch nothing
+  // dimension segments (banded loop only, grad.cu): the pass runs the
+  // y-indices [i_begin, i_end) (i_end < 0: all); with ck_load it first restores
+  // each sample's ring of recent values and recursion state from ck_in; with
+  // ck_save = 1 it saves them before every y-index that is a multiple of
+  // ck_seg (slot index / ck_seg - 1), with ck_save = 2 once after i_end - 1
+  // (slot 0); per slot: ring [W][ck_N] of the pass's value type, state
+  // [4][ck_N] doubles.  tile_finish = 0 skips the per-tile end terms and sums.
+  int64_t i_begin = 0, i_end = -1;
+  int ck_load = 0, ck_save = 0, tile_finish = 1;
+  const void *ck_in_ring = nullptr;
+  const double *ck_in_state = nullptr;
+  void *ck_ring = nullptr;
+  double *ck_state = nullptr;
+  int64_t ck_seg = 0, ck_N = 0;
+  int64_t io_row0 = 0, io_rows = 0;  // rows of the stored-state arrays (0: all d from row 0)
+  int store_p = 0;
 };
 int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);

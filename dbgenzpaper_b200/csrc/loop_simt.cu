@@ -96,12 +96,20 @@ int launch_simt(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
 template <typename T, int GEN>
 int launch_kind(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
   switch (pa.kind) {
-    case kLoopForwardStore: return launch_simt<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
+    case kLoopForwardStore:
+      if (p->lower_inf)
+        return launch_simt<T, pol::Forward<T, GEN, true, typename dbgz::StepSel<T, true>::type>>(p, pa, partials,
+                                                                                             n_tiles);
+      return launch_simt<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
     case kLoopAdjoint: return launch_simt<T, pol::Adjoint<T, GEN>>(p, pa, partials, n_tiles);
     case kLoopLogWeight:
       return launch_simt<T, pol::Forward<T, GEN, false, typename pol::StepOf<T>::type, true>>(p, pa, partials,
                                                                                             n_tiles);
-    default: return launch_simt<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
+    default:
+      if (p->lower_inf)
+        return launch_simt<T, pol::Forward<T, GEN, false, typename dbgz::StepSel<T, true>::type>>(p, pa, partials,
+                                                                                              n_tiles);
+      return launch_simt<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
   }
 }
 

@@ -63,6 +63,15 @@ struct SparseParams {
   int max_block_nnz;       // staging capacity (entries)
   int64_t tile0;           // tiles [tile0, n_tiles) of the pass
   pol::GradIO<T> io;
+  // dimension segments (PassArgs, internal.cuh): y-indices [i_begin, i_end),
+  // checkpoint restore / save of the ring and the recursion state
+  int64_t i_begin, i_end;
+  int ck_load, ck_save, tile_finish;
+  const T *ck_in_ring;
+  const double *ck_in_state;
+  T *ck_ring;
+  double *ck_state;
+  int64_t ck_seg, ck_N;
 };
 
 // Policy: pol::Forward<T, GEN, STORE> or pol::Adjoint<T, GEN> (policies.cuh);
@@ -97,9 +106,26 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
     pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
     // this row's terms of the staged Sobol integers of the tile
     const dbgz::SobolLane sob_lane(r, (uint64_t)(P.gen.sobol_first + pl.gen.gen_base + (j - r)));
+    const int64_t gck = (tile - P.tile0) * TS + r;  // this sample's checkpoint column
+    // save / restore of the ring (slot order) and the recursion state
+    auto ck_store = [&](T *ring_out, double *state_out) {
+      for (int w = 0; w < W; ++w) ring_out[(int64_t)w * P.ck_N + gck] = yr[w * TS + r];
+      double v[4];
+      pl.pack(v);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) state_out[(int64_t)e * P.ck_N + gck] = v[e];
+    };
     int wslot = 0;  // ring slot of y-index i (i mod W)
-    for (int64_t i0 = 0; i0 < P.nY; i0 += CB) {
-      const int nb = (int)(P.nY - i0 < CB ? P.nY - i0 : CB);
+    if (P.ck_load) {
+      for (int w = 0; w < W; ++w) yr[w * TS + r] = P.ck_in_ring[(int64_t)w * P.ck_N + gck];
+      double v[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[e] = P.ck_in_state[(int64_t)e * P.ck_N + gck];
+      pl.unpack(v);
+      wslot = (int)(P.i_begin % W);
+    }
+    for (int64_t i0 = P.i_begin; i0 < P.i_end; i0 += CB) {
+      const int nb = (int)(P.i_end - i0 < CB ? P.i_end - i0 : CB);
       // stage the CSC columns i0+1 .. i0+nb (targets of y-indices i0..i0+nb-1)
       __syncthreads();
       const int64_t p0 = P.colptr[i0 + 1], p1 = P.colptr[i0 + nb + 1];
@@ -127,6 +153,10 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
 #pragma unroll 1
       for (int li = 0; li < nb; ++li) {
         const int64_t i = i0 + li;
+        if (P.ck_save == 1 && i > 0 && i % P.ck_seg == 0) {
+          const int64_t slot = i / P.ck_seg - 1;
+          ck_store(P.ck_ring + slot * (int64_t)W * P.ck_N, P.ck_state + slot * 4 * P.ck_N);
+        }
         uint32_t xs = 0u;
         if constexpr (Policy::kSobolTable)
           if (pl.gen.sobol_staged) xs = sob_lane.at(sob, li);
@@ -171,12 +201,15 @@ __global__ void __launch_bounds__(TS) k_genz_sparse(const SparseParams<T> P) {
         pl.consume(sg, s, li, i);
       }
     }
-    pl.tile_end(P.tgt, r, r >> 5, tile, j < P.m);
-    double pv = pl.tile_value(j < P.m);
-    for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
-    if ((r & 31) == 0) red[r >> 5] = pv;
-    __syncthreads();
-    if (r == 0) P.partials[tile] = ((red[0] + red[1]) + red[2]) + red[3];
+    if (P.ck_save == 2) ck_store(P.ck_ring, P.ck_state);
+    if (P.tile_finish) {
+      pl.tile_end(P.tgt, r, r >> 5, tile, j < P.m);
+      double pv = pl.tile_value(j < P.m);
+      for (int o = 16; o > 0; o >>= 1) pv += __shfl_down_sync(0xffffffffu, pv, o);
+      if ((r & 31) == 0) red[r >> 5] = pv;
+      __syncthreads();
+      if (r == 0) P.partials[tile] = ((red[0] + red[1]) + red[2]) + red[3];
+    }
   }
 }
 
@@ -304,6 +337,20 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
   P.io.gu = pa.grad.gu;
   P.io.dc1 = pa.grad.dc1;
   P.io.tile0 = pa.tile0;
+  P.io.row0 = pa.io_row0;
+  if (pa.io_rows > 0) P.io.rows = pa.io_rows;
+  P.io.store_p = pa.store_p;
+  P.i_begin = pa.i_begin;
+  P.i_end = pa.i_end < 0 ? P.nY : pa.i_end;
+  P.ck_load = pa.ck_load;
+  P.ck_save = pa.ck_save;
+  P.tile_finish = pa.tile_finish;
+  P.ck_in_ring = (const T *)pa.ck_in_ring;
+  P.ck_in_state = pa.ck_in_state;
+  P.ck_ring = (T *)pa.ck_ring;
+  P.ck_state = pa.ck_state;
+  P.ck_seg = pa.ck_seg > 0 ? pa.ck_seg : 1;
+  P.ck_N = pa.ck_N;
   const int64_t bwid = adj ? p->bandwidth_b : p->bandwidth;
   const int W = (int)std::min<int64_t>(bwid + 1, INT32_MAX / 2);
   P.W = W;
@@ -333,12 +380,20 @@ static int launch_sparse(dbgz_problem *p, const PassArgs &pa, double *partials, 
 template <typename T, int GEN>
 static int launch_sparse_kind(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n_tiles) {
   switch (pa.kind) {
-    case kLoopForwardStore: return launch_sparse<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
+    case kLoopForwardStore:
+      if (p->lower_inf)
+        return launch_sparse<T, pol::Forward<T, GEN, true, typename dbgz::StepSel<T, true>::type>>(p, pa, partials,
+                                                                                               n_tiles);
+      return launch_sparse<T, pol::Forward<T, GEN, true>>(p, pa, partials, n_tiles);
     case kLoopAdjoint: return launch_sparse<T, pol::Adjoint<T, GEN>>(p, pa, partials, n_tiles);
     case kLoopLogWeight:
       return launch_sparse<T, pol::Forward<T, GEN, false, typename pol::StepOf<T>::type, true>>(p, pa, partials,
                                                                                               n_tiles);
-    default: return launch_sparse<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
+    default:
+      if (p->lower_inf)
+        return launch_sparse<T, pol::Forward<T, GEN, false, typename dbgz::StepSel<T, true>::type>>(
+            p, pa, partials, n_tiles);
+      return launch_sparse<T, pol::Forward<T, GEN, false>>(p, pa, partials, n_tiles);
   }
 }
 

@@ -647,17 +647,23 @@ int encode_2d(dbgz_ctx *ctx, CUtensorMap *m, void *base, uint64_t inner, uint64_
 }
 
 template <int MODE, int GEN>
-auto pick_kind(const PassArgs &pa) -> decltype(&k_genz_umma<MODE, pol::Forward<float, GEN, false>>) {
+auto pick_kind(const PassArgs &pa, bool lower_inf)
+    -> decltype(&k_genz_umma<MODE, pol::Forward<float, GEN, false>>) {
   switch (pa.kind) {
-    case kLoopForwardStore: return k_genz_umma<MODE, pol::Forward<float, GEN, true>>;
+    case kLoopForwardStore:
+      if (lower_inf) return k_genz_umma<MODE, pol::Forward<float, GEN, true, dbgz::StepFp32LowerInf>>;
+      return k_genz_umma<MODE, pol::Forward<float, GEN, true>>;
     case kLoopAdjoint: return k_genz_umma<MODE, pol::Adjoint<float, GEN>>;
     case kLoopLogWeight: return k_genz_umma<MODE, pol::Forward<float, GEN, false, dbgz::StepFp32, true>>;
-    default: return k_genz_umma<MODE, pol::Forward<float, GEN, false>>;
+    default:
+      if (lower_inf) return k_genz_umma<MODE, pol::Forward<float, GEN, false, dbgz::StepFp32LowerInf>>;
+      return k_genz_umma<MODE, pol::Forward<float, GEN, false>>;
   }
 }
 template <int MODE>
-auto pick_kernel(const PassArgs &pa) -> decltype(pick_kind<MODE, 0>(pa)) {
-  return pa.qmc_type == DBGZ_QMC_SOBOL ? pick_kind<MODE, DBGZ_QMC_SOBOL>(pa) : pick_kind<MODE, DBGZ_QMC_RICHTMYER>(pa);
+auto pick_kernel(const PassArgs &pa, bool lower_inf) -> decltype(pick_kind<MODE, 0>(pa, false)) {
+  return pa.qmc_type == DBGZ_QMC_SOBOL ? pick_kind<MODE, DBGZ_QMC_SOBOL>(pa, lower_inf)
+                                       : pick_kind<MODE, DBGZ_QMC_RICHTMYER>(pa, lower_inf);
 }
 
 template <int MODE>
@@ -688,7 +694,7 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   if (!p->U32.p) DBGZ_TRY(dbgz_make_U32(p));
   const int Pw = 256;
   const int smem = umma_smem_bytes<MODE>(Pw, pa.qmc_type == DBGZ_QMC_SOBOL && !adj);
-  auto kern = pick_kernel<MODE>(pa);
+  auto kern = pick_kernel<MODE>(pa, p->lower_inf);
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   // CTAs per SM from the kernel's own resources: TMEM columns (512 / P),

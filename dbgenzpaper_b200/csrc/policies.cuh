@@ -79,9 +79,13 @@ struct GradIO {
   double *ga = nullptr, *gb = nullptr, *gu = nullptr;  // [((tile - tile0) * 4 + warp) * d + t]
   double dc1 = 0.0;   // dc of variable 0
   int64_t tile0 = 0;  // first tile of the sample chunk these arrays hold (sample g = (tile - tile0) * 128 + r)
+  // first row the arrays hold (a dimension segment's recomputed state holds
+  // rows row0 .. row0 + rows - 1)
+  int64_t row0 = 0;
+  int store_p = 0;    // a forward pass without stored state still writes p (checkpointed gradients)
   __device__ __forceinline__ int64_t at(int64_t row, int64_t g) const {
-    if (sizeof(T) == 4) return ((g >> 7) * rows + row) * 128 + (g & 127);
-    return row * N + g;
+    if (sizeof(T) == 4) return ((g >> 7) * rows + (row - row0)) * 128 + (g & 127);
+    return (row - row0) * N + g;
   }
 };
 
@@ -155,6 +159,7 @@ struct Forward {
     cdf_form = cdf_form_;
     io = io_;
     st.init(c1, dc1, up1);
+    st.set_form(cdf_form_);
     if (LOGW) lw = log(dc1);
   }
   // cooperative: r in [0, 128)
@@ -203,11 +208,14 @@ struct Forward {
   }
   // value of this sample added to the tile's sum of p
   __device__ __forceinline__ double tile_value(bool valid) {
-    if (STORE) io.p[g] = valid ? st.p : 0.0;
+    if (STORE || io.store_p) io.p[g] = valid ? st.p : 0.0;
     if (LOGW) io.p[g] = valid ? lw : -INFINITY;
     return valid ? st.p : 0.0;
   }
   __device__ __forceinline__ void tile_end(const typename TgtT<T>::type *, int, int, int64_t, bool) {}
+  // the recursion's state between two steps (checkpoints of the banded gradient)
+  __device__ __forceinline__ void pack(double (&v)[4]) const { st.pack(v); }
+  __device__ __forceinline__ void unpack(const double (&v)[4]) { st.unpack(v); }
 };
 
 // x rounded to the nearest TF32 value (low 13 mantissa bits zero)
@@ -561,6 +569,12 @@ struct Adjoint {
     }
   }
   __device__ __forceinline__ void consume(const Staged<T> &, T r_sum, int, int64_t) { ybar = (double)r_sum; }
+  // the recursion's state between two steps (segments of the banded gradient)
+  __device__ __forceinline__ void pack(double (&v)[4]) const {
+    v[0] = ybar;
+    v[1] = v[2] = v[3] = 0.0;
+  }
+  __device__ __forceinline__ void unpack(const double (&v)[4]) { ybar = v[0]; }
 
   __device__ __forceinline__ double tile_value(bool) { return 0.0; }
   // variable 0 after the last step: its CDF has no conditioning sum and no

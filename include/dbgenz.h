@@ -117,6 +117,13 @@ int dbgz_release_cached(dbgz_ctx *ctx, uint64_t *freed_bytes);
  * counts run the forward and adjoint passes in chunks of whole 128-sample
  * tiles (default 48 GiB).  No reference counterpart. */
 int dbgz_set_state_budget(dbgz_ctx *ctx, uint64_t bytes);
+/* Banded (QMCDataSparse) gradients keep, instead of every sample's forward
+ * state, a checkpoint every `segment` dimensions (the band's recent values
+ * and the recursion state) and recompute each segment's state from its
+ * checkpoint just before the adjoint sweeps it (default 256; 0 stores the
+ * whole forward state as the dense path does).  The results are the same
+ * bits either way.  No reference counterpart. */
+int dbgz_set_grad_checkpoints(dbgz_ctx *ctx, int64_t segment);
 const char *dbgz_last_error(const dbgz_ctx *ctx);
 
 /* Device-side timing of the library's own work, measured with CUDA events
@@ -131,6 +138,8 @@ typedef struct dbgz_profile {
   double prepare_ms;        /* last dbgz_prepare: upload + factorisation    */
   int64_t prepare_launches; /* kernels the last dbgz_prepare launched       */
   double sigma_adjoint_ms;  /* last dbgz_problem_sigma_adjoint              */
+  int64_t grad_state_bytes; /* last gradient call: stored forward state     */
+  int64_t grad_chunks;      /* last gradient call: sample chunks it ran     */
 } dbgz_profile;
 int dbgz_set_profiling(dbgz_ctx *ctx, int enable);
 int dbgz_get_profile(const dbgz_ctx *ctx, dbgz_profile *out);

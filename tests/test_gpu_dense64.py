@@ -93,7 +93,7 @@ def test_gemm_split_k_strict_upper_accumulate(lib, splits):
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-10)
 
 
-@pytest.mark.parametrize("d", [1, 5, 64, 333])
+@pytest.mark.parametrize("d", [1, 5, 64, 333, 1000, 1500, 2500])
 def test_trinv(lib, d):
     rng = np.random.default_rng(d)
     A = rng.standard_normal((d, d + 5))

@@ -307,3 +307,32 @@ def test_banded_gradient_chunked_and_fp32(dbgz):
             assert np.linalg.norm(x - y) <= 2e-3 * np.linalg.norm(y)
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_FP32_SIMT])
+@pytest.mark.parametrize("qmc,seg,n,band", [("Richtmyer", 32, 150, 6), ("Sobol", 64, 300, 40), ("Sobol", 256, 700, 40),
+                                            ("Richtmyer", 5, 40, 3), ("Richtmyer", 100, 90, 6)])
+def test_banded_gradient_checkpoints_same_bits(dbgz, prec, qmc, seg, n, band):
+    # dimension checkpoints (a checkpoint every `seg` dimensions, each segment
+    # recomputed before the adjoint sweeps it) against storing the whole
+    # forward state: the same kernels on the same values, so P and the
+    # gradients are the same bits; also with the samples split in chunks
+    D = dbgz
+    ctx = D.Context(0)
+    try:
+        S, lo, up, sh = _banded(n, 93 + n)
+        Q = _banded_problem(D, S, lo, up, sh, band, m=600, sobol=qmc == "Sobol", context=ctx)
+        ctx.set_grad_checkpoints(0)
+        full = D.qmc_pnorm_grad(Q, precision=prec)
+        ctx.set_grad_checkpoints(seg)
+        ck = D.qmc_pnorm_grad(Q, precision=prec)
+        ctx.set_state_budget(2 << 20)  # several chunks of tiles
+        ckc = D.qmc_pnorm_grad(Q, precision=prec)
+        Q.close()
+        assert ck[0] == full[0] and ck[1] == full[1]
+        assert np.array_equal(ck[3], full[3]) and np.array_equal(ck[4], full[4])
+        assert ckc[0] == full[0]
+        for x, y in zip(ckc[3:5], full[3:5]):
+            assert np.linalg.norm(x - y) <= 1e-11 * np.linalg.norm(y)
+    finally:
+        ctx.close()

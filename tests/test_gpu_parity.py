@@ -460,3 +460,30 @@ def test_pnorm_sparse_vs_checker(D, oracle, n, band, qmc):
     np.testing.assert_allclose(reps, rc, rtol=1e-12, atol=1e-300)
     P32, _, _, r32 = D.qmc_pnorm(Q, precision=L.PREC_FP32_SIMT, return_reps=True)
     assert abs(P32 - Pc) <= 5e-6 + 2e-5 * abs(Pc), (P32, Pc)
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP64, L.PREC_FP32_SIMT, L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32])
+@pytest.mark.parametrize("gen,sparse", [("Richtmyer", False), ("Sobol", False), ("Sobol", True)])
+def test_one_sided_step_same_bits(D, prec, gen, sparse):
+    # with every lower bound -inf the loops take the one-sided step (the lower
+    # CDF value is one constant); a = -1e300 takes the general step through
+    # the same clamped argument: the per-shift means must be the same bits
+    if sparse and prec in (L.PREC_FP32_SPLIT_BF16, L.PREC_FP32_TF32):
+        pytest.skip("the banded loop has no tensor-core modes")
+    n, m, R = 150, 1000, 3
+    S = _spd(n, 17)
+    rng = np.random.default_rng(18)
+    b = rng.uniform(-1.0, 2.5, n)
+    opts = D.QMC_opts(m=m, n_reps=R, max_pts=2 * m, max_abs_err=0.0)
+    kw = dict(shifts=rng.random((n - 1, R))) if gen == "Richtmyer" else \
+        dict(qmc_type="Sobol", ushifts=rng.integers(0, 2**64, size=(n - 1, R), dtype=np.uint64))
+    cls = D.QMCDataSparse if sparse else D.QMCData
+    out = []
+    for lo in (-np.inf, -1e300):
+        Q = cls(S, np.full(n, lo), b, opts, **kw)
+        try:
+            out.append(D.qmc_pnorm(Q, precision=prec, return_reps=True))
+        finally:
+            Q.close()
+    assert out[0][2] == out[1][2] == 2 * m
+    assert np.array_equal(out[0][3], out[1][3]) and out[0][0] == out[1][0]
