@@ -42,14 +42,14 @@ METRIC = "d=1000 MVN P time at |err|<=1e-5 vs FP64: mixed-prec vs FP64 GPU; grad
 UNIT = "ms"
 MIXED = "fp32_split_bf16"   # mixed-precision mode of the headline number
 # DRAM bytes of one 2^21-sample launch of the split-BF16 loop at d=1000 (ncu capture of a
-# 131,072-sample launch: 0.239 GB read + 0.347 GB written, scaled by the sample count)
-TRAFFIC_PER_LAUNCH = 16 * (238.68e6 + 347.43e6)
+# 131,072-sample launch: 0.249 GB read + 0.348 GB written, scaled by the sample count)
+TRAFFIC_PER_LAUNCH = 16 * (248.69e6 + 347.87e6)
 # warp instructions of one split-BF16 loop launch at d = 1000 per sample (ncu
-# smsp__inst_executed.sum of a 131,072-sample launch: 8.717e8), and its
+# smsp__inst_executed.sum of a 131,072-sample launch: 7.412e8), and its
 # XU (special-function) pipe share; the issue roofline below scales it to the
 # timed launch
-INST_PER_SAMPLE = 8.717e8 / 131072
-XU_PIPE_PCT = 15.3
+INST_PER_SAMPLE = 7.412e8 / 131072
+XU_PIPE_PCT = 12.3
 ISSUE_PROFILE = "profiles/genz_umma_splitbf16_d1000_8192pts_full.md"
 
 
@@ -427,6 +427,15 @@ def run_c5(args, emit=True):
                          "sample_chunks": int(prof.grad_chunks),
                          "full_state_bytes": int(w.m * w.n_reps * 3 * 4 * w.d)}
     out["grad_state"]["fraction_of_full"] = out["grad_state"]["bytes"] / out["grad_state"]["full_state_bytes"]
+    # the alternative: every sample's forward state stored, in sample chunks
+    # within the context's state budget (no recomputation)
+    ctx.set_grad_checkpoints(0)
+    g0, out["fp32_grad_full_state_ms"] = timed(lambda: D.qmc_pnorm_grad(Q, precision=L.PREC_FP32_SIMT),
+                                               max(1, args.steps // 2))
+    lib.dbgz_get_profile(ctx.handle, C.byref(prof))
+    out["grad_full_state"] = {"bytes_per_chunk": int(prof.grad_state_bytes), "sample_chunks": int(prof.grad_chunks),
+                              "same_gradient": bool(np.array_equal(g0[4], g[4]) and g0[0] == g[0])}
+    ctx.set_grad_checkpoints(256)
     Q.close()
     samples = float(w.m * w.n_reps)
     line = {
@@ -437,6 +446,7 @@ def run_c5(args, emit=True):
                    "samples": samples},
         "modes": out, "P_fp32": P32, "P_fp64": P64, "abs_err_fp32_vs_fp64": abs(P32 - P64),
         "qmc_3sem_fp64": e64, "grad_over_fwd": out["fp32_grad_ms"] / out["fp32_ms"],
+        "grad_full_state_over_fwd": out["fp32_grad_full_state_ms"] / out["fp32_ms"],
         "dP_db_norm": float(np.linalg.norm(g[4])), "P_grad_call": g[0],
         "sample_dims_per_s_fp32": samples * (w.d - 1) / (out["fp32_ms"] * 1e-3),
     }
