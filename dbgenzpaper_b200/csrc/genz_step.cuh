@@ -102,22 +102,23 @@ __device__ __forceinline__ uint32_t sobol_warp(const uint32_t *Vl, uint64_t idx)
 // bits), [5 + a] = V[0], V[1] XORed by the bits of a, [9 + b] = V[2..4] by
 // the bits of b.  A step then reads three words (SobolLane::at).
 //
-// sobol_stage_block: the 128 threads r of a tile together (all lanes of
-// their four warps), warp w filling entries 8w..8w+7 of a block of 32: entry
-// li < nv is dimension l0 + dir li when that lies in [0, lmax]; tile first
-// index base0, shift row ush (the shift of dimension l at ush[l]).
+// sobol_stage_entries: the 32 lanes of one warp together fill entries
+// li0 .. li0 + n - 1 of a block of 32: entry li < nv is dimension l0 + dir li
+// when that lies in [0, lmax]; tile first index base0, shift row ush (the
+// shift of dimension l at ush[l]).
 constexpr int kSobolRow = 17;  // words per staged dimension
-__device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[kSobolRow], const uint32_t *V,
-                                                  const uint64_t *ush, uint64_t base0, int64_t l0, int dir,
-                                                  int64_t lmax, int nv, int r) {
+template <int UNROLL>
+__device__ __forceinline__ void sobol_stage_entries(uint32_t (*tab)[kSobolRow], const uint32_t *V,
+                                                    const uint64_t *ush, uint64_t base0, int64_t l0, int dir,
+                                                    int64_t lmax, int nv, int li0, int n) {
   const uint64_t B = base0 & ~31ull;
   const uint32_t gB = (uint32_t)(B ^ (B >> 1));
-  const int wid = r >> 5, ln = r & 31;
+  const int ln = (int)(threadIdx.x & 31);
   // lanes 1..4: bit 5 + ctz(c + ln) of the recurrence (c = B / 32)
   const int zb = (ln >= 1 && ln <= 4) ? 5 + __ffsll((long long)((B >> 5) + (uint64_t)ln)) - 1 : 32;
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const int li = wid * 8 + q;
+#pragma unroll UNROLL
+  for (int q = 0; q < n; ++q) {
+    const int li = li0 + q;
     const int64_t l = l0 + dir * li;
     const bool ok = li < nv && l >= 0 && l <= lmax;
     // x(B): lane k contributes V[k] when bit k of gray(B) is set
@@ -149,6 +150,13 @@ __device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[kSobolRow], co
     }
     if (ln < 17) tab[li][ln] = x;
   }
+}
+// The 128 threads r of a tile together (all lanes of their four warps), warp
+// w filling entries 8w..8w+7.
+__device__ __forceinline__ void sobol_stage_block(uint32_t (*tab)[kSobolRow], const uint32_t *V,
+                                                  const uint64_t *ush, uint64_t base0, int64_t l0, int dir,
+                                                  int64_t lmax, int nv, int r) {
+  sobol_stage_entries<8>(tab, V, ush, base0, l0, dir, lmax, nv, 8 * (r >> 5), 8);
 }
 
 // The shifted integer of tile row r in block dimension li, for the tile
@@ -365,23 +373,57 @@ struct StepFp32 {
     dc = (float)v[2];
     p = v[3];
   }
-  __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
-    float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
-    float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
+  // The tails and the FP32 difference of the interval's masses; need64: the
+  // interval lies in one tail and that difference cancels (the masses are
+  // within a factor 2).
+  __device__ __forceinline__ float cdf_core(float s, float a, float b, float inv_u, float &x0, float &x1,
+                                            bool &need64) {
+    const float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
+    const float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
     const float ea = tail_mass_f32(fabsf(xa));  // mass beyond |alpha| on its side
     const float eb = tail_mass_f32(fabsf(xb));
     // both bounds in the upper tail (hi_t), both in the lower tail (lo_t), or
     // alpha < 0 < beta; selects rather than branches (the step is a serial
     // chain per sample, and branch resolution stalls it)
     const bool hi_t = xa >= 0.0f, lo_t = !hi_t && xb <= 0.0f;
-    float d = hi_t ? ea - eb : (lo_t ? eb - ea : (1.0f - ea) - eb);
-    // the FP32 difference of two close tail masses cancels: FP64 then
-    const bool need64 = (hi_t && eb > 0.5f * ea) || (lo_t && ea > 0.5f * eb);
-    if (need64) d = same_tail_mass64(hi_t ? xa : -xb, hi_t ? xb : -xa);
+    const float d = hi_t ? ea - eb : (lo_t ? eb - ea : (1.0f - ea) - eb);
+    need64 = (hi_t && eb > 0.5f * ea) || (lo_t && ea > 0.5f * eb);
+    x0 = hi_t ? xa : -xb;
+    x1 = hi_t ? xb : -xa;
     lo = hi_t ? 1.0f - ea : ea;
     up = lo_t ? 1.0f - eb : eb;
+    return d;
+  }
+  // The exact factor of a step whose FP32 difference cancels, from the same
+  // inputs (the same x0, x1 bits as cdf_core).
+  static __device__ __forceinline__ float tail_exact(float s, float a, float b, float inv_u) {
+    const float xa = fminf(fmaxf((a - s) * inv_u, -9.0f), 9.0f);
+    const float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
+    const bool hi_t = xa >= 0.0f;
+    return same_tail_mass64(hi_t ? xa : -xb, hi_t ? xb : -xa);
+  }
+  __device__ __forceinline__ void cdf(float s, float a, float b, float inv_u, int /*erfc_form*/) {
+    float x0, x1;
+    bool need64;
+    float d = cdf_core(s, a, b, inv_u, x0, x1, need64);
+    if (need64) d = same_tail_mass64(x0, x1);
     dc = d;
     p *= (double)d;
+  }
+  // cdf without the branch: where the FP32 difference cancels, dc keeps it
+  // and the weight is not multiplied; the caller multiplies the exact factor
+  // (tail_exact) in later.  The next step's u takes dc at the FP32 tail
+  // masses' own accuracy either way (in one tail, u or 1 - u lies between
+  // the two masses and dc's absolute error is at most theirs); the weight
+  // needs dc to relative accuracy, so its factor waits for the exact value.
+  // Returns whether the factor was left out.
+  __device__ __forceinline__ bool cdf_deferred(float s, float a, float b, float inv_u) {
+    float x0, x1;
+    bool need64;
+    const float d = cdf_core(s, a, b, inv_u, x0, x1, need64);
+    dc = d;
+    p *= (double)(need64 ? 1.0f : d);
+    return need64;
   }
 };
 
@@ -397,19 +439,35 @@ struct StepFp32LowerInf : StepFp32 {
     asm volatile("" : "+f"(nine));
     ea9 = tail_mass_f32(nine);
   }
-  __device__ __forceinline__ void cdf(float s, float /*a*/, float b, float inv_u, int /*erfc_form*/) {
+  __device__ __forceinline__ float cdf_core(float s, float b, float inv_u, bool &need64) {
     const float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
     const float ea = ea9;
     const float eb = tail_mass_f32(fabsf(xb));
     // alpha = -9 < 0: the interval is in the lower tail or straddles 0
     const bool lo_t = xb <= 0.0f;
-    float d = lo_t ? eb - ea : (1.0f - ea) - eb;
-    const bool need64 = lo_t && ea > 0.5f * eb;
-    if (need64) d = same_tail_mass64(-xb, 9.0f);
+    const float d = lo_t ? eb - ea : (1.0f - ea) - eb;
+    need64 = lo_t && ea > 0.5f * eb;
     lo = ea;
     up = lo_t ? 1.0f - eb : eb;
+    return d;
+  }
+  static __device__ __forceinline__ float tail_exact(float s, float /*a*/, float b, float inv_u) {
+    const float xb = fminf(fmaxf((b - s) * inv_u, -9.0f), 9.0f);
+    return same_tail_mass64(-xb, 9.0f);
+  }
+  __device__ __forceinline__ void cdf(float s, float /*a*/, float b, float inv_u, int /*erfc_form*/) {
+    bool need64;
+    float d = cdf_core(s, b, inv_u, need64);
+    if (need64) d = tail_exact(s, 0.0f, b, inv_u);
     dc = d;
     p *= (double)d;
+  }
+  __device__ __forceinline__ bool cdf_deferred(float s, float /*a*/, float b, float inv_u) {
+    bool need64;
+    const float d = cdf_core(s, b, inv_u, need64);
+    dc = d;
+    p *= (double)(need64 ? 1.0f : d);
+    return need64;
   }
 };
 

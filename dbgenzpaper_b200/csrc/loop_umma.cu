@@ -130,6 +130,10 @@ struct Misc {
   pol::Staged<float> sg[2];
   double red[4];
   uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
+  // staging buffers: filled by the producer warp (32 cp.async arrivals when
+  // its copies land + 32 arrivals after its own writes), released by the
+  // sample threads after the block
+  uint64_t stg_full[2], stg_free[2];
   uint32_t tmem_base;
   int abort;
   // Sobol integers of the block's dimensions (dbgz::sobol_stage_block); last,
@@ -207,6 +211,8 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       mbar_init(&ms->a_free[i], 1);
       mbar_init(&ms->b_full[i], 1);
       mbar_init(&ms->b_free[i], 1);
+      mbar_init(&ms->stg_full[i], 64);
+      mbar_init(&ms->stg_free[i], 1);
     }
     mbar_init(&ms->bar_s, 1);
     mbar_init(&ms->ws_ready, 1);
@@ -232,25 +238,74 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
   const uint32_t tmem = ms->tmem_base;
 
   if (warp == kProdWarp) {
-    // ---------------------------------------------------------------- TMA
-    if (lane == 0) {
-      uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0}, ws_cnt = 0;
-      uint32_t ja = 0, jb = 0;
-      bool ok = true;
-      for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles && ok; it += gridDim.x) {
-        const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
-        const CUtensorMap *tmu = BATCH ? pb->tm_u : P.tm_u;
-        const int64_t nYi = BATCH ? pb->nY : P.nY, nphase = BATCH ? 1 : nphase1;
-        if (BATCH) {
-          // the maps were written by a host copy before the launch: order
-          // them before the tensor-map proxy reads them (system scope, as the
-          // writer is the host)
-          for (int pp = 0; pp < F::NPART; ++pp)
-            asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(&tmu[pp]) : "memory");
-        }
-        for (int64_t ph = 0; ph < nphase && ok; ++ph) {
-          const Phase f = phase_of(P.P, nYi, ph);
-          if (ph > 0) {
+    // ---------------------------------------------- TMA and block staging
+    // Lane 0 issues the TMA loads (phase starts, U^T panels).  All 32 lanes
+    // stage each block's U triangle, per-dimension constants and Sobol
+    // integers for the sample threads, one block ahead of them (copies by
+    // cp.async that arrive on stg_full when they land; stg_free is the
+    // sample threads' release of a buffer).
+    uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0}, ws_cnt = 0;
+    uint32_t ja = 0, jb = 0;
+    uint32_t st_use[2] = {0, 0}, st_n = 0;  // stagings per buffer, in all
+    bool ok = true;
+    int64_t sit = P.tile0 + blockIdx.x, slb = 0;  // the next block to stage: tile, first y-index
+    auto stage_next = [&]() -> bool {
+      if (sit >= P.n_tiles) return true;
+      const int buf = (int)(st_n & 1);
+      bool w = true;
+      if (st_use[buf] > 0) w = mbar_wait(&ms->stg_free[buf], (st_use[buf] - 1) & 1, abort);
+      if (!__all_sync(0xffffffffu, w)) return false;  // the warp decides together
+      const UmmaProb *pb = BATCH ? P.probs + P.item_prob[sit] : nullptr;
+      const int64_t tile = BATCH ? (int64_t)P.item_tile[sit] : sit;
+      const int64_t dI = BATCH ? pb->d : P.d, nYI = BATCH ? pb->nY : P.nY;
+      const float *U32I = BATCH ? pb->U32 : P.U32;
+      const TargetParams32 *tgtI = BATCH ? pb->tgt : P.tgt;
+      Policy pp;
+      if (BATCH)
+        pp.tile_begin(pb->gen, dI, tile, pb->tiles_per_shift, lane, pb->first[0], pb->first[1], pb->first[2], 0,
+                      P.io);
+      else
+        pp.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, lane, P.c1, P.dc1, P.up1, 0, P.io);
+      const int nv = (int)(nYI - slb < BK ? nYI - slb : BK);
+      // ublk[li][ti] = U[slb + li, slb + ti + 1] for li <= ti < nv, else 0
+#pragma unroll 8
+      for (int ti = 0; ti < BK; ++ti) {
+        const bool v = lane <= ti && ti < nv;
+        pol::cp_async_or_zero<4>(&ms->ublk[buf][lane][ti], v ? U32I + (slb + ti + 1) * dI + slb + lane : U32I, v);
+      }
+      pp.stage_async(ms->sg[buf], tgtI, lane, slb, nv);
+      cp_async_mbar_arrive(&ms->stg_full[buf]);
+      if constexpr (Policy::kSobolTable)
+        if (pp.gen.sobol_staged)
+          dbgz::sobol_stage_entries<1>(ms->sob[buf], pp.gen.V, pp.gen.ushift + pp.k * (dI - 1),
+                                       (uint64_t)(pp.gen.sobol_first + pp.gen.gen_base + (pp.j - lane)),
+                                       pp.sobol_l0(slb), Policy::kSobolDir, dI - 2, nv, 0, BK);
+      mbar_arrive(&ms->stg_full[buf]);
+      ++st_use[buf];
+      ++st_n;
+      slb += BK;
+      if (slb >= nYI) {
+        slb = 0;
+        sit += gridDim.x;
+      }
+      return true;
+    };
+    ok = __all_sync(0xffffffffu, stage_next());  // the CTA's first block
+    for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles && ok; it += gridDim.x) {
+      const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
+      const CUtensorMap *tmu = BATCH ? pb->tm_u : P.tm_u;
+      const int64_t nYi = BATCH ? pb->nY : P.nY, nphase = BATCH ? 1 : nphase1;
+      if (BATCH && lane == 0) {
+        // the maps were written by a host copy before the launch: order
+        // them before the tensor-map proxy reads them (system scope, as the
+        // writer is the host)
+        for (int pp = 0; pp < F::NPART; ++pp)
+          asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(&tmu[pp]) : "memory");
+      }
+      for (int64_t ph = 0; ph < nphase && ok; ++ph) {
+        const Phase f = phase_of(P.P, nYi, ph);
+        if (ph > 0) {
+          if (lane == 0) {
             ok = mbar_wait(&ms->ws_ready, ws_cnt & 1, abort);
             ++ws_cnt;
             const int nbox = (f.Pr + 63) / 64;
@@ -274,38 +329,45 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               ++jb;
             }
           }
-          for (int b = 0; b < f.nb && ok; ++b) {
-            const int ia = ja & 1, ib = jb & 1;
-            ++a_use[ia];  // the sample threads fill this A tile
+          ok = __all_sync(0xffffffffu, ok);
+        }
+        for (int b = 0; b < f.nb && ok; ++b) {
+          if (lane == 0) {
+            const int ib = jb & 1;
+            ++a_use[ja & 1];  // the sample threads fill this A tile
             ++ja;
             if (b_use[ib] > 0) ok = mbar_wait(&ms->b_free[ib], (b_use[ib] - 1) & 1, abort);
-            if (!ok) break;
-            if (b < f.nb - 1) {
-              const int rows = f.Pr - BK * (b + 1);
-              const int nbox = (rows + 63) / 64;
-              mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
-              for (int pp = 0; pp < F::NPART; ++pp)
-                for (int i = 0; i < nbox; ++i)
-                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &tmu[pp],
-                              (int32_t)(f.L + BK * b), (int32_t)(f.L + 1 + BK * (b + 1) + 64 * i),
-                              &ms->b_full[ib]);
-            } else {
-              mbar_arrive(&ms->b_full[ib]);
+            if (ok) {
+              if (b < f.nb - 1) {
+                const int rows = f.Pr - BK * (b + 1);
+                const int nbox = (rows + 63) / 64;
+                mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
+                for (int pp = 0; pp < F::NPART; ++pp)
+                  for (int i = 0; i < nbox; ++i)
+                    tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &tmu[pp],
+                                (int32_t)(f.L + BK * b), (int32_t)(f.L + 1 + BK * (b + 1) + 64 * i),
+                                &ms->b_full[ib]);
+              } else {
+                mbar_arrive(&ms->b_full[ib]);
+              }
+              ++b_use[ib];
+              ++jb;
             }
-            ++b_use[ib];
-            ++jb;
           }
-        }
-      }
-      if (!ok) {
-        set_abort(ms, P.status);
-        // let loads already issued land before the CTA leaves
-        for (int i = 0; i < 2; ++i) {
-          if (a_use[i] > 0) mbar_wait(&ms->a_full[i], (a_use[i] - 1) & 1, abort);
-          if (b_use[i] > 0) mbar_wait(&ms->b_full[i], (b_use[i] - 1) & 1, abort);
+          ok = __all_sync(0xffffffffu, ok);
+          if (ok) ok = __all_sync(0xffffffffu, stage_next());  // the block after this one
         }
       }
     }
+    if (!ok && lane == 0) {
+      set_abort(ms, P.status);
+      // let loads already issued land before the CTA leaves
+      for (int i = 0; i < 2; ++i) {
+        if (a_use[i] > 0) mbar_wait(&ms->a_full[i], (a_use[i] - 1) & 1, abort);
+        if (b_use[i] > 0) mbar_wait(&ms->b_full[i], (b_use[i] - 1) & 1, abort);
+      }
+    }
+    pol::cp_async_wait_all();
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA
     if (lane == 0) {
@@ -405,7 +467,6 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       const int64_t tile = BATCH ? (int64_t)P.item_tile[it] : it;
       const int64_t dI = BATCH ? pb->d : P.d, nYI = BATCH ? pb->nY : P.nY, mI = BATCH ? pb->m : P.m;
       const int64_t tpsI = BATCH ? pb->tiles_per_shift : P.tiles_per_shift;
-      const float *U32I = BATCH ? pb->U32 : P.U32;
       const TargetParams32 *tgtI = BATCH ? pb->tgt : P.tgt;
       double *partsI = BATCH ? pb->partials : P.partials;
       const int64_t nphase = BATCH ? 1 : nphase1;
@@ -419,21 +480,6 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
       // this row's terms of the staged Sobol integers of the tile
       const dbgz::SobolLane sob_lane(r, (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)));
-      // asynchronous staging of one block into buffer `buf` (one commit group)
-      auto stage_block = [&](int buf, int64_t lb, int nv) {
-        for (int e = r; e < BK * BK; e += TS) {
-          const int li = e % BK, ti = e / BK;
-          const bool v = li <= ti && ti < nv;
-          pol::cp_async_or_zero<4>(&ms->ublk[buf][li][ti], v ? U32I + (lb + ti + 1) * dI + lb + li : U32I, v);
-        }
-        pl.stage_async(ms->sg[buf], tgtI, r, lb, nv);
-        if constexpr (Policy::kSobolTable)
-          if (pl.gen.sobol_staged)
-            dbgz::sobol_stage_block(ms->sob[buf], pl.gen.V, pl.gen.ushift + pl.k * (dI - 1),
-                                    (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)), pl.sobol_l0(lb),
-                                    Policy::kSobolDir, dI - 2, nv, r);
-        pol::cp_async_commit();
-      };
       for (int64_t ph = 0; ph < nphase; ++ph) {
         const Phase f = phase_of(P.P, nYI, ph);
         if (ph > 0) {
@@ -447,25 +493,18 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           const int64_t lbase = f.L + BK * b;
           const int nval = (int)((nYI - lbase) < BK ? (nYI - lbase) : BK);
           const int cur = (int)(blk & 1);
-          // the block's U triangle and per-dimension constants: staged during
-          // the previous block of the tile, or now for the tile's first block
-          if (ph == 0 && b == 0) stage_block(cur, lbase, nval);
-          pol::cp_async_wait_all();
-          named_sync(kBarScalar, TS);
-          if (lbase + BK < nYI) {
-            const int64_t nb2 = nYI - lbase - BK;
-            stage_block(cur ^ 1, lbase + BK, (int)(nb2 < BK ? nb2 : BK));
-          }
+          // the block's U triangle and per-dimension constants, staged by the
+          // producer warp during the previous block
+          bool ok = mbar_wait(&ms->stg_full[cur], (blk >> 1) & 1, abort);
           float(*ublk)[kUld] = ms->ublk[cur];
           const pol::Staged<float> &sgc = ms->sg[cur];
           // partial sums of the block's targets, accumulated by the tensor cores
           float s[BK];
-          bool ok = true;
           if (ph == 0 && b == 0) {
 #pragma unroll
             for (int t = 0; t < BK; ++t) s[t] = 0.f;
           } else {
-            ok = mbar_wait(&ms->bar_s, s_cnt & 1, abort);
+            ok = mbar_wait(&ms->bar_s, s_cnt & 1, abort) && ok;
             ++s_cnt;
             tc_fence_after();
             uint32_t v[BK];
@@ -512,7 +551,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                   const float uu[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
                   for (int t = k; t < 8; ++t) s[t] = fmaf(y, uu[t], s[t]);
-                  pl.consume(sgc, s[k], li, l);
+                  if constexpr (Policy::kDeferTail)
+                    pl.consume_deferred(sgc, s[k], li, l, k);
+                  else
+                    pl.consume(sgc, s[k], li, l);
                 }
                 ys[k] = y;
               }
@@ -520,6 +562,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               if (nval - 8 * ch >= 8) steps(std::false_type{});
               else steps(std::true_type{});
               pl.chunk_end(lbase + 8 * ch, nval - 8 * ch);
+              if constexpr (Policy::kDeferTail) pl.tail_repair(sgc, s, 8 * ch, lbase + 8 * ch);
               switch (ch) {
                 case 0: rank8_update<24>(s, ys, &ublk[0][8]); break;
                 case 1: rank8_update<16>(s, ys, &ublk[8][16]); break;
@@ -557,6 +600,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           named_sync(kBarScalar, TS);
           if (r == 0) {
             mbar_arrive(&ms->a_full[ia]);
+            mbar_arrive(&ms->stg_free[cur]);
             if (need_ws && ph < nphase - 1) {
               for (int pp = 0; pp < F::NPART; ++pp)
                 tma_store_2d(&P.tm_y[pp], (int32_t)lbase, slot_row, abuf + ia * SM::ABYTES + pp * SM::APART);

@@ -32,6 +32,8 @@
 // seed (p replaced by 1) and per-sample results are scaled by p when they
 // are accumulated.
 #pragma once
+#include <type_traits>
+
 #include "internal.cuh"
 #include "genz_step.cuh"
 
@@ -129,6 +131,9 @@ struct StepOf<float> {
 template <typename T, int GEN, bool STORE, typename Step = typename StepOf<T>::type, bool LOGW = false>
 struct Forward {
   static constexpr bool kPlain = !STORE;  // a forward pass that keeps no state
+  // consume_deferred + tail_repair available (the FP32 steps): the loop may
+  // run a chunk of steps without the same-tail branch
+  static constexpr bool kDeferTail = std::is_same<T, float>::value;
   // takes staged Sobol integers (GenParams::sobol_staged); not in the pass
   // that keeps the state for the adjoint (measured on the banded d = 10^4,
   // bandwidth 64 workload at 2^14 x 10 Sobol points:
@@ -139,6 +144,7 @@ struct Forward {
   __device__ __forceinline__ int64_t sobol_l0(int64_t lbase) const { return lbase; }
   Step st;
   double lw;  // LOGW: log of the weight so far
+  uint32_t rmask;  // steps k of the current chunk whose weight factor consume_deferred left out
   dbgz::GenParams gen;
   int64_t j, k, g;  // point index in the pass, shift, global sample index
   int64_t d;
@@ -161,6 +167,7 @@ struct Forward {
     st.init(c1, dc1, up1);
     st.set_form(cdf_form_);
     if (LOGW) lw = log(dc1);
+    rmask = 0u;
   }
   // cooperative: r in [0, 128)
   __device__ __forceinline__ void stage(Staged<T> &sg, const typename TgtT<T>::type *tgt, int r,
@@ -206,6 +213,43 @@ struct Forward {
       io.dc[io.at(l + 1, g)] = (T)st.dc;
     }
   }
+  // consume for step k (0..7) of a chunk, without the same-tail branch
+  // (Step::cdf_deferred): a factor left out is recorded in rmask and
+  // multiplied in by tail_repair at the chunk's end
+  __device__ __forceinline__ void consume_deferred(const Staged<T> &sg, T s, int li, int64_t l, int k) {
+    const auto tg = sg.tg[li];
+    const bool left = st.cdf_deferred(s, tg.a, tg.b, tg.inv_u);
+    rmask |= left ? (1u << k) : 0u;
+    if (LOGW) lw += left ? 0.0 : log((double)st.dc);
+    if (STORE) {
+      io.s[io.at(l + 1, g)] = s;
+      io.dc[io.at(l + 1, g)] = (T)st.dc;
+    }
+  }
+  // The factors consume_deferred left out in a chunk of 8 steps starting at
+  // staged index li0 (y-index l0), from the same sums s[0..7] (the chunk's
+  // consumed values, still in place): one warp-uniform branch per chunk,
+  // taken only when some sample of the warp had such a step.  The weight
+  // then has the same factors as with cdf, the FP64 products in another order.
+  template <int N>
+  __device__ __forceinline__ void tail_repair(const Staged<T> &sg, const T (&s)[N], int li0, int64_t l0) {
+    if (__any_sync(0xffffffffu, rmask != 0u)) {
+      // one call site: the step's sum picked by selects (a dynamic index
+      // would put s[] in local memory)
+      for (uint32_t m = rmask; m != 0u; m &= m - 1u) {
+        const int k = __ffs((int)m) - 1;
+        T sk = s[0];
+#pragma unroll
+        for (int kk = 1; kk < 8; ++kk) sk = k == kk ? s[kk] : sk;
+        const auto tg = sg.tg[li0 + k];
+        const float d = Step::tail_exact(sk, tg.a, tg.b, tg.inv_u);
+        st.p *= (double)d;
+        if (LOGW) lw += log((double)d);
+        if (STORE) io.dc[io.at(l0 + k + 1, g)] = d;
+      }
+      rmask = 0u;
+    }
+  }
   // value of this sample added to the tile's sum of p
   __device__ __forceinline__ double tile_value(bool valid) {
     if (STORE || io.store_p) io.p[g] = valid ? st.p : 0.0;
@@ -229,6 +273,7 @@ __device__ __forceinline__ float tf32_rn(float x) {
 template <typename T, int GEN>
 struct Adjoint {
   static constexpr bool kPlain = false;
+  static constexpr bool kDeferTail = false;
   // takes staged Sobol integers (GenParams::sobol_staged) where the loop
   // stages them; the QMC dimension of step li of a block: d - 1 - lbase - li
   static constexpr bool kSobolTable = GEN == DBGZ_QMC_SOBOL;
