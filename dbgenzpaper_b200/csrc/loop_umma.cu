@@ -91,18 +91,39 @@ struct __align__(64) UmmaParams {
   const int32_t *item_prob, *item_tile;
 };
 
-struct Phase {
-  int64_t L;
-  int Pr, nb;
-};
-__device__ __forceinline__ Phase phase_of(int Pw, int64_t nY, int64_t ph) {
-  Phase f;
-  f.L = ph * Pw;
-  int64_t w = nY - f.L;
-  if (w > Pw) w = Pw;
-  f.Pr = (int)((w + BK - 1) / BK) * BK;
-  f.nb = f.Pr / BK;
-  return f;
+// Block schedule of a tile.  y-block X (X = 0 .. nblk - 1) holds y-indices
+// 32X .. 32X + 31, and its targets are those indices + 1.  TMEM holds the
+// partial sums of two halves of 128 targets: half h (the targets of blocks
+// 4h .. 4h + 3) in columns 128 (h & 1) + 0 .. 127, so that a half's columns
+// are free for the half after next as soon as its last block has read them.
+constexpr int HB = 4;    // blocks per half
+constexpr int HC = 128;  // TMEM columns per half
+__device__ __forceinline__ uint32_t tcol(int64_t X) {
+  return (uint32_t)(((X >> 2) & 1) * HC + BK * (X & 3));
+}
+// The last target block that the MMA after block X adds block X's y's to:
+// the rest of X's half and the next half, and after the last block of a
+// half also the half after that (the first contribution to its columns).
+__device__ __forceinline__ int64_t last_target(int64_t X, int64_t nblk) {
+  const int64_t h = X >> 2;
+  const int64_t e = (X & 3) == 3 ? 4 * h + 11 : 4 * h + 7;
+  return e < nblk - 1 ? e : nblk - 1;
+}
+// Re-initialisation of half g >= 2: the contributions of y-blocks
+// 0 .. 4g - 6 to its targets (those of blocks 4g - 5 .. 4g - 1 come from the
+// per-block MMAs), as K chunks of one y-block each, issued after the MMAs of
+// blocks 4g - 5 .. 4g - 2, a quarter each, while the sample threads work on
+// half g - 1.  Block X carries chunks [c0, c1) of half g (empty: c0 == c1).
+__device__ __forceinline__ void reinit_share(int64_t X, int64_t nblk, int64_t &g, int64_t &c0, int64_t &c1) {
+  g = c0 = c1 = 0;
+  if (X < 3) return;
+  const int64_t q = (X + 1) & 3;  // X = 4h + 3 + q
+  const int64_t h = (X - 3 - q) >> 2;
+  if (4 * (h + 2) >= nblk) return;  // no half h + 2
+  g = h + 2;
+  const int64_t n = 4 * h + 3;
+  c0 = q * n / 4;
+  c1 = (q + 1) * n / 4;
 }
 
 __device__ __forceinline__ void named_sync(int id, int n) {
@@ -129,7 +150,11 @@ struct Misc {
   float ublk[2][BK][kUld];
   pol::Staged<float> sg[2];
   double red[4];
-  uint64_t a_full[2], a_free[2], b_full[2], b_free[2], bar_s, ws_ready, drain;
+  // A tiles: a_full (the sample threads wrote a block's y's), a_free (its MMA
+  // is done), a_stored (the producer's store of it to the workspace has read
+  // it, or it needed none); stages (U^T panels, re-initialisation chunks):
+  // b_full, b_free
+  uint64_t a_full[2], a_free[2], a_stored[2], b_full[2], b_free[2], bar_s, drain;
   // staging buffers: filled by the producer warp (32 cp.async arrivals when
   // its copies land + 32 arrivals after its own writes), released by the
   // sample threads after the block
@@ -201,21 +226,25 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
   Misc *ms = reinterpret_cast<Misc *>(sm + SM::off_misc(P.P));
   volatile int *abort = &ms->abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t nphase1 = (P.nY + P.P - 1) / P.P;  // phases of the single problem
-  const int32_t slot_row = (int32_t)blockIdx.x * TS;
-  const int bpart = SM::bpart(P.P);
+  const int32_t slot_row = (int32_t)blockIdx.x * TS;  // this CTA's rows of the y workspace
+  const int bpart = SM::bpart(P.P);                  // one part of a U^T panel in a stage
+  constexpr int kRows = 2 * 64;                      // U^T rows of a re-initialisation chunk
+  constexpr int rpart = kRows * F::ROWB;             // one part of its B, after its A
+  const uint32_t stage_bytes = (uint32_t)SM::bbytes(P.P);
+  static_assert(SM::ABYTES + kRows * F::ROWB * F::NPART <= 256 * F::ROWB * F::NPART,
+                "a re-initialisation chunk fills one stage");
 
   if (tid == 0) {
     for (int i = 0; i < 2; ++i) {
       mbar_init(&ms->a_full[i], 1);
       mbar_init(&ms->a_free[i], 1);
+      mbar_init(&ms->a_stored[i], 1);
       mbar_init(&ms->b_full[i], 1);
       mbar_init(&ms->b_free[i], 1);
       mbar_init(&ms->stg_full[i], 64);
       mbar_init(&ms->stg_free[i], 1);
     }
     mbar_init(&ms->bar_s, 1);
-    mbar_init(&ms->ws_ready, 1);
     mbar_init(&ms->drain, 1);
     ms->abort = 0;
     fence_mbar_init();
@@ -239,13 +268,14 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
 
   if (warp == kProdWarp) {
     // ---------------------------------------------- TMA and block staging
-    // Lane 0 issues the TMA loads (phase starts, U^T panels).  All 32 lanes
-    // stage each block's U triangle, per-dimension constants and Sobol
-    // integers for the sample threads, one block ahead of them (copies by
-    // cp.async that arrive on stg_full when they land; stg_free is the
-    // sample threads' release of a buffer).
-    uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0}, ws_cnt = 0;
-    uint32_t ja = 0, jb = 0;
+    // Lane 0 issues the TMA traffic: the stage ring (per-block U^T panels
+    // and re-initialisation chunks, in the order the MMA warp takes them) and
+    // the stores of the y's to the workspace.  All 32 lanes stage each
+    // block's U triangle, per-dimension constants and Sobol integers for the
+    // sample threads, one block ahead of them (copies by cp.async that arrive
+    // on stg_full when they land; stg_free is the sample threads' release of
+    // a buffer).
+    uint32_t b_use[2] = {0, 0}, jb = 0;
     uint32_t st_use[2] = {0, 0}, st_n = 0;  // stagings per buffer, in all
     bool ok = true;
     int64_t sit = P.tile0 + blockIdx.x, slb = 0;  // the next block to stage: tile, first y-index
@@ -290,11 +320,28 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       }
       return true;
     };
+    // lane 0: the next stage of the ring (U^T panel or re-initialisation
+    // chunk), loaded by `load(stage, full barrier)`
+    auto push = [&](auto &&load) -> bool {
+      const int ib = (int)(jb & 1);
+      if (b_use[ib] > 0 && !mbar_wait(&ms->b_free[ib], (b_use[ib] - 1) & 1, abort)) return false;
+      load(bst + ib * stage_bytes, &ms->b_full[ib]);
+      ++b_use[ib];
+      ++jb;
+      return true;
+    };
+    bool prev_store = false;  // the previous block's y's go to the workspace
+    int64_t prev_lb = 0;      // its first y-index
+    uint32_t n = 0;           // blocks of this CTA so far
     ok = __all_sync(0xffffffffu, stage_next());  // the CTA's first block
     for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles && ok; it += gridDim.x) {
       const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
       const CUtensorMap *tmu = BATCH ? pb->tm_u : P.tm_u;
-      const int64_t nYi = BATCH ? pb->nY : P.nY, nphase = BATCH ? 1 : nphase1;
+      const int64_t nYi = BATCH ? pb->nY : P.nY;
+      const int64_t nblk = (nYi + BK - 1) / BK;
+      // later halves are re-initialised from the workspace (halves 0 and 1
+      // take every contribution from the per-block MMAs)
+      const bool need_ws = !BATCH && nblk > 2 * HB;
       if (BATCH && lane == 0) {
         // the maps were written by a host copy before the launch: order
         // them before the tensor-map proxy reads them (system scope, as the
@@ -302,85 +349,95 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         for (int pp = 0; pp < F::NPART; ++pp)
           asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(&tmu[pp]) : "memory");
       }
-      for (int64_t ph = 0; ph < nphase && ok; ++ph) {
-        const Phase f = phase_of(P.P, nYi, ph);
-        if (ph > 0) {
-          if (lane == 0) {
-            ok = mbar_wait(&ms->ws_ready, ws_cnt & 1, abort);
-            ++ws_cnt;
-            const int nbox = (f.Pr + 63) / 64;
-            for (int64_t kc = 0; kc < f.L / BK && ok; ++kc) {
-              const int ia = ja & 1, ib = jb & 1;
-              if (a_use[ia] > 0) ok = ok && mbar_wait(&ms->a_free[ia], (a_use[ia] - 1) & 1, abort);
-              if (b_use[ib] > 0) ok = ok && mbar_wait(&ms->b_free[ib], (b_use[ib] - 1) & 1, abort);
-              if (!ok) break;
-              mbar_arrive_expect_tx(&ms->a_full[ia], SM::ABYTES);
-              for (int pp = 0; pp < F::NPART; ++pp)
-                tma_load_2d(abuf + ia * SM::ABYTES + pp * SM::APART, &P.tm_y[pp], (int32_t)(kc * BK),
-                            slot_row, &ms->a_full[ia]);
-              mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
+      for (int64_t X = 0; X < nblk && ok; ++X, ++n) {
+        // 1. the U^T panel of the MMA after block X: rows of target blocks
+        //    X + 1 .. last_target, K = block X's y-indices (the last block of
+        //    the tile has no MMA: an empty stage)
+        if (lane == 0)
+          ok = push([&](unsigned char *st, uint64_t *full) {
+            if (X < nblk - 1) {
+              const int rows = BK * (int)(last_target(X, nblk) - X);
+              const int nbox = (rows + 63) / 64;
+              mbar_arrive_expect_tx(full, (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
               for (int pp = 0; pp < F::NPART; ++pp)
                 for (int i = 0; i < nbox; ++i)
-                  tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &tmu[pp],
-                              (int32_t)(kc * BK), (int32_t)(f.L + 1 + 64 * i), &ms->b_full[ib]);
-              ++a_use[ia];
-              ++b_use[ib];
-              ++ja;
-              ++jb;
+                  tma_load_2d(st + pp * bpart + i * 64 * F::ROWB, &tmu[pp], (int32_t)(BK * X),
+                              (int32_t)(BK * (X + 1) + 1 + 64 * i), full);
+            } else {
+              mbar_arrive(full);
             }
+          });
+        ok = __all_sync(0xffffffffu, ok);
+        // 2. the staging of the block after this one
+        if (ok) ok = __all_sync(0xffffffffu, stage_next());
+        if (lane == 0 && ok && n > 0) {
+          // 3. the previous block's A tile, once the sample threads are done
+          //    with it: its y's to the workspace where a re-initialisation
+          //    reads them, then released for reuse
+          const int pa = (int)((n - 1) & 1);
+          ok = mbar_wait(&ms->a_full[pa], ((n - 1) >> 1) & 1, abort);
+          if (ok && prev_store) {
+            for (int pp = 0; pp < F::NPART; ++pp)
+              tma_store_2d(&P.tm_y[pp], (int32_t)prev_lb, slot_row, abuf + pa * SM::ABYTES + pp * SM::APART);
+            bulk_commit();
+            bulk_wait_read_all();
           }
-          ok = __all_sync(0xffffffffu, ok);
+          if (ok) mbar_arrive(&ms->a_stored[pa]);
         }
-        for (int b = 0; b < f.nb && ok; ++b) {
-          if (lane == 0) {
-            const int ib = jb & 1;
-            ++a_use[ja & 1];  // the sample threads fill this A tile
-            ++ja;
-            if (b_use[ib] > 0) ok = mbar_wait(&ms->b_free[ib], (b_use[ib] - 1) & 1, abort);
-            if (ok) {
-              if (b < f.nb - 1) {
-                const int rows = f.Pr - BK * (b + 1);
-                const int nbox = (rows + 63) / 64;
-                mbar_arrive_expect_tx(&ms->b_full[ib], (uint32_t)(nbox * 64 * F::ROWB * F::NPART));
-                for (int pp = 0; pp < F::NPART; ++pp)
-                  for (int i = 0; i < nbox; ++i)
-                    tma_load_2d(bst + ib * SM::bbytes(P.P) + pp * bpart + i * 64 * F::ROWB, &tmu[pp],
-                                (int32_t)(f.L + BK * b), (int32_t)(f.L + 1 + BK * (b + 1) + 64 * i),
-                                &ms->b_full[ib]);
-              } else {
-                mbar_arrive(&ms->b_full[ib]);
-              }
-              ++b_use[ib];
-              ++jb;
-            }
+        // y-blocks that a re-initialisation reads: up to 4 g - 6 for the last half g
+        prev_store = need_ws && X <= 4 * ((nblk + HB - 1) / HB) - 10;
+        prev_lb = BK * X;
+        // 4. the re-initialisation chunks carried by block X (the MMA warp
+        //    issues them after block X's MMA)
+        if (lane == 0 && ok) {
+          int64_t g, c0, c1;
+          reinit_share(X, nblk, g, c0, c1);
+          for (int64_t kc = c0; kc < c1 && ok; ++kc) {
+            // y-block kc must be in the workspace: its store is the newest
+            // (block X - 1) or an older one
+            if (kc == X - 1)
+              bulk_wait_all();
+            else
+              bulk_wait_all_but_1();
+            ok = push([&](unsigned char *st, uint64_t *full) {
+              mbar_arrive_expect_tx(full, (uint32_t)(SM::ABYTES + kRows * F::ROWB * F::NPART));
+              for (int pp = 0; pp < F::NPART; ++pp)
+                tma_load_2d(st + pp * SM::APART, &P.tm_y[pp], (int32_t)(BK * kc), slot_row, full);
+              for (int pp = 0; pp < F::NPART; ++pp)
+                for (int i = 0; i < kRows / 64; ++i)
+                  tma_load_2d(st + SM::ABYTES + pp * rpart + i * 64 * F::ROWB, &tmu[pp], (int32_t)(BK * kc),
+                              (int32_t)(HC * g + 1 + 64 * i), full);
+            });
           }
-          ok = __all_sync(0xffffffffu, ok);
-          if (ok) ok = __all_sync(0xffffffffu, stage_next());  // the block after this one
         }
+        ok = __all_sync(0xffffffffu, ok);
       }
     }
     if (!ok && lane == 0) {
       set_abort(ms, P.status);
-      // let loads already issued land before the CTA leaves
-      for (int i = 0; i < 2; ++i) {
-        if (a_use[i] > 0) mbar_wait(&ms->a_full[i], (a_use[i] - 1) & 1, abort);
-        if (b_use[i] > 0) mbar_wait(&ms->b_full[i], (b_use[i] - 1) & 1, abort);
-      }
+      // let loads already issued land before the CTA leaves (waits that do
+      // not stop at the abort flag, bounded all the same)
+      for (int i = 0; i < 2; ++i)
+        if (b_use[i] > 0) mbar_wait_drain(&ms->b_full[i], (b_use[i] - 1) & 1);
     }
+    if (lane == 0) bulk_wait_all();
     pol::cp_async_wait_all();
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------------- MMA
+    // Per block X: the MMA of block X's y's into the partial sums of target
+    // blocks X + 1 .. last_target (the next block's 32 columns first,
+    // committed to bar_s), then the re-initialisation chunks block X carries.
     if (lane == 0) {
       uint32_t a_use[2] = {0, 0}, b_use[2] = {0, 0};
       uint32_t ja = 0, jb = 0;
       bool ok = true;
       const uint32_t sbo = F::ATOM;
-      auto issue = [&](uint32_t d_col, int ncols, uint32_t a_addr, uint32_t b_addr, bool overwrite) {
+      auto issue = [&](uint32_t d_col, int ncols, uint32_t a_addr, uint32_t b_addr, uint32_t b_part, bool overwrite) {
         // D[:, d_col .. d_col+ncols) (+)= A[128 x 32] * B[ncols x 32]^T; split
-        // BF16 as hi*hi + hi*lo + lo*hi.
+        // BF16 as hi*hi + hi*lo + lo*hi (parts SM::APART / b_part apart).
         for (int c0 = 0; c0 < ncols; c0 += 256) {
-          const int n = ncols - c0 < 256 ? ncols - c0 : 256;
-          const uint32_t idesc = instr_desc(F::IDESC_FMT, F::IDESC_FMT, 128, (uint32_t)n);
+          const int nn = ncols - c0 < 256 ? ncols - c0 : 256;
+          const uint32_t idesc = instr_desc(F::IDESC_FMT, F::IDESC_FMT, 128, (uint32_t)nn);
           const uint32_t bo = (uint32_t)(c0 * F::ROWB);
           for (int ks = 0; ks < F::NKS; ++ks) {
             const uint32_t acc0 = (overwrite && ks == 0) ? 0u : 1u;
@@ -388,7 +445,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
             const uint64_t b0 = smem_desc(b_addr + bo + 32 * ks, sbo, F::LAYOUT);
             if (MODE == DBGZ_PREC_FP32_SPLIT_BF16) {
               const uint64_t a1 = smem_desc(a_addr + SM::APART + 32 * ks, sbo, F::LAYOUT);
-              const uint64_t b1 = smem_desc(b_addr + bpart + bo + 32 * ks, sbo, F::LAYOUT);
+              const uint64_t b1 = smem_desc(b_addr + b_part + bo + 32 * ks, sbo, F::LAYOUT);
               mma_f16(tmem + d_col + c0, a0, b0, idesc, acc0);
               mma_f16(tmem + d_col + c0, a0, b1, idesc, 1u);
               mma_f16(tmem + d_col + c0, a1, b0, idesc, 1u);
@@ -399,49 +456,54 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         }
       };
       for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles && ok; it += gridDim.x) {
-        const int64_t nYi = BATCH ? P.probs[P.item_prob[it]].nY : P.nY, nphase = BATCH ? 1 : nphase1;
-        for (int64_t ph = 0; ph < nphase && ok; ++ph) {
-          const Phase f = phase_of(P.P, nYi, ph);
-          const int64_t nkc = ph > 0 ? f.L / BK : 0;
-          for (int64_t kc = 0; kc < nkc && ok; ++kc) {
-            const int ia = ja & 1, ib = jb & 1;
-            ok = mbar_wait(&ms->a_full[ia], a_use[ia] & 1, abort) &&
-                 mbar_wait(&ms->b_full[ib], b_use[ib] & 1, abort);
-            if (!ok) break;
-            tc_fence_after();
-            issue(0, f.Pr, smem_u32(abuf + ia * SM::ABYTES), smem_u32(bst + ib * SM::bbytes(P.P)),
-                  kc == 0);
+        const int64_t nYi = BATCH ? P.probs[P.item_prob[it]].nY : P.nY;
+        const int64_t nblk = (nYi + BK - 1) / BK;
+        for (int64_t X = 0; X < nblk && ok; ++X) {
+          const int ia = ja & 1, ib = jb & 1;
+          ok = mbar_wait(&ms->a_full[ia], a_use[ia] & 1, abort) &&
+               mbar_wait(&ms->b_full[ib], b_use[ib] & 1, abort);
+          if (!ok) break;
+          tc_fence_after();
+          if (X < nblk - 1) {
+            const uint32_t aa = smem_u32(abuf + ia * SM::ABYTES);
+            const uint32_t bb = smem_u32(bst + ib * stage_bytes);
+            const int64_t E = last_target(X, nblk), h = X >> 2;
+            // the first MMA of a tile writes the columns it touches; the MMA
+            // after the last block of half h is the first into half h + 2
+            issue(tcol(X + 1), BK, aa, bb, (uint32_t)bpart, X == 0);  // the next block's columns
+            mma_commit(&ms->bar_s);
+            for (int64_t Y = X + 2; Y <= E;) {
+              // target blocks Y .. Ye of one half: contiguous columns
+              const int64_t Yh = Y >> 2;
+              const int64_t Ye = 4 * Yh + 3 < E ? 4 * Yh + 3 : E;
+              issue(tcol(Y), (int)(BK * (Ye - Y + 1)), aa, bb + (uint32_t)(BK * (Y - X - 1) * F::ROWB),
+                    (uint32_t)bpart, X == 0 || Yh == h + 2);
+              Y = Ye + 1;
+            }
             mma_commit(&ms->a_free[ia]);
             mma_commit(&ms->b_free[ib]);
-            if (kc == nkc - 1) mma_commit(&ms->bar_s);
-            ++a_use[ia];
-            ++b_use[ib];
-            ++ja;
-            ++jb;
+          } else {
+            mbar_arrive(&ms->a_free[ia]);
+            mbar_arrive(&ms->b_free[ib]);
           }
-          for (int b = 0; b < f.nb && ok; ++b) {
-            const int ia = ja & 1, ib = jb & 1;
-            ok = mbar_wait(&ms->a_full[ia], a_use[ia] & 1, abort) &&
-                 mbar_wait(&ms->b_full[ib], b_use[ib] & 1, abort);
+          ++a_use[ia];
+          ++b_use[ib];
+          ++ja;
+          ++jb;
+          // re-initialisation chunks: D = half g's columns, A = y-block kc
+          // (from the workspace), B = U^T rows of half g's targets
+          int64_t g, c0, c1;
+          reinit_share(X, nblk, g, c0, c1);
+          const int nbg = (int)(nblk - HB * g < HB ? nblk - HB * g : HB);
+          for (int64_t kc = c0; kc < c1 && ok; ++kc) {
+            const int ic = jb & 1;
+            ok = mbar_wait(&ms->b_full[ic], b_use[ic] & 1, abort);
             if (!ok) break;
             tc_fence_after();
-            if (b < f.nb - 1) {
-              const bool first = (ph == 0 && b == 0);
-              const uint32_t aa = smem_u32(abuf + ia * SM::ABYTES);
-              const uint32_t bb = smem_u32(bst + ib * SM::bbytes(P.P));
-              issue((uint32_t)(BK * (b + 1)), BK, aa, bb, first);  // next block's columns
-              mma_commit(&ms->bar_s);
-              const int rest = f.Pr - BK * (b + 2);
-              if (rest > 0) issue((uint32_t)(BK * (b + 2)), rest, aa, bb + BK * F::ROWB, first);
-              mma_commit(&ms->a_free[ia]);
-              mma_commit(&ms->b_free[ib]);
-            } else {
-              mbar_arrive(&ms->a_free[ia]);
-              mbar_arrive(&ms->b_free[ib]);
-            }
-            ++a_use[ia];
-            ++b_use[ib];
-            ++ja;
+            const uint32_t st = smem_u32(bst + ic * stage_bytes);
+            issue((uint32_t)((g & 1) * HC), BK * nbg, st, st + SM::ABYTES, (uint32_t)rpart, false);
+            mma_commit(&ms->b_free[ic]);
+            ++b_use[ic];
             ++jb;
           }
         }
@@ -450,17 +512,14 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       mma_commit(&ms->drain);
       if (!mbar_wait(&ms->drain, 0, abort)) {
         // abort was raised elsewhere: still give the tensor cores time to finish
-        const uint64_t t0 = globaltimer();
-        while (!mbar_try_wait(&ms->drain, 0) && globaltimer() - t0 < kWaitLimitNs) {
-        }
+        mbar_wait_drain(&ms->drain, 0);
       }
     }
   } else {
     // ------------------------------------------------------ sample threads
     const int r = tid;  // sample row = TMEM lane
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
-    uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0, ws_cnt = 0;
-    const bool need_ws = !BATCH && nphase1 > 1;
+    uint32_t a_use[2] = {0, 0}, ja = 0, s_cnt = 0;
     uint32_t blk = 0;  // blocks run by this CTA (selects the staging buffer)
     for (int64_t it = P.tile0 + blockIdx.x; it < P.n_tiles; it += gridDim.x) {
       const UmmaProb *pb = BATCH ? P.probs + P.item_prob[it] : nullptr;
@@ -469,7 +528,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       const int64_t tpsI = BATCH ? pb->tiles_per_shift : P.tiles_per_shift;
       const TargetParams32 *tgtI = BATCH ? pb->tgt : P.tgt;
       double *partsI = BATCH ? pb->partials : P.partials;
-      const int64_t nphase = BATCH ? 1 : nphase1;
+      const int64_t nblk = (nYI + BK - 1) / BK;
       const int64_t k_shift = tile / tpsI;
       const int64_t jt = tile - k_shift * tpsI;
       const int64_t j = jt * TS + r;
@@ -480,17 +539,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
       // this row's terms of the staged Sobol integers of the tile
       const dbgz::SobolLane sob_lane(r, (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)));
-      for (int64_t ph = 0; ph < nphase; ++ph) {
-        const Phase f = phase_of(P.P, nYI, ph);
-        if (ph > 0) {
-          for (int64_t kc = 0; kc < f.L / BK; ++kc) {
-            ++a_use[ja & 1];
-            ++ja;
-          }
-        }
-        for (int b = 0; b < f.nb; ++b) {
+      {
+        for (int64_t X = 0; X < nblk; ++X) {
           const int ia = ja & 1;
-          const int64_t lbase = f.L + BK * b;
+          const int64_t lbase = BK * X;
           const int nval = (int)((nYI - lbase) < BK ? (nYI - lbase) : BK);
           const int cur = (int)(blk & 1);
           // the block's U triangle and per-dimension constants, staged by the
@@ -500,7 +552,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           const pol::Staged<float> &sgc = ms->sg[cur];
           // partial sums of the block's targets, accumulated by the tensor cores
           float s[BK];
-          if (ph == 0 && b == 0) {
+          if (X == 0) {
 #pragma unroll
             for (int t = 0; t < BK; ++t) s[t] = 0.f;
           } else {
@@ -508,18 +560,19 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
             ++s_cnt;
             tc_fence_after();
             uint32_t v[BK];
-            tmem_ld_32x32b_x32(tmem + lane_base + (uint32_t)(BK * b), v);
+            tmem_ld_32x32b_x32(tmem + lane_base + tcol(X), v);
             tmem_wait_ld();
 #pragma unroll
             for (int t = 0; t < BK; ++t) s[t] = __uint_as_float(v[t]);
           }
           // the A tile must be free: its previous MMA done, its previous store read
-          if (a_use[ia] > 0) ok = mbar_wait(&ms->a_free[ia], (a_use[ia] - 1) & 1, abort) && ok;
-          if (r == 0) bulk_wait_read_all();
+          if (a_use[ia] > 0)
+            ok = mbar_wait(&ms->a_free[ia], (a_use[ia] - 1) & 1, abort) &&
+                 mbar_wait(&ms->a_stored[ia], (a_use[ia] - 1) & 1, abort) && ok;
           if (!ok) set_abort(ms, P.status);
-          named_sync(kBarScalar, TS);
-          if (*abort) goto done;
-          {
+          // a warp that gives up still meets the others at the block's end,
+          // where the decision to leave is taken together
+          if (!*abort) {
             // 4 chunks of 8 sequential steps.  s[] is kept in a frame that
             // rotates by 8 per chunk, so that every register index is static:
             // in chunk ch, s[t] is the partial sum of target lbase + 8 ch + t + 1.
@@ -597,20 +650,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           }
           fence_proxy_async_smem();
           tc_fence_before();
-          named_sync(kBarScalar, TS);
+          if (bar_red_or(kBarScalar, TS, *abort != 0)) goto done;
           if (r == 0) {
             mbar_arrive(&ms->a_full[ia]);
             mbar_arrive(&ms->stg_free[cur]);
-            if (need_ws && ph < nphase - 1) {
-              for (int pp = 0; pp < F::NPART; ++pp)
-                tma_store_2d(&P.tm_y[pp], (int32_t)lbase, slot_row, abuf + ia * SM::ABYTES + pp * SM::APART);
-              bulk_commit();
-              if (b == f.nb - 1) {
-                bulk_wait_all();
-                mbar_arrive(&ms->ws_ready);
-                ++ws_cnt;
-              }
-            }
           }
           ++a_use[ia];
           ++ja;
@@ -627,10 +670,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         if (r == 0) partsI[tile] = ((ms->red[0] + ms->red[1]) + ms->red[2]) + ms->red[3];
       }
     }
-  done:
-    pol::cp_async_wait_all();
-    if (r == 0) bulk_wait_all();
-    (void)ws_cnt;
+  done:;
   }
   tc_fence_before();
   __syncthreads();
@@ -759,7 +799,6 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
             smem_per_sm, fa.numRegs, NT, regs_per_sm);
   if (per_sm < 1) return dbgz_fail(ctx, DBGZ_ERR_CUDA, "tensor-core loop does not fit on an SM");
   const int64_t grid = std::min<int64_t>(n_tiles - pa.tile0, (int64_t)per_sm * ctx->num_sms);
-  const int64_t nphase = (nY + Pw - 1) / Pw;
   UmmaParams P{};
   P.d = d;
   P.nY = nY;
@@ -804,7 +843,6 @@ int launch_umma(dbgz_problem *p, const PassArgs &pa, double *partials, int64_t n
   if (F::NPART > 1) DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_u[1], u1.p, (uint64_t)Dp, (uint64_t)d, 64));
   // Y workspace: one 128-row slot per CTA, parts side by side
   const size_t part_bytes = (size_t)grid * TS * Dp * F::ESZ;
-  (void)nphase;
   DBGZ_TRY(dbgz_ensure(ctx, p->yws, part_bytes * F::NPART));
   for (int pp = 0; pp < F::NPART; ++pp)
     DBGZ_TRY(encode_2d<MODE>(ctx, &P.tm_y[pp], (char *)p->yws.p + pp * part_bytes, (uint64_t)Dp,
