@@ -42,14 +42,14 @@ METRIC = "d=1000 MVN P time at |err|<=1e-5 vs FP64: mixed-prec vs FP64 GPU; grad
 UNIT = "ms"
 MIXED = "fp32_split_bf16"   # mixed-precision mode of the headline number
 # DRAM bytes of one 2^21-sample launch of the split-BF16 loop at d=1000 (ncu capture of a
-# 131,072-sample launch: 0.249 GB read + 0.348 GB written, scaled by the sample count)
-TRAFFIC_PER_LAUNCH = 16 * (248.69e6 + 347.87e6)
+# 131,072-sample launch: 0.239 GB read + 0.328 GB written, scaled by the sample count)
+TRAFFIC_PER_LAUNCH = 16 * (239.36e6 + 328.14e6)
 # warp instructions of one split-BF16 loop launch at d = 1000 per sample (ncu
-# smsp__inst_executed.sum of a 131,072-sample launch: 7.412e8), and its
+# smsp__inst_executed.sum of a 131,072-sample launch: 6.788e8), and its
 # XU (special-function) pipe share; the issue roofline below scales it to the
 # timed launch
-INST_PER_SAMPLE = 7.412e8 / 131072
-XU_PIPE_PCT = 12.3
+INST_PER_SAMPLE = 6.788e8 / 131072
+XU_PIPE_PCT = 15.4
 ISSUE_PROFILE = "profiles/genz_umma_splitbf16_d1000_8192pts_full.md"
 
 
