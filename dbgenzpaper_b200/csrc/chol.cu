@@ -90,6 +90,17 @@ k_genz_block_smem(double *M, int64_t n, double *a, double *b, double *dvec, doub
   cholk::genz_block_smem(M, n, a, b, dvec, svec, perm, i0, i1, ii1, eps0_ptr, rank, genz_sh);
 }
 
+// The same with the block's factor entries on chip (panels of up to
+// cholk::kOnchipSlots candidates, blocks of up to cholk::kOnchipPiv pivots):
+// the slot warps and the y_i warp.
+constexpr int kOnchipThreads = cholk::kOnchipSlots + 32;
+__global__ void __launch_bounds__(kOnchipThreads)
+k_genz_block_onchip(double *M, int64_t n, double *a, double *b, double *dvec, double *svec, int64_t *perm,
+                    int64_t i0, int64_t i1, int64_t ii1, const double *eps0_ptr, int64_t *rank) {
+  extern __shared__ double genz_sh[];
+  cholk::genz_block_onchip(M, n, a, b, dvec, svec, perm, i0, i1, ii1, eps0_ptr, rank, genz_sh);
+}
+
 // One bs1 block of cholesky_rowmax! (src/cholesky.jl:290-357), one CTA: the
 // pivot is the largest remaining diagonal of the panel (first on ties, NaN
 // never chosen unless it is the current row's own), the rank test m_ii > 0
@@ -429,7 +440,16 @@ int dbgz_chol_genz_dev(dbgz_ctx *ctx, int64_t n, double *M, double *a, double *b
         for (int64_t i0 = ii0; i0 <= ii1 && rc == DBGZ_OK; i0 += bs1) {
           int64_t i1 = std::min(ii1, i0 + bs1 - 1);
           const int64_t panel = ii1 - i0 + 1;
-          if (panel <= kGenzSmemPanel) {
+          if (panel <= cholk::kOnchipSlots && i1 - i0 + 1 <= cholk::kOnchipPiv) {
+            static bool attr_oc[64] = {};
+            if (ctx->device < 0 || ctx->device >= 64 || !attr_oc[ctx->device]) {
+              cudaFuncSetAttribute(k_genz_block_onchip, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)cholk::genz_block_onchip_bytes(cholk::kOnchipSlots));
+              if (ctx->device >= 0 && ctx->device < 64) attr_oc[ctx->device] = true;
+            }
+            k_genz_block_onchip<<<1, kOnchipThreads, cholk::genz_block_onchip_bytes(panel), st>>>(
+                M, n, a, b, dvec, svec, perm, i0, i1, ii1, eps0, rank);
+          } else if (panel <= kGenzSmemPanel) {
             const size_t sm = cholk::genz_block_smem_bytes(panel);
             static bool attr[64] = {};
             if (ctx->device < 0 || ctx->device >= 64 || !attr[ctx->device]) {

@@ -361,6 +361,298 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
   write_back();
 }
 
+// genz_block_smem with the block's factor entries kept on chip.  The entries
+// m[l, k] of the block's pivots l for every candidate k of the panel, which
+// the row update's dot products read, live in the registers of the
+// candidate's thread (the first kFReg pivots) and in shared memory (the rest),
+// and follow their candidate through the swaps.  Thread t < kOnchipSlots owns
+// panel position i0 + t; it takes the value M[i, k] its update needs while it
+// does its part of the row/column swap, so the pivot chain makes no global
+// read but that one.  A last warp computes y_i (:533-546) while the slot
+// threads run the update's dot products (named barrier 2: y_i ready).  Panels
+// of at most kOnchipSlots positions, blocks of at most kOnchipPiv pivots.  Same
+// operations in the same order as genz_block_dev: the same bits.
+constexpr int kFReg = 16;          // block pivots whose entries live in registers
+constexpr int kOnchipPiv = 64;     // pivots per block at most
+constexpr int kOnchipSlots = 512;  // slot threads; the block has one more warp
+__host__ __device__ inline size_t genz_block_onchip_bytes(int64_t panel_len) {
+  return (size_t)(56 + 8 * (kOnchipPiv - kFReg)) * (size_t)panel_len + 8 * 2 * kFReg;
+}
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ void named_bar_arrive(int id, int nthreads) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ void genz_block_onchip(double *M, int64_t n, double *a, double *b, double *dvec,
+                                                  double *svec, int64_t *perm, int64_t i0, int64_t i1,
+                                                  int64_t ii1, const double *eps0_ptr, int64_t *rank, double *sh) {
+  __shared__ double red_v[32];
+  __shared__ int64_t red_i[32];
+  __shared__ int64_t sh_im;
+  __shared__ double sh_mraw, sh_dii, sh_yi, sh_mij_im;
+  const double c2 = dm_div(1.0, dm_sqrt(2.0));
+  const double is2pi = dm_div(2.0, dm_sqrt(dm_mul(2.0, M_PI)));
+  const double eps0 = eps0_ptr[0];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  constexpr int NS = kOnchipSlots, NALL = kOnchipSlots + 32;
+  if (rank[0] < n) return;  // an earlier block already stopped
+  const int64_t len = ii1 - i0 + 1;
+  double *s_d = sh, *s_s = sh + len, *s_a = sh + 2 * len, *s_b = sh + 3 * len, *s_g = sh + 4 * len,
+         *s_o = sh + 5 * len;
+  int64_t *s_p = reinterpret_cast<int64_t *>(sh + 6 * len);
+  double *s_f = sh + 7 * len;                        // [kOnchipPiv - kFReg][len]: pivots kFReg.. of each position
+  double *s_piv = s_f + (kOnchipPiv - kFReg) * len;  // the pivot's register entries
+  double *s_x = s_piv + kFReg;                       // the displaced candidate's register entries
+  for (int64_t k = tid; k < len; k += blockDim.x) {
+    const int64_t g = i0 + k;
+    s_d[k] = 0.0;
+    s_s[k] = svec[g];
+    s_a[k] = a[g];
+    s_b[k] = b[g];
+    s_g[k] = M[g * n + g];
+    s_p[k] = perm[g];
+  }
+  __syncthreads();
+  auto write_back = [&]() {
+    __syncthreads();
+    for (int64_t k = tid; k < len; k += blockDim.x) {
+      const int64_t g = i0 + k;
+      dvec[g] = s_d[k];
+      svec[g] = s_s[k];
+      a[g] = s_a[k];
+      b[g] = s_b[k];
+      perm[g] = s_p[k];
+    }
+  };
+  const bool yw = wid == NS / 32;  // the y_i warp
+  const int t = tid;               // this thread's panel position: kk = i0 + t
+  const bool has_slot = !yw && t < len;
+  const int64_t kk = i0 + t;
+  double f[kFReg];                 // m[i0 + u, kk] for u < kFReg
+#pragma unroll
+  for (int u = 0; u < kFReg; ++u) f[u] = 0.0;
+  double mij = 0.0;                // M[i, kk] of the coming update
+  // pivot score of this position for step i (:500-512), and the warp's minimum
+  auto score = [&](int64_t i) {
+    double bv = 0.0;
+    int64_t bi = INT64_MAX;
+    if (has_slot && kk >= i) {
+      double m_kk = dm_sub(s_g[t], s_d[t]);
+      m_kk = m_kk < 0 ? 0.0 : dm_sqrt(m_kk);
+      double a_k = dm_mul(dm_div(dm_sub(s_a[t], s_s[t]), m_kk), c2);
+      double b_k = dm_mul(dm_div(dm_sub(s_b[t], s_s[t]), m_kk), c2);
+      double o = dm_sub(det_erf(b_k), det_erf(a_k));
+      s_o[t] = o;
+      bv = o;
+      bi = kk;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
+      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
+      if (lane + off < 32 && i2 != INT64_MAX) {
+        if (bi == INT64_MAX) { bv = v2; bi = i2; }
+        else argmin_combine(bv, bi, v2, i2);
+      }
+    }
+    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+  };
+  for (int64_t i = i0; i <= i1; ++i) {
+    const int np = (int)(i - i0);  // block pivots before i
+    // one call site of the scores (their special functions are long code)
+    if (!yw) score(i);
+    __syncthreads();
+    if (wid == 0) {
+      // the warps' minima reduced by warp 0 (strict total order: the minimum
+      // does not depend on the order of combination)
+      constexpr int nw = NS / 32;
+      double v = lane < nw ? red_v[lane] : 0.0;
+      int64_t im = lane < nw ? red_i[lane] : INT64_MAX;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double v2 = __shfl_down_sync(0xffffffffu, v, off);
+        const int64_t i2 = __shfl_down_sync(0xffffffffu, im, off);
+        if (lane + off < 32 && i2 != INT64_MAX) {
+          if (im == INT64_MAX) { v = v2; im = i2; }
+          else argmin_combine(v, im, v2, i2);
+        }
+      }
+      im = __shfl_sync(0xffffffffu, im, 0);
+      const int64_t qi = np, qm = im - i0;
+      if (lane == 0) {
+        sh_im = im;
+        sh_dii = s_o[qm];
+        sh_mraw = dm_sub(s_g[qm], s_d[qm]);
+      }
+      __syncwarp();
+      if (im != i && lane < 6) {  // :518-523 (and the diagonal, which the row/column swap moves)
+        if (lane == 0) {
+          const int64_t tp = s_p[qi]; s_p[qi] = s_p[qm]; s_p[qm] = tp;
+        } else {
+          double *arr = lane == 1 ? s_d : lane == 2 ? s_s : lane == 3 ? s_a : lane == 4 ? s_b : s_g;
+          const double tt = arr[qm]; arr[qm] = arr[qi]; arr[qi] = tt;
+        }
+      }
+    }
+    __syncthreads();
+    const int64_t im = sh_im;
+    const int qm = (int)(im - i0);
+    const double m_raw = sh_mraw;
+    const bool stop = !(m_raw > eps0);  // the rank test of :533-537
+    const double m_pp = stop ? 0.0 : dm_sqrt(m_raw);
+    if (yw) {
+      // y_i (:538-546) while the slot threads swap and update
+      if (lane == 0) {
+        if (stop) {
+          rank[0] = i;  // 0-based i == reference's i - 1
+        } else {
+          double a_norm = dm_div(dm_sub(s_a[np], s_s[np]), m_pp);
+          double b_norm = dm_div(dm_sub(s_b[np], s_s[np]), m_pp);
+          double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
+          double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
+          sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), sh_dii);
+        }
+      }
+      __syncwarp();
+      if (stop) {
+        write_back();
+        return;
+      }
+      named_bar_arrive(2, NALL);
+    } else {
+      // the pivot's register entries for every candidate's dot product, the
+      // displaced candidate's for its new position
+      if (t == qm) {
+#pragma unroll
+        for (int u = 0; u < kFReg; ++u) s_piv[u] = f[u];
+      }
+      if (im != i && t == np) {
+#pragma unroll
+        for (int u = 0; u < kFReg; ++u) s_x[u] = f[u];
+      }
+      if (im != i) {
+        // the shared-memory entries of the two positions trade places
+        for (int u = kFReg + t; u < np; u += NS) {
+          double *row = s_f + (int64_t)(u - kFReg) * len;
+          const double tt = row[np];
+          row[np] = row[qm];
+          row[qm] = tt;
+        }
+        // :525-530, rows i <-> im over columns i0..n-1, then columns i <-> im,
+        // in one pass: for k outside {i, im} the two swaps touch four distinct
+        // elements; the 2 x 2 block on {i, im} ends up as (i,i) <- (im,im),
+        // (im,im) <- (i,i), (i,im) <- (im,i), (im,i) <- (i,im), and (i,i)
+        // then takes the pivot m_ii.  Position k's thread does index k
+        // (k >= i0), so it keeps the value its update reads: M[k, i] after the
+        // swap, or M[i, k] for the block's first pivot.  Two indices at a time:
+        // both loaded before either is stored.
+        auto swap_pair = [&](int64_t k0, int64_t k1) {
+          const bool live0 = k0 >= 0 && k0 != i && k0 != im, live1 = k1 >= 0 && k1 != i && k1 != im;
+          const bool row0 = live0 && k0 >= i0, row1 = live1 && k1 >= i0;
+          const double ri0 = row0 ? M[k0 * n + i] : 0.0, rm0 = row0 ? M[k0 * n + im] : 0.0;
+          const double ci0 = live0 ? M[i * n + k0] : 0.0, cm0 = live0 ? M[im * n + k0] : 0.0;
+          const double ri1 = row1 ? M[k1 * n + i] : 0.0, rm1 = row1 ? M[k1 * n + im] : 0.0;
+          const double ci1 = live1 ? M[i * n + k1] : 0.0, cm1 = live1 ? M[im * n + k1] : 0.0;
+          auto store = [&](int64_t k, bool live, bool row, double r_i, double r_m, double c_i, double c_m) {
+            if (row) {
+              M[k * n + i] = r_m;
+              M[k * n + im] = r_i;
+            }
+            if (live) {
+              M[i * n + k] = c_m;
+              M[im * n + k] = c_i;
+              if (k == kk) mij = np == 0 ? r_m : c_m;
+            }
+            if (k == i) {
+              const double ii = M[i * n + i], mm = M[im * n + im], im_i = M[i * n + im], i_im = M[im * n + i];
+              M[i * n + i] = stop ? mm : m_pp;
+              M[im * n + im] = ii;
+              M[im * n + i] = im_i;
+              M[i * n + im] = i_im;
+              sh_mij_im = np == 0 ? im_i : i_im;  // for position im
+            }
+          };
+          store(k0, live0, row0, ri0, rm0, ci0, cm0);
+          store(k1, live1, row1, ri1, rm1, ci1, cm1);
+        };
+        int64_t pend = -1;
+        auto push = [&](int64_t k) {
+          if (pend < 0) {
+            pend = k;
+          } else {
+            swap_pair(pend, k);
+            pend = -1;
+          }
+        };
+        for (int64_t k = i0 + t; k < n; k += NS) push(k);
+        for (int64_t k = t; k < i0; k += NS) push(k);
+        if (pend >= 0) swap_pair(pend, -1);
+      } else {
+        if (has_slot && kk > i) mij = np == 0 ? M[kk * n + i] : M[i * n + kk];
+        if (t == np && !stop) M[i * n + i] = m_pp;
+      }
+      named_bar_sync(1, NS);
+      if (im != i) {
+        if (t == np) {
+#pragma unroll
+          for (int u = 0; u < kFReg; ++u) f[u] = s_piv[u];
+        } else if (t == qm) {
+#pragma unroll
+          for (int u = 0; u < kFReg; ++u) f[u] = s_x[u];
+          mij = sh_mij_im;
+        }
+      }
+      if (stop) {
+        write_back();
+        return;
+      }
+      // the update of step i (:547-570) for this position
+      const bool upd = has_slot && kk > i;
+      double m = 0.0;
+      if (upd) {
+        if (np == 0) {
+          m = dm_div(mij, m_pp);
+        } else {
+          // the ascending fma chain over the block's pivots l = i0 .. i - 1
+          double acc = 0.0;
+#pragma unroll
+          for (int u = 0; u < kFReg; ++u)
+            if (u < np) acc = dm_fma(f[u], s_piv[u], acc);
+          int u = kFReg;
+          for (; u + 8 <= np; u += 8) {
+            double x[8], y[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const double *row = s_f + (int64_t)(u + e - kFReg) * len;
+              x[e] = row[t];
+              y[e] = row[np];
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e) acc = dm_fma(x[e], y[e], acc);
+          }
+          for (; u < np; ++u) {
+            const double *row = s_f + (int64_t)(u - kFReg) * len;
+            acc = dm_fma(row[t], row[np], acc);
+          }
+          m = dm_div(dm_sub(mij, acc), m_pp);
+        }
+        s_d[t] = dm_add(s_d[t], dm_mul(m, m));
+        if (np < kFReg) {
+#pragma unroll
+          for (int u2 = 0; u2 < kFReg; ++u2) f[u2] = u2 == np ? m : f[u2];
+        } else {
+          s_f[(int64_t)(np - kFReg) * len + t] = m;
+        }
+        M[kk * n + i] = m;
+        M[i * n + kk] = m;
+      }
+      named_bar_sync(2, NALL);  // y_i
+      if (upd) s_s[t] = dm_add(s_s[t], dm_mul(sh_yi, m));
+    }
+  }
+  write_back();
+}
+
 // C[j,k] -= sum_{l=p0..p1} A(l,j) * B(l,k) for j,k in [c0, c1], one
 // ascending fma chain per element.  A(l,j) = M[j,l] (row form, the
 // reference's lower-triangle copy) when a_row, else M[l,j]; B(l,k) = M[l,k].

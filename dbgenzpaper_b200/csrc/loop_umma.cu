@@ -212,6 +212,14 @@ __device__ __forceinline__ void rank8_update(float (&s)[BK], const float (&ys)[8
   }
 }
 
+// Policies that can run a chunk without per-step votes and redo it (Adjoint).
+template <typename P, typename = void>
+struct chunk_redo : std::false_type {};
+template <typename P>
+struct chunk_redo<P, std::void_t<decltype(P::kChunkRedo)>> : std::bool_constant<P::kChunkRedo> {};
+template <typename P>
+constexpr bool chunk_redo_v = chunk_redo<P>::value;
+
 // Policy: pol::Forward<float, GEN, STORE> or pol::Adjoint<float, GEN>.
 // BATCH: work items are (problem, tile) pairs of a batched launch, each
 // problem single-phase; every role walks the same static item sequence.
@@ -588,7 +596,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
               pl.chunk_begin(lbase + 8 * ch, nval - 8 * ch);
               // full chunks (all but the last of a problem) run without the
               // per-step bounds test: one uniform branch per chunk instead of 8
-              auto steps = [&](auto checked) {
+              auto steps = [&](auto checked, auto fast) {
 #pragma unroll
               for (int k = 0; k < 8; ++k) {
                 const int li = 8 * ch + k;
@@ -598,7 +606,10 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                   uint32_t xs = 0u;
                   if constexpr (Policy::kSobolTable)
                     if (pl.gen.sobol_staged) xs = sob_lane.at(ms->sob[cur], li);
-                  y = pl.emit_k(sgc, li, l, k, xs);
+                  if constexpr (decltype(fast)::value)
+                    y = pl.emit_k_fast(sgc, li, l, k, xs);
+                  else
+                    y = pl.emit_k(sgc, li, l, k, xs);
                   const float4 *urow = reinterpret_cast<const float4 *>(&ublk[li][8 * ch]);
                   const float4 u0 = urow[0], u1 = urow[1];
                   const float uu[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
@@ -612,8 +623,29 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 ys[k] = y;
               }
               };
-              if (nval - 8 * ch >= 8) steps(std::false_type{});
-              else steps(std::true_type{});
+              auto run = [&](auto fast) {
+                if (nval - 8 * ch >= 8) steps(std::false_type{}, fast);
+                else steps(std::true_type{}, fast);
+              };
+              if constexpr (chunk_redo_v<Policy>) {
+                // the chunk without per-step votes; redone with them from its
+                // saved state when a lane's FP32 terms left FP32 range
+                float s_save[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t) s_save[t] = s[t];
+                const double yb_save = pl.ybar;
+                pl.bad = false;
+                run(std::true_type{});
+                if (__any_sync(0xffffffffu, pl.bad)) {
+#pragma unroll
+                  for (int t = 0; t < 8; ++t) s[t] = s_save[t];
+                  pl.ybar = yb_save;
+                  pl.fp64_done = 0u;
+                  run(std::false_type{});
+                }
+              } else {
+                run(std::false_type{});
+              }
               pl.chunk_end(lbase + 8 * ch, nval - 8 * ch);
               if constexpr (Policy::kDeferTail) pl.tail_repair(sgc, s, 8 * ch, lbase + 8 * ch);
               switch (ch) {

@@ -204,6 +204,9 @@ struct Forward {
   __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int, uint32_t xs) {
     return emit(sg, li, l, xs);
   }
+  __device__ __forceinline__ T emit_k_fast(const Staged<T> &sg, int li, int64_t l, int k, uint32_t xs) {
+    return emit_k(sg, li, l, k, xs);
+  }
   __device__ __forceinline__ void consume(const Staged<T> &sg, T s, int li, int64_t l) {
     const auto tg = sg.tg[li];
     st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
@@ -274,6 +277,10 @@ template <typename T, int GEN>
 struct Adjoint {
   static constexpr bool kPlain = false;
   static constexpr bool kDeferTail = false;
+  // the loop may run a chunk with emit_k_fast (no per-step vote) and redo it
+  // with emit_k when some lane's FP32 terms left FP32 range (bad)
+  static constexpr bool kChunkRedo = sizeof(T) == 4;
+  bool bad;
   // takes staged Sobol integers (GenParams::sobol_staged) where the loop
   // stages them; the QMC dimension of step li of a block: d - 1 - lbase - li
   static constexpr bool kSobolTable = GEN == DBGZ_QMC_SOBOL;
@@ -551,6 +558,25 @@ struct Adjoint {
         asm volatile("prefetch.global.L2 [%0];" ::"l"(io.dc + io.at(t, g)));
       }
     }
+  }
+  // emit_k without the per-step warp vote (FP32 paths): the FP32 terms in
+  // any case, `bad` set where they are not finite; the loop then redoes the
+  // chunk with emit_k from the chunk's saved state, which gives exactly what
+  // emit_k alone would have given
+  __device__ __forceinline__ T emit_k_fast(const Staged<T> &sg, int li, int64_t l, int kk, uint32_t xs) {
+    const int64_t t = d - 1 - l;
+    const bool has_u = t <= d - 2;
+    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_staged != 0) : 0.0;
+    float fa, fb, fu;
+    const float sb = variable32(sg.tg[li], (float)w, has_u, (float)pre_y[kk], (float)pre_s[kk],
+                                (float)pre_dc[kk], true, fa, fb, fu);
+    const float wa = wrel * fa, wb = wrel * fb, wu = wrel * fu;
+    bad = bad || !(isfinite(sb) && isfinite(wa) && isfinite(wb) && isfinite(wu));
+    acc_a[kk] = wa;
+    acc_b[kk] = wb;
+    acc_u[kk] = wu;
+    store_gemm(t, has_u, pre_y[kk], p * (double)sb);
+    return (T)sb;
   }
   __device__ __forceinline__ T emit_k(const Staged<T> &sg, int li, int64_t l, int kk, uint32_t xs) {
     if (sizeof(T) != 4) return emit_from(sg, li, l, pre_y[kk], pre_s[kk], pre_dc[kk], xs);
