@@ -313,11 +313,6 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
       }
       pp.stage_async(ms->sg[buf], tgtI, lane, slb, nv);
       cp_async_mbar_arrive(&ms->stg_full[buf]);
-      if constexpr (Policy::kSobolTable)
-        if (pp.gen.sobol_staged)
-          dbgz::sobol_stage_entries<1>(ms->sob[buf], pp.gen.V, pp.gen.ushift + pp.k * (dI - 1),
-                                       (uint64_t)(pp.gen.sobol_first + pp.gen.gen_base + (pp.j - lane)),
-                                       pp.sobol_l0(slb), Policy::kSobolDir, dI - 2, nv, 0, BK);
       mbar_arrive(&ms->stg_full[buf]);
       ++st_use[buf];
       ++st_n;
@@ -547,6 +542,22 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
         pl.tile_begin(P.gen, P.d, tile, P.tiles_per_shift, r, P.c1, P.dc1, P.up1, 0, P.io);
       // this row's terms of the staged Sobol integers of the tile
       const dbgz::SobolLane sob_lane(r, (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)));
+      // the Sobol integers of a block's dimensions, staged by the sample
+      // threads themselves (warp-wide shuffles, 8 dimensions per warp) into
+      // buffer `buf`; visible to all of them after the next block barrier
+      const bool sob_staged = Policy::kSobolTable && pl.gen.sobol_staged;
+      auto stage_sobol = [&](int buf, int64_t lb) {
+        if constexpr (Policy::kSobolTable) {
+          const int nv = (int)(nYI - lb < BK ? nYI - lb : BK);
+          dbgz::sobol_stage_block(ms->sob[buf], pl.gen.V, pl.gen.ushift + pl.k * (dI - 1),
+                                  (uint64_t)(pl.gen.sobol_first + pl.gen.gen_base + (pl.j - r)), pl.sobol_l0(lb),
+                                  Policy::kSobolDir, dI - 2, nv, r);
+        }
+      };
+      if (sob_staged) {
+        stage_sobol((int)(blk & 1), 0);  // the tile's first block, now
+        named_sync(kBarScalar, TS);
+      }
       {
         for (int64_t X = 0; X < nblk; ++X) {
           const int ia = ja & 1;
@@ -556,6 +567,9 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
           // the block's U triangle and per-dimension constants, staged by the
           // producer warp during the previous block
           bool ok = mbar_wait(&ms->stg_full[cur], (blk >> 1) & 1, abort);
+          // the next block's Sobol integers while the tensor cores finish this
+          // block's partial sums
+          if (sob_staged && X + 1 < nblk) stage_sobol(cur ^ 1, lbase + BK);
           float(*ublk)[kUld] = ms->ublk[cur];
           const pol::Staged<float> &sgc = ms->sg[cur];
           // partial sums of the block's targets, accumulated by the tensor cores
