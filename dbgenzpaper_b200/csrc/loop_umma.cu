@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ Umm
                 float s_save[8];
 #pragma unroll
                 for (int t = 0; t < 8; ++t) s_save[t] = s[t];
-                const double yb_save = pl.ybar;
+                const auto yb_save = pl.ybar;
                 pl.bad = false;
                 run(std::true_type{});
                 if (__any_sync(0xffffffffu, pl.bad)) {

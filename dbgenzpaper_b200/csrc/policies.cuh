@@ -289,7 +289,10 @@ struct Adjoint {
   dbgz::GenParams gen;
   int64_t j, k, g, d, tile;
   GradIO<T> io;
-  double ybar;  // saved receiver value: ybar of the variable the next step handles
+  // saved receiver value: ybar of the variable the next step handles, in the
+  // working type (it is a sum of the loop's working type; no round trip
+  // through FP64 on the FP32 chain)
+  T ybar;
   double p;     // this sample's weight (the seed scale)
   // FP32 paths: the warp's largest weight, and this sample's weight relative
   // to it (in [0, 1]); the per-variable sums over the warp's samples are then
@@ -311,7 +314,7 @@ struct Adjoint {
     j = (tile - k * tiles_per_shift) * 128 + r;
     g = (tile - io_.tile0) * 128 + r;
     io = io_;
-    ybar = 0.0;  // variable d-1 has no u: nothing downstream of it
+    ybar = T(0);  // variable d-1 has no u: nothing downstream of it
     p = io.p[g];
     warp = r >> 5;
     lane = r & 31;
@@ -397,10 +400,10 @@ struct Adjoint {
     if (sizeof(T) == 4) {
       if (dc > T(1e-30)) pex = (double)__fdividef(1.0f, (float)dc);
       else if (dc > T(0)) pex = 1.0 / (double)dc;
-      if (has_u && fabs(y) < T(8.12585)) ubar = ybar * (double)__fdividef(1.0f, (float)(rpi * exp(T(-0.5) * y * y)));
+      if (has_u && fabs(y) < T(8.12585)) ubar = (double)ybar * (double)__fdividef(1.0f, (float)(rpi * exp(T(-0.5) * y * y)));
     } else {
       pex = dc > T(0) ? 1.0 / (double)dc : 0.0;
-      if (has_u && fabs(y) < T(8.12585)) ubar = ybar / (double)(rpi * exp(T(-0.5) * y * y));
+      if (has_u && fabs(y) < T(8.12585)) ubar = (double)ybar / (double)(rpi * exp(T(-0.5) * y * y));
     }
     const double eb = pex + ubar * w, cb = -pex + ubar * (1.0 - w);
     const double rU = (double)inv_u * 1.4142135623730951;  // 1 / U_tt
@@ -639,13 +642,13 @@ struct Adjoint {
       io.gu[row] = (double)su * wmax;
     }
   }
-  __device__ __forceinline__ void consume(const Staged<T> &, T r_sum, int, int64_t) { ybar = (double)r_sum; }
+  __device__ __forceinline__ void consume(const Staged<T> &, T r_sum, int, int64_t) { ybar = r_sum; }
   // the recursion's state between two steps (segments of the banded gradient)
   __device__ __forceinline__ void pack(double (&v)[4]) const {
-    v[0] = ybar;
+    v[0] = (double)ybar;
     v[1] = v[2] = v[3] = 0.0;
   }
-  __device__ __forceinline__ void unpack(const double (&v)[4]) { ybar = v[0]; }
+  __device__ __forceinline__ void unpack(const double (&v)[4]) { ybar = (T)v[0]; }
 
   __device__ __forceinline__ double tile_value(bool) { return 0.0; }
   // variable 0 after the last step: its CDF has no conditioning sum and no
