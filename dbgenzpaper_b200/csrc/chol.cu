@@ -223,17 +223,51 @@ k_schur_update(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t
 // row l finishes X[l] and broadcasts it, then every lane updates its rows
 // r > l.  U[l0:l0+31, pass rows] is staged in shared memory (coalesced
 // 256-byte row segments of the column-major M) and shared by the CTA's
-// kTrsmWarps columns.
+// kTrsmWarps columns; the chunks are double-buffered, the next one copied by
+// cp.async while the current one is used (U is read only: X's columns lie
+// beyond p1).
 constexpr int kTrsmWarps = 8, kTrsmSlots = 8, kTrsmPass = 32 * kTrsmSlots, kTrsmLc = 32;
 constexpr int kTrsmLd = kTrsmPass + 1;  // padded row of the staged chunk
+constexpr int kTrsmChunk = kTrsmLc * kTrsmLd;  // doubles per staged chunk
+__device__ __forceinline__ void trsm_cp8(double *dst, const double *src, bool valid) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
 __global__ void __launch_bounds__(32 * kTrsmWarps)
 k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, const int64_t *rank) {
   if (rank && rank[0] < n) return;  // after a rank failure: no update
-  extern __shared__ double Us[];  // [kTrsmLc][kTrsmLd]: Us[lc * kTrsmLd + rr] = U[l0 + lc, q0 + rr]
+  // two chunks [kTrsmLc][kTrsmLd]: Us[lc * kTrsmLd + rr] = U[l0 + lc, q0 + rr]
+  extern __shared__ double Us2[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t c = c0 + (int64_t)blockIdx.x * kTrsmWarps + warp;
   const bool active = c <= c1;
   double *X = M + (active ? c : c0) * n;
+  // the chunk sequence: passes q0, and in each the chunks l0 = p0, p0 + 32, ... <= q1
+  auto stage = [&](int buf, int64_t q0, int64_t l0) {
+    const int64_t q1 = q0 + kTrsmPass - 1 < p1 ? q0 + kTrsmPass - 1 : p1;
+    const int nrows = (int)(q1 - q0 + 1);
+    const int nl = (int)((q1 - l0 + 1) < kTrsmLc ? (q1 - l0 + 1) : kTrsmLc);
+    double *Us = Us2 + buf * kTrsmChunk;
+    for (int idx = threadIdx.x; idx < kTrsmPass * kTrsmLc; idx += blockDim.x) {
+      const int rr = idx / kTrsmLc, lc = idx % kTrsmLc;
+      const bool v = rr < nrows && lc < nl;
+      trsm_cp8(Us + lc * kTrsmLd + rr, v ? M + (q0 + rr) * n + l0 + lc : M, v);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  auto next_chunk = [&](int64_t &q0, int64_t &l0) -> bool {  // advance; false at the end
+    const int64_t q1 = q0 + kTrsmPass - 1 < p1 ? q0 + kTrsmPass - 1 : p1;
+    l0 += kTrsmLc;
+    if (l0 > q1) {
+      q0 += kTrsmPass;
+      l0 = p0;
+    }
+    return q0 <= p1;
+  };
+  int64_t sq = p0, sl = p0;  // the chunk being staged
+  bool more = true;
+  stage(0, sq, sl);
+  int buf = 0;
   for (int64_t q0 = p0; q0 <= p1; q0 += kTrsmPass) {
     const int64_t q1 = q0 + kTrsmPass - 1 < p1 ? q0 + kTrsmPass - 1 : p1;
     const int nrows = (int)(q1 - q0 + 1);
@@ -246,12 +280,19 @@ k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, 
     }
     for (int64_t l0 = p0; l0 <= q1; l0 += kTrsmLc) {
       const int nl = (int)((q1 - l0 + 1) < kTrsmLc ? (q1 - l0 + 1) : kTrsmLc);
+      // the next chunk into the other buffer (the buffer it overwrites was
+      // last read before the barrier that ended the previous chunk)
       __syncthreads();
-      for (int idx = threadIdx.x; idx < kTrsmPass * kTrsmLc; idx += blockDim.x) {
-        const int rr = idx / kTrsmLc, lc = idx % kTrsmLc;
-        Us[lc * kTrsmLd + rr] = (rr < nrows && lc < nl) ? M[(q0 + rr) * n + l0 + lc] : 0.0;
+      if (more) more = next_chunk(sq, sl);
+      if (more) {
+        stage(buf ^ 1, sq, sl);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
       }
       __syncthreads();
+      const double *Us = Us2 + buf * kTrsmChunk;
+      buf ^= 1;
       if (!active) continue;
       if (l0 < q0) {
         // rows of earlier passes: X[l] is final (written by this lane)
@@ -296,6 +337,7 @@ k_trsm_ut(double *M, int64_t n, int64_t p0, int64_t p1, int64_t c0, int64_t c1, 
     }
     __syncwarp();
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 // One bs1 block of cholesky_classic! (src/cholesky.jl:180-198), one CTA.
@@ -380,8 +422,8 @@ int launch_trsm(dbgz_ctx *ctx, double *M, int64_t n, int64_t p0, int64_t p1, int
                 int64_t c1, const int64_t *rank = nullptr) {
   if (c1 < c0) return DBGZ_OK;
   const int64_t nc = c1 - c0 + 1;
-  const size_t smem = sizeof(double) * kTrsmLc * kTrsmLd;
-  // 66 KB of dynamic shared memory needs the opt-in, once per device
+  const size_t smem = sizeof(double) * 2 * kTrsmChunk;
+  // 132 KB of dynamic shared memory needs the opt-in, once per device
   static bool attr_set[64] = {};
   if (ctx->device < 0 || ctx->device >= 64 || !attr_set[ctx->device]) {
     DBGZ_CUDA_TRY(ctx, cudaFuncSetAttribute(k_trsm_ut, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

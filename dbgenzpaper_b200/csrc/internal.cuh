@@ -200,7 +200,7 @@ int dbgz_loop_simt(dbgz_problem *p, const PassArgs &pa, int precision, double *p
                    int64_t n_tiles);
 int dbgz_loop_umma(dbgz_problem *p, const PassArgs &pa, int precision, double *partials,
                    int64_t n_tiles);
-// Forward tensor-core loop over many single-phase problems (d - 1 <= 256) in
+// Forward tensor-core loop over many problems of at most two halves (d - 1 <= 256) in
 // one launch (batch.cu).  Host tables cover all problems of the batch;
 // `probs` lists the ones to run here, largest first.  Device pointers: FP64
 // factors (dM + off2[k]), FP32 factors, FP32 targets, 3 first-dimension

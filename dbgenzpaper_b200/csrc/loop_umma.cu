@@ -8,22 +8,24 @@
 //
 // Decomposition.  One CTA owns a tile of 128 samples (128 consecutive points
 // of one shift) = the 128 TMEM lanes = the M of every MMA.  y-indices are
-// processed in phases of P (= TMEM columns, 256) and, inside a phase, blocks
-// of 32:
-//   * phase start (phase > 0): S[:, phase targets] = Y[:, 0:L] U[0:L, phase]
-//     -- a K = L GEMM whose A operand (this tile's earlier y's) streams back
-//     from a per-CTA workspace in HBM/L2 and B (U^T panel) from the
-//     converted factor, both by TMA, into TMEM columns 0..P-1;
-//   * block b: the 128 sample threads read their 32 partial sums of the
+// processed in blocks of 32; TMEM holds the partial sums of the next targets
+// as two halves of 128 columns (half h = the targets of blocks 4h..4h+3):
+//   * block X: the 128 sample threads read their 32 partial sums of the
 //     block's targets from TMEM (tcgen05.ld), run the 32 sequential steps
-//     with an in-register rank-1 update for the block's own triangle, and
-//     write their y's (split hi/lo BF16, or TF32) as the A tile of the next
-//     MMA in shared memory (and to the workspace by TMA store when later
-//     phases need them);
-//   * after block b: S[:, targets of blocks b+1..] += Y_b U[b rows, ...] on
-//     the tensor cores -- first the 32 columns the next block needs
-//     (committed to its own barrier so the sample threads can go on), then
-//     the rest of the phase, which overlaps with the next block's steps.
+//     with in-register updates for the block's own triangle, and write their
+//     y's (split hi/lo BF16, or TF32) as the A tile of the next MMA in shared
+//     memory (the producer stores it to a per-CTA workspace in HBM/L2 when a
+//     later half's re-initialisation reads it);
+//   * after block X: S[:, targets of blocks X+1 .. end of the next half] +=
+//     Y_X U[X rows, ...] on the tensor cores -- first the 32 columns the next
+//     block needs (committed to their own barrier so the sample threads can
+//     go on), then the rest, which overlaps with the next block's steps;
+//     after the last block of a half also the first (overwriting)
+//     contribution to the half after next, in the columns just freed;
+//   * re-initialisation of half g >= 2: the contributions of y-blocks
+//     0 .. 4g-6, a K = 32 GEMM chunk per y-block (A streamed back from the
+//     workspace, B the U^T rows of half g, both by TMA), issued a quarter
+//     per block during the blocks before half g is needed.
 // Warp roles: warps 0-3 sample threads, warp 4 TMEM owner + MMA issuer,
 // warp 5 TMA producer.  Every wait is bounded (sm100.cuh); a timeout sets
 // DBGZ_ERR_TIMEOUT in the status word and the CTA drains and leaves.
@@ -62,8 +64,8 @@ struct Fmt<DBGZ_PREC_FP32_TF32> {
 };
 
 // One problem of a batched launch (global memory): its U^T panel maps and
-// the per-problem fields the kernel otherwise takes from UmmaParams.  Single
-// phase only (d - 1 <= the phase width): no y workspace.
+// the per-problem fields the kernel otherwise takes from UmmaParams.  At most
+// two halves (d - 1 <= 256): no re-initialisation, no y workspace.
 struct __align__(64) UmmaProb {
   CUtensorMap tm_u[2];
   int64_t d, nY, m, tiles_per_shift;
@@ -222,7 +224,7 @@ constexpr bool chunk_redo_v = chunk_redo<P>::value;
 
 // Policy: pol::Forward<float, GEN, STORE> or pol::Adjoint<float, GEN>.
 // BATCH: work items are (problem, tile) pairs of a batched launch, each
-// problem single-phase; every role walks the same static item sequence.
+// problem at most two halves; every role walks the same static item sequence.
 template <int MODE, typename Policy, bool BATCH = false>
 __global__ void __launch_bounds__(NT, 2) k_genz_umma(const __grid_constant__ UmmaParams P) {
   using F = Fmt<MODE>;
@@ -942,7 +944,7 @@ int setup_umma_batch(dbgz_ctx *ctx, const UmmaBatchArgs &A, UmmaBatchPlan *B) {
   int64_t n_items = 0;
   for (int64_t i = 0; i < nsel; ++i) {
     const int64_t k = A.probs[i], d = A.dims[k];
-    if (d - 1 > Pw) return dbgz_fail(ctx, DBGZ_ERR_DIMENSION, "tensor batch: d = %lld needs more than one phase", (long long)d);
+    if (d - 1 > Pw) return dbgz_fail(ctx, DBGZ_ERR_DIMENSION, "tensor batch: d = %lld needs more than two halves", (long long)d);
     dims[i] = d;
     off2[i] = A.off2[k];
     ld[i] = ((d - 1 + 63) / 64) * 64;

@@ -574,7 +574,9 @@ struct Adjoint {
     const float sb = variable32(sg.tg[li], (float)w, has_u, (float)pre_y[kk], (float)pre_s[kk],
                                 (float)pre_dc[kk], true, fa, fb, fu);
     const float wa = wrel * fa, wb = wrel * fb, wu = wrel * fu;
-    bad = bad || !(isfinite(sb) && isfinite(wa) && isfinite(wb) && isfinite(wu));
+    // one test for the four: an infinite or NaN term makes the sum so (a
+    // finite sum that overflows only costs a redo)
+    bad = bad || !isfinite((sb + wa) + (wb + wu));
     acc_a[kk] = wa;
     acc_b[kk] = wb;
     acc_u[kk] = wu;
