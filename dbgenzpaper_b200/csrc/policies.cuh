@@ -379,6 +379,21 @@ struct Adjoint {
     return fabs(fma(u, 2.0, -1.0));
   }
 
+  // point_w in FP32 for the FP32 paths: the same floats as
+  // StepFp32::quantile forms them (Richtmyer: the FP64 fraction, then FP32),
+  // without a conversion back and forth through FP64
+  __device__ __forceinline__ float point_w32(const Staged<T> &sg, int li, int64_t t, uint32_t xs,
+                                             bool staged) const {
+    if (GEN == 0) {
+      double x = __dmul_rn((double)(gen.gen_base + j + 1), sg.qv[li]);
+      x = x - floor(x);
+      float uf = (float)sg.shv[li] + (float)x;
+      uf = uf > 1.0f ? uf - 1.0f : uf;
+      return fabsf(fmaf(uf, 2.0f, -1.0f));
+    }
+    return (float)point_w(sg, li, t, xs, staged);
+  }
+
   // adjoint of variable t given ybar_t; returns sbar_t (unit seed), records
   // the per-variable gradient terms (unit seed; accumulate scales by p).
   // The bound arguments and the normal densities are formed in T (FP32
@@ -569,10 +584,10 @@ struct Adjoint {
   __device__ __forceinline__ T emit_k_fast(const Staged<T> &sg, int li, int64_t l, int kk, uint32_t xs) {
     const int64_t t = d - 1 - l;
     const bool has_u = t <= d - 2;
-    const double w = has_u ? point_w(sg, li, t, xs, gen.sobol_staged != 0) : 0.0;
+    const float w = has_u ? point_w32(sg, li, t, xs, gen.sobol_staged != 0) : 0.0f;
     float fa, fb, fu;
-    const float sb = variable32(sg.tg[li], (float)w, has_u, (float)pre_y[kk], (float)pre_s[kk],
-                                (float)pre_dc[kk], true, fa, fb, fu);
+    const float sb = variable32(sg.tg[li], w, has_u, (float)pre_y[kk], (float)pre_s[kk], (float)pre_dc[kk], true, fa,
+                                fb, fu);
     const float wa = wrel * fa, wb = wrel * fb, wu = wrel * fu;
     // one test for the four: an infinite or NaN term makes the sum so (a
     // finite sum that overflows only costs a redo)
