@@ -698,7 +698,24 @@ def main():
             "over_fwd": statistics.mean(g_ms) / ms_mix, "steps": kg,
             "host_dP_dB_ms": statistics.mean(host_ms),
             "outputs": "P, dP/da, dP/db, dP/dSigma on the device; dP/dB = 2 G B on the host",
-            "model": "Sigma = B B' + diag(psi), B 1000x20, thresholds fixed in correlation units"}
+            "model": "Sigma = B B' + diag(psi), B 1000x20, thresholds fixed in correlation units",
+            "state_bytes": int(prof.grad_state_bytes), "sample_chunks": int(prof.grad_chunks)}
+    # the same gradient with the stored state capped at 1/8 of what one chunk
+    # holds: the samples run in at least 8 chunks of tiles (the memory bound
+    # of the dense path; no recomputation)
+    full_state = int(prof.grad_state_bytes) * max(1, int(prof.grad_chunks))
+    ctx.set_state_budget(max(1, full_state // 8))
+    try:
+        res_b, _, _ = grad_step(Qg, prec_mixed)
+        gb_ms = [grad_step(Qg, prec_mixed)[1] for _ in range(kg)]
+        b_state, b_chunks = int(prof.grad_state_bytes), int(prof.grad_chunks)
+    finally:
+        ctx.set_state_budget(48 << 30)
+    den = max(float(np.max(np.abs(res_g[5]))), 1e-300)
+    grad["state_budget_eighth"] = {
+        "ms_per_step": statistics.mean(gb_ms), "over_fwd": statistics.mean(gb_ms) / ms_mix,
+        "state_bytes": b_state, "sample_chunks": b_chunks, "full_state_bytes": full_state,
+        "max_rel_diff_dP_dSigma": float(np.max(np.abs(res_b[5] - res_g[5]))) / den}
     Qg.close()
     # accuracy where P is O(0.1): the same covariance with the reference's own
     # bound design (+-k sqrt(S_ii), P(independent) = 0.25), same points

@@ -47,8 +47,20 @@ __global__ void k_adj_prepare(const double *U, const double *Ubar, int64_t d, do
 __global__ void k_adj_rowsum(const double *S, const double *R, int64_t d, double *rs) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= d) return;
+  // the same ascending chain, its operands loaded 16 at a time ahead of it
   double acc = 0.0;
-  for (int64_t j = 0; j < d; ++j) acc = fma(S[j * d + i], R[j * d + i], acc);
+  int64_t j = 0;
+  for (; j + 16 <= d; j += 16) {
+    double x[16], y[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x[u] = S[(j + u) * d + i];
+      y[u] = R[(j + u) * d + i];
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) acc = fma(x[u], y[u], acc);
+  }
+  for (; j < d; ++j) acc = fma(S[j * d + i], R[j * d + i], acc);
   rs[i] = acc;
 }
 __global__ void k_adj_colsum(const double *S, const double *R, int64_t d, const double *rs, double *r) {
@@ -149,7 +161,7 @@ int dbgz_sigma_adjoint_dev(dbgz_problem *p, const double *dU, const double *da, 
       rc = dbgz_fail(ctx, DBGZ_ERR_CUDA, "sigma_adjoint: dense kernel launch failed (%s)", cudaGetErrorString(ce));
       break;
     }
-    k_adj_rowsum<<<(unsigned)((d + 127) / 128), 128, 0, st>>>(M, R, d, rs);
+    k_adj_rowsum<<<(unsigned)((d + 31) / 32), 32, 0, st>>>(M, R, d, rs);  // a warp per 32 rows: more SMs
     dbgz_count_launch(ctx);
     k_adj_colsum<<<(unsigned)((d + 7) / 8), 256, 0, st>>>(M, R, d, rs, r);
     dbgz_count_launch(ctx);

@@ -234,9 +234,9 @@ __global__ void k_trinv64(const double *U, int64_t d, double *X) {
 
 // The same back substitution with the next column of U loaded into
 // registers while the current one is applied, and one barrier per step:
-// every thread forms x_r = rhs_r / U_rr itself (the same operation on the
-// same operands), so the step's only exchange is the right-hand side in
-// shared memory.  Thread t owns rows t + 128 q, q < Q (d <= 128 Q).
+// every thread forms x_r itself (the same operation on the same operands),
+// so the step's only exchange is the right-hand side in shared memory.
+// Thread t owns rows t + 128 q, q < Q (d <= 128 Q).
 template <int Q>
 __global__ void __launch_bounds__(128) k_trinv64_pf(const double *U, int64_t d, double *X) {
   extern __shared__ double rhs[];
@@ -244,7 +244,10 @@ __global__ void __launch_bounds__(128) k_trinv64_pf(const double *U, int64_t d, 
   const int tid = threadIdx.x;
   for (int64_t i = tid; i < d; i += 128) rhs[i] = i == c ? 1.0 : 0.0;
   double ucur[Q], unext[Q];
-  double dcur = U[c * d + c], dnext = 1.0;
+  // x_r = rhs_r * (1 / U_rr): the reciprocal of the next step's diagonal is
+  // formed while the current step runs, so the chain of steps carries a
+  // multiplication, not a division (within an ulp of rhs_r / U_rr)
+  double dcur = 1.0 / U[c * d + c], dnext = 1.0;
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int64_t i = tid + 128 * q;
@@ -254,14 +257,14 @@ __global__ void __launch_bounds__(128) k_trinv64_pf(const double *U, int64_t d, 
   for (int64_t r = c; r >= 0; --r) {
     if (r > 0) {
       const double *un = U + (r - 1) * d;
-      dnext = un[r - 1];
+      dnext = 1.0 / un[r - 1];
 #pragma unroll
       for (int q = 0; q < Q; ++q) {
         const int64_t i = tid + 128 * q;
         unext[q] = i < r - 1 ? un[i] : 0.0;
       }
     }
-    const double xr = rhs[r] / dcur;
+    const double xr = rhs[r] * dcur;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
       const int64_t i = tid + 128 * q;
