@@ -12,20 +12,27 @@
 
 namespace cholk {
 
-__device__ __forceinline__ bool julia_min_less(double x, double y) {
-  // Base.isgreater order used by findmin/argmin: NaN lowest, -0.0 < +0.0.
-  if (x != x) return y == y;
-  if (y != y) return false;
-  if (x < y) return true;
-  if (x == y && x == 0.0) return signbit(x) && !signbit(y);
-  return false;
+// The order findmin/argmin use (Base.isgreater: NaN lowest, -0.0 below +0.0,
+// then by value) as an unsigned key: NaN -> 0, otherwise the IEEE bits made
+// monotone (negative values complemented, non-negative ones with the sign bit
+// set), so -0.0 sorts below +0.0 and equal values give equal keys.  The
+// largest key, +inf's, is below ~0, which marks "no candidate".
+__device__ __forceinline__ unsigned long long argmin_key(double x) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  if (x != x) return 0ull;
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
 
-__device__ __forceinline__ void argmin_combine(double &v, int64_t &i, double v2, int64_t i2) {
-  if (julia_min_less(v2, v) || (!julia_min_less(v, v2) && i2 < i)) {
-    v = v2;
-    i = i2;
-  }
+// The warp's least key and, among the lanes that hold it, the least index
+// (ties go to the first candidate, as findmin's do): three warp
+// min-reductions on 32-bit words, no compare-and-branch tree.  Lanes without a
+// candidate pass key ~0 and index ~0.
+__device__ __forceinline__ void warp_argmin(unsigned long long &key, unsigned &idx) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mh = __reduce_min_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_min_sync(0xffffffffu, hi == mh ? lo : 0xffffffffu);
+  idx = __reduce_min_sync(0xffffffffu, (hi == mh && lo == ml) ? idx : 0xffffffffu);
+  key = ((unsigned long long)mh << 32) | ml;
 }
 
 // One bs1 block [i0, i1] of cholesky_genz! inside the bs2 panel ending at
@@ -34,8 +41,8 @@ __device__ __forceinline__ void argmin_combine(double &v, int64_t &i, double v2,
 __device__ __forceinline__ void genz_block_dev(double *M, int64_t n, double *a, double *b, double *dvec,
                                                double *svec, double *ovec, int64_t *perm, int64_t i0,
                                                int64_t i1, int64_t ii1, const double *eps0_ptr, int64_t *rank) {
-  __shared__ double red_v[32];
-  __shared__ int64_t red_i[32];
+  __shared__ unsigned long long red_k[32];
+  __shared__ unsigned red_t[32];
   __shared__ int64_t sh_im;
   __shared__ double sh_mii, sh_yi;
   __shared__ int sh_stop;
@@ -48,8 +55,8 @@ __device__ __forceinline__ void genz_block_dev(double *M, int64_t n, double *a, 
   __syncthreads();
   for (int64_t i = i0; i <= i1; ++i) {
     // pivot scores :500-512, then argmin :514
-    double bv = 0.0;
-    int64_t bi = INT64_MAX;
+    unsigned long long key = ~0ull;  // this thread's least key, at its first position
+    unsigned pos = ~0u;
     for (int64_t k = i + tid; k <= ii1; k += blockDim.x) {
       double m_kk = dm_sub(M[k * n + k], dvec[k]);
       m_kk = m_kk < 0 ? 0.0 : dm_sqrt(m_kk);
@@ -57,27 +64,26 @@ __device__ __forceinline__ void genz_block_dev(double *M, int64_t n, double *a, 
       double b_k = dm_mul(dm_div(dm_sub(b[k], svec[k]), m_kk), c2);
       double o = dm_sub(det_erf(b_k), det_erf(a_k));
       ovec[k] = o;
-      if (bi == INT64_MAX) { bv = o; bi = k; }
-      else argmin_combine(bv, bi, o, k);
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
-      if (lane + off < 32 && i2 != INT64_MAX) {
-        if (bi == INT64_MAX) { bv = v2; bi = i2; }
-        else argmin_combine(bv, bi, v2, i2);
+      const unsigned long long ko = argmin_key(o);
+      if (ko < key) {
+        key = ko;
+        pos = (unsigned)(k - i0);
       }
     }
-    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+    warp_argmin(key, pos);
+    if (lane == 0) {
+      red_k[wid] = key;
+      red_t[wid] = pos;
+    }
     __syncthreads();
+    if (wid == 0) {
+      const int nw = (int)(blockDim.x >> 5);
+      key = lane < nw ? red_k[lane] : ~0ull;
+      pos = lane < nw ? red_t[lane] : ~0u;
+      warp_argmin(key, pos);
+    }
     if (tid == 0) {
-      double v = red_v[0];
-      int64_t im = red_i[0];
-      for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-        if (red_i[w] == INT64_MAX) continue;
-        if (im == INT64_MAX) { v = red_v[w]; im = red_i[w]; }
-        else argmin_combine(v, im, red_v[w], red_i[w]);
-      }
+      const int64_t im = i0 + (int64_t)pos;
       double d_ii = ovec[im];
       double m_ii = dm_sub(M[im * n + im], dvec[im]);
       if (im != i) {  // :518-523
@@ -166,8 +172,8 @@ __host__ __device__ inline size_t genz_block_smem_bytes(int64_t panel_len) { ret
 __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a, double *b, double *dvec,
                                                 double *svec, int64_t *perm, int64_t i0, int64_t i1, int64_t ii1,
                                                 const double *eps0_ptr, int64_t *rank, double *sh) {
-  __shared__ double red_v[32];
-  __shared__ int64_t red_i[32];
+  __shared__ unsigned long long red_k[32];
+  __shared__ unsigned red_t[32];
   __shared__ int64_t sh_im;
   __shared__ double sh_mii, sh_yi;
   __shared__ int sh_stop;
@@ -203,8 +209,8 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
   };
   for (int64_t i = i0; i <= i1; ++i) {
     // pivot scores :500-512, then argmin :514
-    double bv = 0.0;
-    int64_t bi = INT64_MAX;
+    unsigned long long key = ~0ull;  // this thread's least key, at its first position
+    unsigned pos = ~0u;
     for (int64_t k = i + tid; k <= ii1; k += blockDim.x) {
       const int64_t q = k - i0;
       double m_kk = dm_sub(s_g[q], s_d[q]);
@@ -213,34 +219,26 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
       double b_k = dm_mul(dm_div(dm_sub(s_b[q], s_s[q]), m_kk), c2);
       double o = dm_sub(det_erf(b_k), det_erf(a_k));
       s_o[q] = o;
-      if (bi == INT64_MAX) { bv = o; bi = k; }
-      else argmin_combine(bv, bi, o, k);
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
-      if (lane + off < 32 && i2 != INT64_MAX) {
-        if (bi == INT64_MAX) { bv = v2; bi = i2; }
-        else argmin_combine(bv, bi, v2, i2);
+      const unsigned long long ko = argmin_key(o);
+      if (ko < key) {
+        key = ko;
+        pos = (unsigned)q;
       }
     }
-    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
+    warp_argmin(key, pos);
+    if (lane == 0) {
+      red_k[wid] = key;
+      red_t[wid] = pos;
+    }
     __syncthreads();
     if (wid == 0) {
-      // the warps' minima reduced by warp 0 as a shuffle tree: the order
-      // (value in findmin order, then index) is a strict total order, so the
-      // minimum does not depend on the order of combination
+      // the warps' minima reduced by warp 0 (the key order with the position
+      // as tie-break is a strict total order: the same pivot in any grouping)
       const int nw = (int)(blockDim.x >> 5);
-      double v = lane < nw ? red_v[lane] : 0.0;
-      int64_t im = lane < nw ? red_i[lane] : INT64_MAX;
-      for (int off = 16; off > 0; off >>= 1) {
-        const double v2 = __shfl_down_sync(0xffffffffu, v, off);
-        const int64_t i2 = __shfl_down_sync(0xffffffffu, im, off);
-        if (lane + off < 32 && i2 != INT64_MAX) {
-          if (im == INT64_MAX) { v = v2; im = i2; }
-          else argmin_combine(v, im, v2, i2);
-        }
-      }
+      key = lane < nw ? red_k[lane] : ~0ull;
+      pos = lane < nw ? red_t[lane] : ~0u;
+      warp_argmin(key, pos);
+      const int64_t im = i0 + (int64_t)pos;
       if (lane == 0) {
       const int64_t qi = i - i0, qm = im - i0;
       double d_ii = s_o[qm];
@@ -388,10 +386,9 @@ __device__ __forceinline__ void named_bar_arrive(int id, int nthreads) {
 __device__ __forceinline__ void genz_block_onchip(double *M, int64_t n, double *a, double *b, double *dvec,
                                                   double *svec, int64_t *perm, int64_t i0, int64_t i1,
                                                   int64_t ii1, const double *eps0_ptr, int64_t *rank, double *sh) {
-  __shared__ double red_v[32];
-  __shared__ int64_t red_i[32];
-  __shared__ int64_t sh_im;
-  __shared__ double sh_mraw, sh_dii, sh_yi, sh_mij_im;
+  __shared__ unsigned long long red_k[32];
+  __shared__ unsigned red_t[32];
+  __shared__ double sh_yi, sh_mij_im;
   const double c2 = dm_div(1.0, dm_sqrt(2.0));
   const double is2pi = dm_div(2.0, dm_sqrt(dm_mul(2.0, M_PI)));
   const double eps0 = eps0_ptr[0];
@@ -436,8 +433,8 @@ __device__ __forceinline__ void genz_block_onchip(double *M, int64_t n, double *
   double mij = 0.0;                // M[i, kk] of the coming update
   // pivot score of this position for step i (:500-512), and the warp's minimum
   auto score = [&](int64_t i) {
-    double bv = 0.0;
-    int64_t bi = INT64_MAX;
+    unsigned long long key = ~0ull;
+    unsigned pos = ~0u;
     if (has_slot && kk >= i) {
       double m_kk = dm_sub(s_g[t], s_d[t]);
       m_kk = m_kk < 0 ? 0.0 : dm_sqrt(m_kk);
@@ -445,81 +442,63 @@ __device__ __forceinline__ void genz_block_onchip(double *M, int64_t n, double *
       double b_k = dm_mul(dm_div(dm_sub(s_b[t], s_s[t]), m_kk), c2);
       double o = dm_sub(det_erf(b_k), det_erf(a_k));
       s_o[t] = o;
-      bv = o;
-      bi = kk;
+      key = argmin_key(o);
+      pos = (unsigned)t;
     }
-    for (int off = 16; off > 0; off >>= 1) {
-      double v2 = __shfl_down_sync(0xffffffffu, bv, off);
-      int64_t i2 = __shfl_down_sync(0xffffffffu, bi, off);
-      if (lane + off < 32 && i2 != INT64_MAX) {
-        if (bi == INT64_MAX) { bv = v2; bi = i2; }
-        else argmin_combine(bv, bi, v2, i2);
-      }
+    warp_argmin(key, pos);
+    if (lane == 0) {
+      red_k[wid] = key;
+      red_t[wid] = pos;
     }
-    if (lane == 0) { red_v[wid] = bv; red_i[wid] = bi; }
   };
   for (int64_t i = i0; i <= i1; ++i) {
     const int np = (int)(i - i0);  // block pivots before i
     // one call site of the scores (their special functions are long code)
     if (!yw) score(i);
     __syncthreads();
-    if (wid == 0) {
-      // the warps' minima reduced by warp 0 (strict total order: the minimum
-      // does not depend on the order of combination)
-      constexpr int nw = NS / 32;
-      double v = lane < nw ? red_v[lane] : 0.0;
-      int64_t im = lane < nw ? red_i[lane] : INT64_MAX;
-      for (int off = 16; off > 0; off >>= 1) {
-        const double v2 = __shfl_down_sync(0xffffffffu, v, off);
-        const int64_t i2 = __shfl_down_sync(0xffffffffu, im, off);
-        if (lane + off < 32 && i2 != INT64_MAX) {
-          if (im == INT64_MAX) { v = v2; im = i2; }
-          else argmin_combine(v, im, v2, i2);
-        }
-      }
-      im = __shfl_sync(0xffffffffu, im, 0);
-      const int64_t qi = np, qm = im - i0;
-      if (lane == 0) {
-        sh_im = im;
-        sh_dii = s_o[qm];
-        sh_mraw = dm_sub(s_g[qm], s_d[qm]);
-      }
-      __syncwarp();
-      if (im != i && lane < 6) {  // :518-523 (and the diagonal, which the row/column swap moves)
-        if (lane == 0) {
-          const int64_t tp = s_p[qi]; s_p[qi] = s_p[qm]; s_p[qm] = tp;
-        } else {
-          double *arr = lane == 1 ? s_d : lane == 2 ? s_s : lane == 3 ? s_a : lane == 4 ? s_b : s_g;
-          const double tt = arr[qm]; arr[qm] = arr[qi]; arr[qi] = tt;
-        }
-      }
-    }
-    __syncthreads();
-    const int64_t im = sh_im;
-    const int qm = (int)(im - i0);
-    const double m_raw = sh_mraw;
+    // every warp reduces the warps' minima itself (the key order with the
+    // position as tie-break is a strict total order: the same pivot in each)
+    unsigned long long key = lane < NS / 32 ? red_k[lane] : ~0ull;
+    unsigned pos = lane < NS / 32 ? red_t[lane] : ~0u;
+    warp_argmin(key, pos);
+    const int qm = (int)pos;
+    const int64_t im = i0 + qm;
+    const double m_raw = dm_sub(s_g[qm], s_d[qm]);
     const bool stop = !(m_raw > eps0);  // the rank test of :533-537
     const double m_pp = stop ? 0.0 : dm_sqrt(m_raw);
     if (yw) {
       // y_i (:538-546) while the slot threads swap and update
+      // (the pivot's values are read at qm, before its swap with position np)
       if (lane == 0) {
         if (stop) {
           rank[0] = i;  // 0-based i == reference's i - 1
         } else {
-          double a_norm = dm_div(dm_sub(s_a[np], s_s[np]), m_pp);
-          double b_norm = dm_div(dm_sub(s_b[np], s_s[np]), m_pp);
+          double a_norm = dm_div(dm_sub(s_a[qm], s_s[qm]), m_pp);
+          double b_norm = dm_div(dm_sub(s_b[qm], s_s[qm]), m_pp);
           double ea = det_exp(dm_div(-dm_mul(a_norm, a_norm), 2.0));
           double eb = det_exp(dm_div(-dm_mul(b_norm, b_norm), 2.0));
-          sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), sh_dii);
+          sh_yi = dm_div(dm_mul(dm_sub(ea, eb), is2pi), s_o[qm]);
         }
       }
       __syncwarp();
+      named_bar_arrive(1, NALL);  // its reads of position qm are done
       if (stop) {
         write_back();
         return;
       }
       named_bar_arrive(2, NALL);
     } else {
+      // :518-523, the per-position values of np and qm trade places after
+      // barrier 1, when every read of them for this step is done: d and s,
+      // which the displaced candidate's update uses next, by the two threads
+      // (each takes the other's now and stores its own), the rest by thread np
+      const bool swp = im != i && (t == np || t == qm);
+      double x_d = 0.0, x_s = 0.0;
+      if (swp) {
+        const int o2 = t == np ? qm : np;
+        x_d = s_d[o2];
+        x_s = s_s[o2];
+      }
       // the pivot's register entries for every candidate's dot product, the
       // displaced candidate's for its new position
       if (t == qm) {
@@ -591,7 +570,18 @@ __device__ __forceinline__ void genz_block_onchip(double *M, int64_t n, double *
         if (has_slot && kk > i) mij = np == 0 ? M[kk * n + i] : M[i * n + kk];
         if (t == np && !stop) M[i * n + i] = m_pp;
       }
-      named_bar_sync(1, NS);
+      named_bar_sync(1, NALL);
+      if (swp) {
+        s_d[t] = x_d;
+        s_s[t] = x_s;
+        if (t == np) {
+          const int64_t tp = s_p[np]; s_p[np] = s_p[qm]; s_p[qm] = tp;
+          double tt;
+          tt = s_a[np]; s_a[np] = s_a[qm]; s_a[qm] = tt;
+          tt = s_b[np]; s_b[np] = s_b[qm]; s_b[qm] = tt;
+          tt = s_g[np]; s_g[np] = s_g[qm]; s_g[qm] = tt;
+        }
+      }
       if (im != i) {
         if (t == np) {
 #pragma unroll
