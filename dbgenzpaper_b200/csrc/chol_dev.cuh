@@ -373,6 +373,7 @@ __device__ __forceinline__ void genz_block_smem(double *M, int64_t n, double *a,
 constexpr int kFReg = 16;          // block pivots whose entries live in registers
 constexpr int kOnchipPiv = 64;     // pivots per block at most
 constexpr int kOnchipSlots = 512;  // slot threads; the block has one more warp
+constexpr int kSwapBatch = 2;      // swap indices per memory round trip
 __host__ __device__ inline size_t genz_block_onchip_bytes(int64_t panel_len) {
   return (size_t)(56 + 8 * (kOnchipPiv - kFReg)) * (size_t)panel_len + 8 * 2 * kFReg;
 }
@@ -523,49 +524,63 @@ __device__ __forceinline__ void genz_block_onchip(double *M, int64_t n, double *
         // (im,im) <- (i,i), (i,im) <- (im,i), (im,i) <- (i,im), and (i,i)
         // then takes the pivot m_ii.  Position k's thread does index k
         // (k >= i0), so it keeps the value its update reads: M[k, i] after the
-        // swap, or M[i, k] for the block's first pivot.  Two indices at a time:
-        // both loaded before either is stored.
-        auto swap_pair = [&](int64_t k0, int64_t k1) {
-          const bool live0 = k0 >= 0 && k0 != i && k0 != im, live1 = k1 >= 0 && k1 != i && k1 != im;
-          const bool row0 = live0 && k0 >= i0, row1 = live1 && k1 >= i0;
-          const double ri0 = row0 ? M[k0 * n + i] : 0.0, rm0 = row0 ? M[k0 * n + im] : 0.0;
-          const double ci0 = live0 ? M[i * n + k0] : 0.0, cm0 = live0 ? M[im * n + k0] : 0.0;
-          const double ri1 = row1 ? M[k1 * n + i] : 0.0, rm1 = row1 ? M[k1 * n + im] : 0.0;
-          const double ci1 = live1 ? M[i * n + k1] : 0.0, cm1 = live1 ? M[im * n + k1] : 0.0;
-          auto store = [&](int64_t k, bool live, bool row, double r_i, double r_m, double c_i, double c_m) {
+        // swap, or M[i, k] for the block's first pivot.  This thread's indices
+        // are its own position i0 + t, then the indices outside the panel
+        // ([0, i0) and (ii1, n), numbered o = 0, 1, ...) o = t + e NS:
+        // kSwapBatch of them at a time, all loaded before any is stored (no
+        // element is shared between threads), so the swap costs one memory
+        // round trip per batch -- one in all when n <= len + NS.
+        const int64_t nOwn = has_slot ? 1 : 0;
+        const int64_t nOut = t < n - len ? (n - len - t + NS - 1) / NS : 0;
+        for (int64_t e0 = 0; e0 < nOwn + nOut; e0 += kSwapBatch) {
+          auto kidx = [&](int e) -> int64_t {
+            const int64_t q = e0 + e;
+            if (q < nOwn) return kk;
+            if (q >= nOwn + nOut) return -1;
+            const int64_t o = t + (q - nOwn) * NS;
+            return o < i0 ? o : o + len;
+          };
+          double ri[kSwapBatch], rm[kSwapBatch], ci[kSwapBatch], cm[kSwapBatch];
+          bool diag = false;
+#pragma unroll
+          for (int e = 0; e < kSwapBatch; ++e) {
+            const int64_t k = kidx(e);
+            diag = diag || k == i;
+            const bool live = k >= 0 && k != i && k != im, row = live && k >= i0;
+            ri[e] = row ? M[k * n + i] : 0.0;
+            rm[e] = row ? M[k * n + im] : 0.0;
+            ci[e] = live ? M[i * n + k] : 0.0;
+            cm[e] = live ? M[im * n + k] : 0.0;
+          }
+          double d_ii = 0.0, d_mm = 0.0, d_mi = 0.0, d_im = 0.0;
+          if (diag) {
+            d_ii = M[i * n + i];
+            d_mm = M[im * n + im];
+            d_mi = M[i * n + im];
+            d_im = M[im * n + i];
+          }
+#pragma unroll
+          for (int e = 0; e < kSwapBatch; ++e) {
+            const int64_t k = kidx(e);
+            const bool live = k >= 0 && k != i && k != im, row = live && k >= i0;
             if (row) {
-              M[k * n + i] = r_m;
-              M[k * n + im] = r_i;
+              M[k * n + i] = rm[e];
+              M[k * n + im] = ri[e];
             }
             if (live) {
-              M[i * n + k] = c_m;
-              M[im * n + k] = c_i;
-              if (k == kk) mij = np == 0 ? r_m : c_m;
+              M[i * n + k] = cm[e];
+              M[im * n + k] = ci[e];
+              if (k == kk) mij = np == 0 ? rm[e] : cm[e];
             }
-            if (k == i) {
-              const double ii = M[i * n + i], mm = M[im * n + im], im_i = M[i * n + im], i_im = M[im * n + i];
-              M[i * n + i] = stop ? mm : m_pp;
-              M[im * n + im] = ii;
-              M[im * n + i] = im_i;
-              M[i * n + im] = i_im;
-              sh_mij_im = np == 0 ? im_i : i_im;  // for position im
-            }
-          };
-          store(k0, live0, row0, ri0, rm0, ci0, cm0);
-          store(k1, live1, row1, ri1, rm1, ci1, cm1);
-        };
-        int64_t pend = -1;
-        auto push = [&](int64_t k) {
-          if (pend < 0) {
-            pend = k;
-          } else {
-            swap_pair(pend, k);
-            pend = -1;
           }
-        };
-        for (int64_t k = i0 + t; k < n; k += NS) push(k);
-        for (int64_t k = t; k < i0; k += NS) push(k);
-        if (pend >= 0) swap_pair(pend, -1);
+          if (diag) {
+            M[i * n + i] = stop ? d_mm : m_pp;
+            M[im * n + im] = d_ii;
+            M[im * n + i] = d_mi;
+            M[i * n + im] = d_im;
+            sh_mij_im = np == 0 ? d_mi : d_im;  // for position im
+          }
+        }
       } else {
         if (has_slot && kk > i) mij = np == 0 ? M[kk * n + i] : M[i * n + kk];
         if (t == np && !stop) M[i * n + i] = m_pp;
