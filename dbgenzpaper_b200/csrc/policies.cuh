@@ -89,6 +89,14 @@ struct GradIO {
     if (sizeof(T) == 4) return ((g >> 7) * rows + (row - row0)) * 128 + (g & 127);
     return (row - row0) * N + g;
   }
+  // at(row, g) = at0(g) + row * stride(): the sample's part, computed once per
+  // tile, and a row stride (a constant 128 for FP32), so that a step's
+  // address is one multiply-add on the row (constant offsets inside a chunk)
+  __device__ __forceinline__ int64_t at0(int64_t g) const {
+    if (sizeof(T) == 4) return ((g >> 7) * rows - row0) * 128 + (g & 127);
+    return g - row0 * N;
+  }
+  __device__ __forceinline__ int64_t stride() const { return sizeof(T) == 4 ? (int64_t)128 : N; }
 };
 
 // Asynchronous global -> shared copy of `BYTES` (4, 8 or 16) bytes, or zeros
@@ -147,6 +155,7 @@ struct Forward {
   uint32_t rmask;  // steps k of the current chunk whose weight factor consume_deferred left out
   dbgz::GenParams gen;
   int64_t j, k, g;  // point index in the pass, shift, global sample index
+  int64_t ga0;      // io.at0(g)
   int64_t d;
   int cdf_form;
   GradIO<T> io;
@@ -164,6 +173,7 @@ struct Forward {
     g = (tile - io_.tile0) * 128 + r;
     cdf_form = cdf_form_;
     io = io_;
+    ga0 = io.at0(g);
     st.init(c1, dc1, up1);
     st.set_form(cdf_form_);
     if (LOGW) lw = log(dc1);
@@ -195,7 +205,7 @@ struct Forward {
   // them (GenParams::sobol_staged), else unused
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
     const T y = st.template quantile<!STORE>(gen, d, j, k, l, sg.qv[li], sg.shv[li], xs);
-    if (STORE) io.y[io.at(l, g)] = y;
+    if (STORE) io.y[ga0 + l * io.stride()] = y;
     return y;
   }
   // chunked form (8 steps whose per-sample inputs may be loaded up front)
@@ -212,8 +222,8 @@ struct Forward {
     st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
     if (LOGW) lw += log((double)st.dc);
     if (STORE) {
-      io.s[io.at(l + 1, g)] = s;
-      io.dc[io.at(l + 1, g)] = (T)st.dc;
+      io.s[ga0 + (l + 1) * io.stride()] = s;
+      io.dc[ga0 + (l + 1) * io.stride()] = (T)st.dc;
     }
   }
   // consume for step k (0..7) of a chunk, without the same-tail branch
@@ -225,8 +235,8 @@ struct Forward {
     rmask |= left ? (1u << k) : 0u;
     if (LOGW) lw += left ? 0.0 : log((double)st.dc);
     if (STORE) {
-      io.s[io.at(l + 1, g)] = s;
-      io.dc[io.at(l + 1, g)] = (T)st.dc;
+      io.s[ga0 + (l + 1) * io.stride()] = s;
+      io.dc[ga0 + (l + 1) * io.stride()] = (T)st.dc;
     }
   }
   // The factors consume_deferred left out in a chunk of 8 steps starting at
@@ -248,7 +258,7 @@ struct Forward {
         const float d = Step::tail_exact(sk, tg.a, tg.b, tg.inv_u);
         st.p *= (double)d;
         if (LOGW) lw += log((double)d);
-        if (STORE) io.dc[io.at(l0 + k + 1, g)] = d;
+        if (STORE) io.dc[ga0 + (l0 + k + 1) * io.stride()] = d;
       }
       rmask = 0u;
     }
@@ -288,6 +298,7 @@ struct Adjoint {
   __device__ __forceinline__ int64_t sobol_l0(int64_t lbase) const { return d - 1 - lbase; }
   dbgz::GenParams gen;
   int64_t j, k, g, d, tile;
+  int64_t ga0;  // io.at0(g)
   GradIO<T> io;
   // saved receiver value: ybar of the variable the next step handles, in the
   // working type (it is a sum of the loop's working type; no round trip
@@ -314,6 +325,7 @@ struct Adjoint {
     j = (tile - k * tiles_per_shift) * 128 + r;
     g = (tile - io_.tile0) * 128 + r;
     io = io_;
+    ga0 = io.at0(g);
     ybar = T(0);  // variable d-1 has no u: nothing downstream of it
     p = io.p[g];
     warp = r >> 5;
@@ -519,7 +531,7 @@ struct Adjoint {
   // is not done.)
   __device__ __forceinline__ void store_gemm(int64_t t, bool, T, double psb) const {
     if (!io.sbar) return;
-    io.sbar[io.at(t, g)] = sizeof(T) == 4 ? (T)tf32_rn((float)psb) : (T)psb;
+    io.sbar[ga0 + t * io.stride()] = sizeof(T) == 4 ? (T)tf32_rn((float)psb) : (T)psb;
   }
   __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc, uint32_t xs) {
     const int64_t t = d - 1 - l;
@@ -543,8 +555,8 @@ struct Adjoint {
   }
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
     const int64_t t = d - 1 - l;
-    const T y = t <= d - 2 ? io.y[io.at(t, g)] : T(0);
-    return emit_from(sg, li, l, y, io.s[io.at(t, g)], io.dc[io.at(t, g)], xs);
+    const T y = t <= d - 2 ? io.y[ga0 + t * io.stride()] : T(0);
+    return emit_from(sg, li, l, y, io.s[ga0 + t * io.stride()], io.dc[ga0 + t * io.stride()], xs);
   }
   // chunked form: the stored state of the chunk's 8 steps (steps l0 .. l0+7,
   // n of them valid) is loaded before the first, so the loads overlap; in
@@ -558,9 +570,9 @@ struct Adjoint {
     for (int kk = 0; kk < 8; ++kk) {
       const int64_t t = d - 1 - (l0 + kk);
       const bool v = kk < n;
-      pre_y[kk] = (v && t <= d - 2) ? io.y[io.at(t, g)] : T(0);
-      pre_s[kk] = v ? io.s[io.at(t, g)] : T(0);
-      pre_dc[kk] = v ? io.dc[io.at(t, g)] : T(0);
+      pre_y[kk] = (v && t <= d - 2) ? io.y[ga0 + t * io.stride()] : T(0);
+      pre_s[kk] = v ? io.s[ga0 + t * io.stride()] : T(0);
+      pre_dc[kk] = v ? io.dc[ga0 + t * io.stride()] : T(0);
       acc_a[kk] = acc_b[kk] = acc_u[kk] = 0.0f;
     }
     fp64_done = 0u;
@@ -571,9 +583,9 @@ struct Adjoint {
     for (int kk = 0; kk < 8; ++kk) {
       const int64_t t = d - 1 - (l0 + 8 + kk);
       if (t >= 1) {
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(io.y + io.at(t, g)));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(io.s + io.at(t, g)));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(io.dc + io.at(t, g)));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(io.y + ga0 + t * io.stride()));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(io.s + ga0 + t * io.stride()));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(io.dc + ga0 + t * io.stride()));
       }
     }
   }
@@ -675,7 +687,7 @@ struct Adjoint {
     sg0.qv[0] = gen.q ? gen.q[0] : 0.0;
     sg0.shv[0] = shift_at<T>(gen, k * (d - 1));
     const double w = point_w(sg0, 0, 0, 0u, false);
-    const T y = io.y[io.at(0, g)];
+    const T y = io.y[ga0];
     double ga, gb, gu;
     variable(tgt[0], w, true, y, T(0), (T)io.dc1, false, ga, gb, gu);
     accumulate(0, ga, gb, gu);
