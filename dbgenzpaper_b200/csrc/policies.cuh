@@ -298,6 +298,7 @@ struct Adjoint {
   __device__ __forceinline__ int64_t sobol_l0(int64_t lbase) const { return d - 1 - lbase; }
   dbgz::GenParams gen;
   int64_t j, k, g, d, tile;
+  double jd;    // gen.gen_base + j + 1: the lattice point's multiplier
   int64_t ga0;  // io.at0(g)
   GradIO<T> io;
   // saved receiver value: ybar of the variable the next step handles, in the
@@ -323,6 +324,7 @@ struct Adjoint {
     tile = tile_;
     k = tile / tiles_per_shift;
     j = (tile - k * tiles_per_shift) * 128 + r;
+    jd = (double)(gen.gen_base + j + 1);
     g = (tile - io_.tile0) * 128 + r;
     io = io_;
     ga0 = io.at0(g);
@@ -370,7 +372,7 @@ struct Adjoint {
                                             bool staged) const {
     double u;
     if (GEN == 0) {
-      double x = __dmul_rn((double)(gen.gen_base + j + 1), sg.qv[li]);
+      double x = __dmul_rn(jd, sg.qv[li]);
       x = x - floor(x);
       if (sizeof(T) == 4) {
         float uf = (float)sg.shv[li] + (float)x;
@@ -397,7 +399,7 @@ struct Adjoint {
   __device__ __forceinline__ float point_w32(const Staged<T> &sg, int li, int64_t t, uint32_t xs,
                                              bool staged) const {
     if (GEN == 0) {
-      double x = __dmul_rn((double)(gen.gen_base + j + 1), sg.qv[li]);
+      double x = __dmul_rn(jd, sg.qv[li]);
       x = x - floor(x);
       float uf = (float)sg.shv[li] + (float)x;
       uf = uf > 1.0f ? uf - 1.0f : uf;
