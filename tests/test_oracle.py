@@ -28,6 +28,42 @@ def test_det_erf_exp_accuracy(oracle):
     assert oracle.det_exp(-float("inf")) == 0.0
 
 
+def test_det_erf_within_two_ulp_of_correctly_rounded(oracle):
+    # the fitted polynomials of det_erf against 40-digit erf rounded once
+    mp = pytest.importorskip("mpmath")
+    mp.mp.dps = 40
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([rng.uniform(0, 6.5, 3000), rng.uniform(0, 1e-3, 200),
+                         2.5 * (1 + rng.uniform(-1e-9, 1e-9, 200)), -rng.uniform(0, 6.5, 200)])
+    for x in xs:
+        r = float(mp.erf(mp.mpf(float(x))))
+        assert abs(oracle.det_erf(float(x)) - r) <= 2 * math.ulp(r if r != 0 else 1e-300), x
+
+
+def test_det_erf_tables_match_their_fit():
+    # the coefficient tables in detmath.h are what detmath_fit.py prints
+    import contextlib
+    import importlib.util
+    import io
+    import re
+    here = os.path.join(os.path.dirname(os.path.dirname(__file__)), "dbgenzpaper_b200", "csrc")
+    pytest.importorskip("mpmath")
+    spec = importlib.util.spec_from_file_location("detmath_fit", os.path.join(here, "detmath_fit.py"))
+    fit = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(fit)
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        fit.main()
+    header = open(os.path.join(here, "detmath.h")).read()
+
+    def table(text, name):
+        body = re.search(r"#define %s \{(.*?)\}" % name, text, re.S).group(1)
+        return [float.fromhex(v.strip()) for v in body.replace("\\", "").split(",")]
+
+    for name in ("DBGZ_ERF_SMALL_TABLE", "DBGZ_ERFC_MID_TABLE"):
+        assert table(header, name) == table(buf.getvalue(), name)
+
+
 def test_erfinv_accuracy(oracle):
     for u in np.concatenate([np.linspace(-0.999999, 0.999999, 801), [1 - 2e-16, -1 + 2e-16, 1e-300]]):
         r = sp_erfinv(u)
