@@ -50,7 +50,7 @@ TRAFFIC_PER_LAUNCH = 16 * (239.36e6 + 328.14e6)
 # timed launch
 INST_PER_SAMPLE = 6.788e8 / 131072
 XU_PIPE_PCT = 15.4
-ISSUE_PROFILE = "profiles/genz_umma_splitbf16_d1000_8192pts_full.md"
+ISSUE_PROFILE = "ncu --set full of the split-BF16 loop at d=1000, 8192 points x 16 shifts (profiles/)"
 
 
 def _peaks():
@@ -853,7 +853,7 @@ def main():
                 "inst_per_launch": INST_PER_SAMPLE * w.samples,
                 "inst_per_sample_dim": INST_PER_SAMPLE / (d - 1),
                 "xu_pipe_pct_of_peak": XU_PIPE_PCT,
-                "source": "instruction count from the ncu capture in " + ISSUE_PROFILE +
+                "source": "instruction count from " + ISSUE_PROFILE +
                           " scaled by the sample count; time from this run's CUDA events",
                 "applies_to": "fp32_split_bf16" if args.precision == "fp32_split_bf16" else "stale: other precision"},
             "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

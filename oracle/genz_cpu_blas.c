@@ -1,7 +1,7 @@
 /*
  * genz_cpu_blas.c -- the reference's Float64 qmc_loop! as it runs on a CPU:
  * the timed CPU baseline of bench.py (its cpu_baseline leg and the
- * --impl reference arm).  BASELINE INFRASTRUCTURE ONLY, like the checker in
+ * --impl reference arm).  CPU-BASELINE INFRASTRUCTURE ONLY, like the checker in
  * genz_oracle.c: nothing in dbgenzpaper_b200/ links or calls it.
  *
  * Where genz_oracle.c restates the reference for exact comparison (scalar
