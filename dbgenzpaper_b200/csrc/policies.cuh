@@ -205,7 +205,7 @@ struct Forward {
   // them (GenParams::sobol_staged), else unused
   __device__ __forceinline__ T emit(const Staged<T> &sg, int li, int64_t l, uint32_t xs = 0u) {
     const T y = st.template quantile<!STORE>(gen, d, j, k, l, sg.qv[li], sg.shv[li], xs);
-    if (STORE) io.y[ga0 + l * io.stride()] = y;
+    if (STORE) __stcs(io.y + ga0 + l * io.stride(), y);
     return y;
   }
   // chunked form (8 steps whose per-sample inputs may be loaded up front)
@@ -222,8 +222,8 @@ struct Forward {
     st.cdf(s, tg.a, tg.b, tg.inv_u, cdf_form);
     if (LOGW) lw += log((double)st.dc);
     if (STORE) {
-      io.s[ga0 + (l + 1) * io.stride()] = s;
-      io.dc[ga0 + (l + 1) * io.stride()] = (T)st.dc;
+      __stcs(io.s + ga0 + (l + 1) * io.stride(), s);
+      __stcs(io.dc + ga0 + (l + 1) * io.stride(), (T)st.dc);
     }
   }
   // consume for step k (0..7) of a chunk, without the same-tail branch
@@ -235,8 +235,8 @@ struct Forward {
     rmask |= left ? (1u << k) : 0u;
     if (LOGW) lw += left ? 0.0 : log((double)st.dc);
     if (STORE) {
-      io.s[ga0 + (l + 1) * io.stride()] = s;
-      io.dc[ga0 + (l + 1) * io.stride()] = (T)st.dc;
+      __stcs(io.s + ga0 + (l + 1) * io.stride(), s);
+      __stcs(io.dc + ga0 + (l + 1) * io.stride(), (T)st.dc);
     }
   }
   // The factors consume_deferred left out in a chunk of 8 steps starting at
@@ -258,7 +258,7 @@ struct Forward {
         const float d = Step::tail_exact(sk, tg.a, tg.b, tg.inv_u);
         st.p *= (double)d;
         if (LOGW) lw += log((double)d);
-        if (STORE) io.dc[ga0 + (l0 + k + 1) * io.stride()] = d;
+        if (STORE) __stcs(io.dc + ga0 + (l0 + k + 1) * io.stride(), (T)d);
       }
       rmask = 0u;
     }
@@ -533,7 +533,7 @@ struct Adjoint {
   // is not done.)
   __device__ __forceinline__ void store_gemm(int64_t t, bool, T, double psb) const {
     if (!io.sbar) return;
-    io.sbar[ga0 + t * io.stride()] = sizeof(T) == 4 ? (T)tf32_rn((float)psb) : (T)psb;
+    __stcs(io.sbar + ga0 + t * io.stride(), sizeof(T) == 4 ? (T)tf32_rn((float)psb) : (T)psb);
   }
   __device__ __forceinline__ T emit_from(const Staged<T> &sg, int li, int64_t l, T y, T s, T dc, uint32_t xs) {
     const int64_t t = d - 1 - l;
@@ -572,9 +572,9 @@ struct Adjoint {
     for (int kk = 0; kk < 8; ++kk) {
       const int64_t t = d - 1 - (l0 + kk);
       const bool v = kk < n;
-      pre_y[kk] = (v && t <= d - 2) ? io.y[ga0 + t * io.stride()] : T(0);
-      pre_s[kk] = v ? io.s[ga0 + t * io.stride()] : T(0);
-      pre_dc[kk] = v ? io.dc[ga0 + t * io.stride()] : T(0);
+      pre_y[kk] = (v && t <= d - 2) ? __ldcs(io.y + ga0 + t * io.stride()) : T(0);
+      pre_s[kk] = v ? __ldcs(io.s + ga0 + t * io.stride()) : T(0);
+      pre_dc[kk] = v ? __ldcs(io.dc + ga0 + t * io.stride()) : T(0);
       acc_a[kk] = acc_b[kk] = acc_u[kk] = 0.0f;
     }
     fp64_done = 0u;
